@@ -1,0 +1,218 @@
+"""B200-native ALE-BGK time step behind the reference's solver-step interface.
+
+Host-side mirror of panchiittp/ALEBGK4Paper's GPU driver API
+(Solver/Solver.cpp:67-89): :class:`Case` builds one of the reference's six
+lid-driven-cavity clouds on the host (TestCases/TestCases.cpp:56-294), and
+:class:`Solver` keeps it on one B200 and advances it with the sm_100a kernels
+of ``libalebgk_b200.so`` through the C-ABI of ``include/alebgk.h``.  Method
+names follow the reference's ``cuda*`` functions so that code written against
+the reference reads the same.  There is no CPU fallback: every call goes
+through the CUDA library and fails loudly if it cannot.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _abi
+
+__all__ = ["Case", "Solver", "AlebgkError", "load_library", "CASE_NAMES"]
+
+CASE_NAMES = ("cavity2d", "cavity3d", "cavity2d-square", "cavity2d-circle",
+              "cavity3d-sphere", "cavity3d-cube")
+
+
+class AlebgkError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"alebgk error {code}: {msg}")
+        self.code = code
+
+
+def load_library():
+    return _abi.load()
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(_abi.c_double_p)
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(_abi.c_int_p)
+
+
+def _check(rc: int, ctx=None):
+    if rc != 0:
+        lib = _abi.load()
+        buf = ctypes.create_string_buffer(512)
+        lib.alebgk_last_error(ctx, buf, 512)
+        raise AlebgkError(rc, buf.value.decode(errors="replace"))
+
+
+class Case:
+    """A case cloud built on the host, as TestCases/main.cpp:193-345 builds it.
+
+    Arrays (numpy, owned by this object): ``xyz`` (N,3), ``meshv`` (N,3),
+    ``wall`` (N,7), ``boundary`` (N,), ``body_id`` (N,), ``nnb`` (N,),
+    ``nbr`` (N,128), ``g`` (N,gstride) FP64, ``macro`` (N,7).
+    """
+
+    def __init__(self, name: str, Nx: int = -1, Nv: int = -1, dt: float = -1.0,
+                 mls_order: int = 2, fixed_body: bool = False, body_scale: float = 1.0):
+        lib = _abi.load()
+        h = ctypes.c_void_p()
+        _check(lib.alebgk_case_build(name.encode(), int(Nx), int(Nv), float(dt),
+                                     int(mls_order), int(bool(fixed_body)),
+                                     float(body_scale), ctypes.byref(h)))
+        try:
+            info = np.zeros(8, np.int32)
+            prm = np.zeros(24)
+            _check(lib.alebgk_case_info(h, _ip(info), _dp(prm)))
+            view = _abi.Cloud()
+            _check(lib.alebgk_case_view(h, ctypes.byref(view)))
+            N, gs = int(info[0]), int(info[3])
+            self.name = name
+            self.N, self.dim, self.Nv, self.gstride = N, int(info[1]), int(info[2]), gs
+            self.nbodies, self.mls_order, self.Nx = int(info[4]), int(info[5]), int(info[6])
+            self.moving_bodies = bool(info[7])
+            keys = ("dt", "tau", "R", "dx", "dy", "dz", "radius", "minDist", "dv",
+                    "vmin", "vmax", "rho0", "Tw", "xleft", "xright", "ybottom", "ytop",
+                    "zfront", "zback", "dt_requested", "tfinal", "dHS", "lid_speed",
+                    "save_every")
+            self.params = {k: float(v) for k, v in zip(keys, prm)}
+            self.dt = self.params["dt"]
+
+            def arr(ptr, n, dtype, shape):
+                return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dtype).reshape(shape)
+
+            self.xyz = arr(view.xyz, 3 * N, np.float64, (N, 3))
+            self.meshv = arr(view.meshv, 3 * N, np.float64, (N, 3))
+            self.wall = arr(view.wall, 7 * N, np.float64, (N, 7))
+            self.boundary = arr(view.boundary, N, np.int32, (N,))
+            self.body_id = arr(view.body_id, N, np.int32, (N,))
+            self.nnb = arr(view.nnb, N, np.int32, (N,))
+            self.nbr = arr(view.nbr, N * _abi.MAX_NEIGH, np.int32, (N, _abi.MAX_NEIGH))
+            self.g = arr(view.g, N * gs, np.float64, (N, gs))
+            self.macro = arr(view.macro, 7 * N, np.float64, (N, 7))
+            bodies = np.zeros(32 * max(1, self.nbodies))
+            _check(lib.alebgk_case_bodies(h, _dp(bodies)))
+            self.bodies = bodies.reshape(-1, 32)[: self.nbodies].copy()
+        finally:
+            lib.alebgk_case_free(h)
+
+    def config(self, precision: int = 32, device: int = 0) -> _abi.Config:
+        cfg = _abi.Config()
+        cfg.dim, cfg.N, cfg.Nv = self.dim, self.N, self.Nv
+        cfg.mls_order, cfg.precision, cfg.limiter = self.mls_order, precision, 2
+        cfg.tau_variable, cfg.device = 0, device
+        cfg.R, cfg.tau, cfg.dHS = self.params["R"], self.params["tau"], self.params["dHS"]
+        cfg.vmin, cfg.dv, cfg.radius = self.params["vmin"], self.params["dv"], self.params["radius"]
+        return cfg
+
+    def cloud(self) -> _abi.Cloud:
+        """A C-ABI view of this case's arrays (kept alive by this object)."""
+        self._keep = [np.ascontiguousarray(a) for a in
+                      (self.xyz, self.meshv, self.wall, self.boundary, self.body_id,
+                       self.nnb, self.nbr, self.g, self.macro)]
+        xyz, mv, wall, b, bid, nnb, nbr, g, mac = self._keep
+        return _abi.Cloud(_dp(xyz), _dp(mv), _dp(wall), _ip(b), _ip(bid), _ip(nnb),
+                          _ip(nbr), _dp(g), _dp(mac))
+
+
+class Solver:
+    """One device-resident cloud advanced by the B200 step.
+
+    Mirrors the reference's CUDA driver API (Solver/Solver.cpp:67-89):
+    construction is ``cudaUploadCloud``; ``cudaStep``, ``cudaDownloadMoments``,
+    ``cudaDownloadFull``, ``cudaTotalMass``, ``cudaLimiterCounts``,
+    ``cudaMlsCounts``, ``cudaMassBudget``, ``cudaWallMomentum`` and
+    ``cudaFreeCloud`` keep the reference's names and meaning.
+    """
+
+    def __init__(self, case: Case, precision: int = 32, device: int = 0,
+                 dt: float | None = None, config: _abi.Config | None = None):
+        self.lib = _abi.load()
+        self.case = case
+        self.N, self.gstride, self.dim = case.N, case.gstride, case.dim
+        self.precision = precision
+        self.dt = float(dt if dt is not None else case.dt)
+        cfg = config if config is not None else case.config(precision, device)
+        self.cfg = cfg
+        h = ctypes.c_void_p()
+        _check(self.lib.alebgk_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self.ctx = h
+        self.cudaUploadCloud(case)
+
+    # -- reference-named API ------------------------------------------------
+    def cudaUploadCloud(self, case: Case):
+        cl = case.cloud()
+        _check(self.lib.alebgk_upload(self.ctx, ctypes.byref(cl), self.dt), self.ctx)
+
+    def cudaStep(self, nsteps: int = 1):
+        _check(self.lib.alebgk_step(self.ctx, int(nsteps)), self.ctx)
+
+    step = cudaStep
+
+    def sync(self):
+        _check(self.lib.alebgk_sync(self.ctx), self.ctx)
+
+    def cudaDownloadMoments(self, out: np.ndarray | None = None) -> np.ndarray:
+        m = out if out is not None else np.zeros((self.N, 7))
+        _check(self.lib.alebgk_download_moments(self.ctx, _dp(m)), self.ctx)
+        return m
+
+    def cudaDownloadFull(self):
+        g = np.zeros((self.N, self.gstride))
+        m = np.zeros((self.N, 7))
+        _check(self.lib.alebgk_download_full(self.ctx, _dp(g), _dp(m)), self.ctx)
+        return g, m
+
+    def counters(self) -> dict:
+        c = _abi.Counters()
+        _check(self.lib.alebgk_get_counters(self.ctx, ctypes.byref(c)), self.ctx)
+        return {k: getattr(c, k) for k, _ in _abi.Counters._fields_}
+
+    def cudaLimiterCounts(self):
+        c = self.counters()
+        return c["positivity_fixes"], c["transport_flags"]
+
+    def cudaMlsCounts(self):
+        c = self.counters()
+        return c["mls_degenerate"], 0
+
+    def cudaMassBudget(self):
+        c = self.counters()
+        return c["mass_after_transport"] * c["mass_scale"], c["mass_end"]
+
+    def cudaTotalMass(self) -> float:
+        v = ctypes.c_double()
+        _check(self.lib.alebgk_total_mass(self.ctx, ctypes.byref(v)), self.ctx)
+        return v.value
+
+    def cudaWallMomentum(self) -> np.ndarray:
+        d = np.zeros(self.N)
+        _check(self.lib.alebgk_wall_momentum(self.ctx, _dp(d)), self.ctx)
+        return d
+
+    def body_loads(self, centres: np.ndarray, areas: np.ndarray) -> np.ndarray:
+        nb = len(areas)
+        c = np.ascontiguousarray(centres, np.float64).reshape(nb, 3)
+        a = np.ascontiguousarray(areas, np.float64)
+        out = np.zeros((nb, 6))
+        _check(self.lib.alebgk_body_loads(self.ctx, nb, _dp(c), _dp(a), _dp(out)), self.ctx)
+        return out
+
+    def cudaFreeCloud(self):
+        if getattr(self, "ctx", None):
+            self.lib.alebgk_destroy(self.ctx)
+            self.ctx = None
+
+    close = cudaFreeCloud
+
+    def __del__(self):
+        try:
+            self.cudaFreeCloud()
+        except Exception:
+            pass

@@ -1,0 +1,115 @@
+"""ctypes declarations of ``include/alebgk.h`` (the library's C-ABI)."""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libalebgk_b200.so")
+
+c_int_p = ctypes.POINTER(ctypes.c_int)
+c_double_p = ctypes.POINTER(ctypes.c_double)
+
+MAX_NEIGH = 128
+NSTAGES = 8
+STAGES = ("transport", "post_transport", "redo", "mass_after_transport",
+          "finalize", "recollide", "mass_end", "step_begin")
+OK, EINVAL, ECUDA, ESTATE, ENOMEM, EDEVICE = 0, -1, -2, -3, -4, -5
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("dim", ctypes.c_int), ("N", ctypes.c_int), ("Nv", ctypes.c_int),
+        ("mls_order", ctypes.c_int), ("precision", ctypes.c_int),
+        ("limiter", ctypes.c_int), ("tau_variable", ctypes.c_int),
+        ("device", ctypes.c_int),
+        ("R", ctypes.c_double), ("tau", ctypes.c_double), ("dHS", ctypes.c_double),
+        ("vmin", ctypes.c_double), ("dv", ctypes.c_double), ("radius", ctypes.c_double),
+        ("periodic", ctypes.c_int * 3), ("L", ctypes.c_double * 3),
+    ]
+
+
+class Cloud(ctypes.Structure):
+    _fields_ = [
+        ("xyz", c_double_p), ("meshv", c_double_p), ("wall", c_double_p),
+        ("boundary", c_int_p), ("body_id", c_int_p), ("nnb", c_int_p),
+        ("nbr", c_int_p), ("g", c_double_p), ("macro", c_double_p),
+    ]
+
+
+class Counters(ctypes.Structure):
+    _fields_ = [
+        ("steps", ctypes.c_int64), ("transport_flags", ctypes.c_int),
+        ("positivity_fixes", ctypes.c_int), ("mood_fail", ctypes.c_int),
+        ("mls_degenerate", ctypes.c_int),
+        ("mass_before", ctypes.c_double), ("mass_after_transport", ctypes.c_double),
+        ("mass_scale", ctypes.c_double), ("mass_end", ctypes.c_double),
+        ("error_word", ctypes.c_int),
+    ]
+
+
+# name -> (restype, argtypes); every exported symbol of include/alebgk.h
+SIGNATURES = {
+    "alebgk_create": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(ctypes.c_void_p)]),
+    "alebgk_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "alebgk_last_error": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
+    "alebgk_upload": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Cloud), ctypes.c_double]),
+    "alebgk_upload_state": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p]),
+    "alebgk_download_moments": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "alebgk_download_full": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p]),
+    "alebgk_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "alebgk_sync": (ctypes.c_int, [ctypes.c_void_p]),
+    "alebgk_step_timed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_float)]),
+    "alebgk_profile_steps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_float)]),
+    "alebgk_coeff_build": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(Cloud),
+                                          ctypes.c_double, ctypes.POINTER(ctypes.c_void_p)]),
+    "alebgk_coeff_info": (ctypes.c_int, [ctypes.c_void_p, c_int_p]),
+    "alebgk_coeff_get": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p, c_int_p,
+                                        c_double_p]),
+    "alebgk_coeff_free": (None, [ctypes.c_void_p]),
+    "alebgk_get_counters": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Counters)]),
+    "alebgk_total_mass": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "alebgk_wall_momentum": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "alebgk_device_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                                           c_int_p, c_int_p]),
+    "alebgk_body_loads": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p,
+                                         c_double_p, c_double_p]),
+    "alebgk_body_set_surface_velocity": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                                        c_double_p, c_double_p]),
+    "alebgk_case_build": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_double, ctypes.POINTER(ctypes.c_void_p)]),
+    "alebgk_case_free": (None, [ctypes.c_void_p]),
+    "alebgk_case_info": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_double_p]),
+    "alebgk_case_view": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Cloud)]),
+    "alebgk_case_bodies": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "alebgk_case_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                          ctypes.POINTER(Config)]),
+}
+
+_lib = None
+
+
+def load(path: str | None = None) -> ctypes.CDLL:
+    """Loads the in-tree library and declares every C-ABI signature.
+
+    Raises if the library is missing: there is no fallback implementation.
+    """
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(
+            f"{p} is missing: build it with `python -m alebgk4paper_b200.build` "
+            "(the ALE-BGK step has no CPU fallback)")
+    lib = ctypes.CDLL(p)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib

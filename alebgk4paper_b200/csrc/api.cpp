@@ -1,0 +1,670 @@
+// api.cpp -- the C-ABI of include/alebgk.h: contexts, upload/download,
+// coefficient build, CUDA-graph step, body loads, host case set-up.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "cases.h"
+#include "coeffs.h"
+#include "ctx.h"
+
+using namespace alebgk;
+
+namespace {
+
+std::string gCreateError;
+
+int fail(alebgk_ctx *c, int code, const std::string &msg)
+{
+    if (c) c->err = msg; else gCreateError = msg;
+    return code;
+}
+
+#define CK(call)                                                              \
+    do {                                                                      \
+        cudaError_t e_ = (call);                                              \
+        if (e_ != cudaSuccess)                                                \
+            return fail(c, ALEBGK_ECUDA, std::string(#call) + ": " +          \
+                                              cudaGetErrorString(e_));        \
+    } while (0)
+
+template <typename P>
+cudaError_t dalloc(P **p, size_t n)
+{
+    return cudaMalloc(reinterpret_cast<void **>(p), std::max<size_t>(n, 1) * sizeof(P));
+}
+
+void freeBuffers(alebgk_ctx *c)
+{
+    DeviceBuffers &d = c->d;
+    void *ptrs[] = {d.f[0], d.f[1], d.coef, d.pos, d.meshv, d.wall, d.boundary,
+                    d.bodyId, d.cls, d.nslot, d.slots, d.macro, d.mood, d.flag,
+                    d.list, d.mass, d.dpx, d.bodyTmp, d.bodyOut, d.stage, d.sc};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    d = DeviceBuffers();
+    for (auto &g : c->graph)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    c->uploaded = false;
+}
+
+}  // namespace
+
+extern "C" {
+
+int alebgk_create(const alebgk_config *cfg, alebgk_ctx **out)
+{
+    alebgk_ctx *c = nullptr;
+    if (!cfg || !out) return fail(nullptr, ALEBGK_EINVAL, "null argument");
+    *out = nullptr;
+    if (cfg->dim != 2 && cfg->dim != 3)
+        return fail(nullptr, ALEBGK_EINVAL, "dim must be 2 or 3");
+    if (cfg->N <= 0 || cfg->Nv < 2)
+        return fail(nullptr, ALEBGK_EINVAL, "N must be > 0 and Nv >= 2");
+    if (cfg->precision != 32 && cfg->precision != 64)
+        return fail(nullptr, ALEBGK_EINVAL, "precision must be 32 or 64");
+    if (cfg->mls_order != 1 && cfg->mls_order != 2)
+        return fail(nullptr, ALEBGK_EINVAL, "mls_order must be 1 or 2");
+    if (cfg->limiter != 0 && cfg->limiter != 2)
+        return fail(nullptr, ALEBGK_EINVAL, "limiter must be 0 (none) or 2 (MOOD)");
+    if (!(cfg->tau > 0) || !(cfg->R > 0) || !(cfg->dv > 0) || !(cfg->radius > 0))
+        return fail(nullptr, ALEBGK_EINVAL, "tau, R, dv and radius must be > 0");
+    const int gs = (cfg->dim == 3) ? cfg->Nv * cfg->Nv * cfg->Nv : 2 * cfg->Nv * cfg->Nv;
+    if ((size_t)gs * sizeof(double) > 200 * 1024)
+        return fail(nullptr, ALEBGK_EINVAL,
+                    "a particle's distribution exceeds the 200 KB per-particle "
+                    "shared-memory row of the finalize kernel");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(nullptr, ALEBGK_ECUDA, "no CUDA device available");
+    if (cfg->device < 0 || cfg->device >= ndev)
+        return fail(nullptr, ALEBGK_EINVAL, "device ordinal out of range");
+    c = new (std::nothrow) alebgk_ctx();
+    if (!c) return fail(nullptr, ALEBGK_ENOMEM, "host allocation failed");
+    c->cfg = *cfg;
+    cudaError_t e = cudaSetDevice(cfg->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess)
+    {
+        gCreateError = std::string("stream creation: ") + cudaGetErrorString(e);
+        delete c;
+        return ALEBGK_ECUDA;
+    }
+    StepParams &p = c->sp;
+    p.N = cfg->N; p.dim = cfg->dim; p.Nv = cfg->Nv;
+    p.V = (cfg->dim == 3) ? cfg->Nv * cfg->Nv * cfg->Nv : cfg->Nv * cfg->Nv;
+    p.L = (cfg->dim == 3) ? 1 : 2;
+    p.gs = p.V * p.L;
+    const int align = (cfg->precision == 64) ? 2 : 4;   // 16-byte rows
+    p.ldf = (p.gs + align - 1) / align * align;
+    p.limiter = cfg->limiter; p.tauVar = cfg->tau_variable;
+    p.mlsOrder = cfg->mls_order;
+    for (int a = 0; a < 3; ++a) { p.periodic[a] = cfg->periodic[a]; p.Lp[a] = cfg->L[a]; }
+    p.R = cfg->R; p.tau = cfg->tau; p.dHS = cfg->dHS;
+    p.vmin = cfg->vmin; p.dv = cfg->dv;
+    p.dvN = (cfg->dim == 3) ? cfg->dv * cfg->dv * cfg->dv : cfg->dv * cfg->dv;
+    p.h = cfg->radius;
+    *out = c;
+    return ALEBGK_OK;
+}
+
+int alebgk_destroy(alebgk_ctx *c)
+{
+    if (!c) return ALEBGK_OK;
+    cudaSetDevice(c->cfg.device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    freeBuffers(c);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return ALEBGK_OK;
+}
+
+int alebgk_last_error(const alebgk_ctx *c, char *buf, size_t len)
+{
+    if (!buf || len == 0) return ALEBGK_EINVAL;
+    const std::string &s = c ? c->err : gCreateError;
+    size_t n = std::min(len - 1, s.size());
+    std::memcpy(buf, s.data(), n);
+    buf[n] = '\0';
+    return ALEBGK_OK;
+}
+
+int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
+{
+    if (!c || !cl) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (!cl->xyz || !cl->meshv || !cl->wall || !cl->boundary || !cl->body_id ||
+        !cl->nnb || !cl->nbr || !cl->g || !cl->macro)
+        return fail(c, ALEBGK_EINVAL, "alebgk_upload needs every cloud member");
+    if (!(dt > 0)) return fail(c, ALEBGK_EINVAL, "dt must be > 0");
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    freeBuffers(c);
+    StepParams &p = c->sp;
+    p.dt = dt;
+    const int N = p.N;
+    for (int i = 0; i < N; ++i)
+    {
+        if (cl->nnb[i] < 0 || cl->nnb[i] > ALEBGK_MAX_NEIGH)
+            return fail(c, ALEBGK_EINVAL, "neighbour count out of range at particle " +
+                                              std::to_string(i));
+        for (int s = 0; s < cl->nnb[i]; ++s)
+        {
+            int j = cl->nbr[(size_t)i * ALEBGK_MAX_NEIGH + s];
+            if (j < 0 || j >= N || j == i)
+                return fail(c, ALEBGK_EINVAL, "neighbour index out of range at particle " +
+                                                  std::to_string(i));
+        }
+    }
+    CoeffInput in;
+    in.dim = p.dim; in.N = N; in.Nv = p.Nv; in.mlsOrder = p.mlsOrder;
+    in.dt = dt; in.h = p.h; in.vmin = p.vmin; in.dv = p.dv;
+    for (int a = 0; a < 3; ++a) { in.periodic[a] = p.periodic[a] != 0; in.L[a] = p.Lp[a]; }
+    in.xyz = cl->xyz; in.meshv = cl->meshv; in.wall = cl->wall;
+    in.boundary = cl->boundary; in.nnb = cl->nnb; in.nbr = cl->nbr;
+    in.maxNeigh = ALEBGK_MAX_NEIGH;
+    CoeffTables tb;
+    std::string err;
+    if (!buildCoefficients(in, tb, &err)) return fail(c, ALEBGK_EINVAL, err);
+    p.S = tb.S;
+    c->ncls = tb.ncls;
+    c->degenerateParticles = 0;
+    for (int k = 0; k < tb.ncls; ++k)
+        if (tb.degenerate[k]) c->degenerateParticles += tb.members[k];
+
+    const bool f64 = c->cfg.precision == 64;
+    const size_t es = f64 ? 8 : 4;
+    DeviceBuffers &d = c->d;
+    const size_t fBytes = (size_t)N * p.ldf * es;
+    CK(cudaMalloc(&d.f[0], fBytes));
+    CK(cudaMalloc(&d.f[1], fBytes));
+    CK(cudaMemsetAsync(d.f[0], 0, fBytes, c->stream));
+    CK(cudaMemsetAsync(d.f[1], 0, fBytes, c->stream));
+    const size_t ncoef = (size_t)tb.ncls * tb.S * tb.V;
+    CK(cudaMalloc(&d.coef, std::max<size_t>(ncoef, 1) * es));
+    if (f64)
+        CK(cudaMemcpy(d.coef, tb.coef.data(), ncoef * 8, cudaMemcpyHostToDevice));
+    else
+    {
+        std::vector<float> cf(ncoef);
+        for (size_t q = 0; q < ncoef; ++q) cf[q] = (float)tb.coef[q];
+        CK(cudaMemcpy(d.coef, cf.data(), ncoef * 4, cudaMemcpyHostToDevice));
+    }
+    CK(dalloc(&d.pos, 3 * (size_t)N));
+    CK(dalloc(&d.meshv, 3 * (size_t)N));
+    CK(dalloc(&d.wall, 7 * (size_t)N));
+    CK(dalloc(&d.boundary, N));
+    CK(dalloc(&d.bodyId, N));
+    CK(dalloc(&d.cls, N));
+    CK(dalloc(&d.nslot, N));
+    CK(dalloc(&d.slots, (size_t)N * tb.S));
+    CK(dalloc(&d.macro, 6 * (size_t)N));
+    CK(dalloc(&d.mood, N));
+    CK(dalloc(&d.flag, N));
+    CK(dalloc(&d.list, N));
+    CK(dalloc(&d.mass, N));
+    CK(dalloc(&d.dpx, N));
+    CK(dalloc(&d.bodyTmp, 6 * (size_t)N));
+    CK(dalloc(&d.bodyOut, 64 * 6));
+    CK(dalloc(&d.sc, 1));
+    CK(dalloc(&d.stage, (size_t)N * p.gs));
+    CK(cudaMemcpy(d.pos, cl->xyz, 24 * (size_t)N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.meshv, cl->meshv, 24 * (size_t)N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.wall, cl->wall, 56 * (size_t)N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.boundary, cl->boundary, 4 * (size_t)N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.bodyId, cl->body_id, 4 * (size_t)N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.cls, tb.cls.data(), 4 * (size_t)N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.nslot, tb.nslot.data(), 4 * (size_t)N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.slots, tb.slots.data(), 4 * (size_t)N * tb.S, cudaMemcpyHostToDevice));
+    CK(cudaMemset(d.dpx, 0, 8 * (size_t)N));
+    CK(cudaMemset(d.sc, 0, sizeof(StepScalars)));
+    CK(prepareKernels(c));
+    c->bodyIdHost.assign(cl->body_id, cl->body_id + N);
+    c->cur = 0;
+    c->uploaded = true;
+    return alebgk_upload_state(c, cl->g, cl->macro);
+}
+
+int alebgk_upload_state(alebgk_ctx *c, const double *g, const double *macro)
+{
+    if (!c || !g || !macro) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    CK(cudaSetDevice(c->cfg.device));
+    const StepParams &p = c->sp;
+    const int N = p.N;
+    std::vector<double> mac(6 * (size_t)N);
+    std::vector<int> mood(N);
+    for (int i = 0; i < N; ++i)
+    {
+        for (int q = 0; q < 6; ++q) mac[6 * (size_t)i + q] = macro[7 * (size_t)i + q];
+        mood[i] = macro[7 * (size_t)i + 6] != 0.0;
+    }
+    CK(cudaMemcpy(c->d.macro, mac.data(), mac.size() * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d.mood, mood.data(), 4 * (size_t)N, cudaMemcpyHostToDevice));
+    cudaError_t e = cudaMemcpyAsync(c->d.stage, g, (size_t)N * p.gs * 8,
+                                    cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = launchConvertIn(c, c->d.stage, c->cur);
+    if (e == cudaSuccess) e = launchMassInit(c);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess)
+        return fail(c, ALEBGK_ECUDA, std::string("state upload: ") + cudaGetErrorString(e));
+    return ALEBGK_OK;
+}
+
+int alebgk_step(alebgk_ctx *c, int nsteps)
+{
+    if (!c) return ALEBGK_EINVAL;
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    if (nsteps < 0) return fail(c, ALEBGK_EINVAL, "nsteps must be >= 0");
+    CK(cudaSetDevice(c->cfg.device));
+    for (int n = 0; n < nsteps; ++n)
+    {
+        const int from = c->cur;
+        if (!c->graph[from])
+        {
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            cudaError_t le = launchStep(c, from);
+            cudaError_t ee = cudaStreamEndCapture(c->stream, &g);
+            if (le != cudaSuccess || ee != cudaSuccess)
+            {
+                if (g) cudaGraphDestroy(g);
+                return fail(c, ALEBGK_ECUDA,
+                            std::string("step capture: ") +
+                                cudaGetErrorString(le != cudaSuccess ? le : ee));
+            }
+            cudaError_t ie = cudaGraphInstantiate(&c->graph[from], g, 0);
+            cudaGraphDestroy(g);
+            if (ie != cudaSuccess)
+                return fail(c, ALEBGK_ECUDA, std::string("graph instantiate: ") +
+                                                 cudaGetErrorString(ie));
+        }
+        CK(cudaGraphLaunch(c->graph[from], c->stream));
+        c->cur = 1 - from;
+    }
+    return ALEBGK_OK;
+}
+
+int alebgk_sync(alebgk_ctx *c)
+{
+    if (!c) return ALEBGK_EINVAL;
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->uploaded)
+    {
+        StepScalars s;
+        CK(cudaMemcpy(&s, c->d.sc, sizeof s, cudaMemcpyDeviceToHost));
+        if (s.err) return fail(c, ALEBGK_EDEVICE, "device error word " + std::to_string(s.err));
+    }
+    return ALEBGK_OK;
+}
+
+int alebgk_step_timed(alebgk_ctx *c, int nsteps, float *ms)
+{
+    if (!c || !ms) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    CK(cudaSetDevice(c->cfg.device));
+    // Capture the graphs first so that instantiation stays outside the
+    // timed region.
+    for (int from = 0; from < 2 && nsteps > 0; ++from)
+        if (!c->graph[from])
+        {
+            int r = alebgk_step(c, 1);
+            if (r) return r;
+        }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, c->stream));
+    int r = alebgk_step(c, nsteps);
+    CK(cudaEventRecord(e1, c->stream));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaEventElapsedTime(ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return r;
+}
+
+int alebgk_profile_steps(alebgk_ctx *c, int nsteps, float *ms)
+{
+    if (!c || !ms) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    CK(cudaSetDevice(c->cfg.device));
+    // launch order -> stage index of include/alebgk.h
+    static const int stageOf[ALEBGK_NSTAGES] = {7, 0, 1, 2, 3, 4, 5, 6};
+    cudaEvent_t ev[ALEBGK_NSTAGES + 1];
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    for (int q = 0; q < ALEBGK_NSTAGES; ++q) ms[q] = 0.0f;
+    int rc = ALEBGK_OK;
+    for (int n = 0; n < nsteps && rc == ALEBGK_OK; ++n)
+    {
+        cudaError_t e = launchStep(c, c->cur, ev);
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev[ALEBGK_NSTAGES]);
+        if (e != cudaSuccess)
+        {
+            rc = fail(c, ALEBGK_ECUDA, std::string("profiled step: ") + cudaGetErrorString(e));
+            break;
+        }
+        for (int q = 0; q < ALEBGK_NSTAGES; ++q)
+        {
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, ev[q], ev[q + 1]);
+            ms[stageOf[q]] += t;
+        }
+        c->cur = 1 - c->cur;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    return rc;
+}
+
+int alebgk_download_moments(alebgk_ctx *c, double *macro)
+{
+    if (!c || !macro) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    CK(cudaSetDevice(c->cfg.device));
+    const int N = c->sp.N;
+    std::vector<double> mac(6 * (size_t)N);
+    std::vector<int> mood(N);
+    CK(cudaMemcpyAsync(mac.data(), c->d.macro, mac.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(mood.data(), c->d.mood, 4 * (size_t)N, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < N; ++i)
+    {
+        for (int q = 0; q < 6; ++q) macro[7 * (size_t)i + q] = mac[6 * (size_t)i + q];
+        macro[7 * (size_t)i + 6] = mood[i];
+    }
+    return ALEBGK_OK;
+}
+
+int alebgk_download_full(alebgk_ctx *c, double *g, double *macro)
+{
+    if (!c || !g) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    CK(cudaSetDevice(c->cfg.device));
+    const StepParams &p = c->sp;
+    cudaError_t e = launchConvertOut(c, c->d.stage, c->cur);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(g, c->d.stage, (size_t)p.N * p.gs * 8, cudaMemcpyDeviceToHost,
+                            c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess)
+        return fail(c, ALEBGK_ECUDA, std::string("download: ") + cudaGetErrorString(e));
+    return macro ? alebgk_download_moments(c, macro) : ALEBGK_OK;
+}
+
+int alebgk_get_counters(alebgk_ctx *c, alebgk_counters *out)
+{
+    if (!c || !out) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    StepScalars s;
+    CK(cudaMemcpy(&s, c->d.sc, sizeof s, cudaMemcpyDeviceToHost));
+    std::memset(out, 0, sizeof *out);
+    out->steps = s.steps;
+    out->transport_flags = s.nflag;
+    out->positivity_fixes = s.nfix;
+    out->mood_fail = s.moodfail;
+    out->mls_degenerate = c->degenerateParticles;
+    out->mass_after_transport = s.massNew;
+    out->mass_scale = s.sigma;
+    out->mass_end = s.massEnd;
+    out->mass_before = (s.sigma != 0.0) ? s.sigma * s.massNew : s.massOld;
+    out->error_word = s.err;
+    return ALEBGK_OK;
+}
+
+int alebgk_total_mass(alebgk_ctx *c, double *mass)
+{
+    if (!c || !mass) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    StepScalars s;
+    CK(cudaMemcpy(&s, c->d.sc, sizeof s, cudaMemcpyDeviceToHost));
+    *mass = s.massOld;
+    return ALEBGK_OK;
+}
+
+int alebgk_wall_momentum(alebgk_ctx *c, double *dpx)
+{
+    if (!c || !dpx) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaMemcpyAsync(dpx, c->d.dpx, 8 * (size_t)c->sp.N, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return ALEBGK_OK;
+}
+
+int alebgk_device_state(alebgk_ctx *c, void **f, int *ldf, int *elem_bytes)
+{
+    if (!c) return ALEBGK_EINVAL;
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    if (f) *f = c->d.f[c->cur];
+    if (ldf) *ldf = c->sp.ldf;
+    if (elem_bytes) *elem_bytes = c->cfg.precision == 64 ? 8 : 4;
+    return ALEBGK_OK;
+}
+
+int alebgk_body_loads(alebgk_ctx *c, int nbodies, const double *centre,
+                      const double *area, double *out)
+{
+    if (!c || !centre || !area || !out) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (nbodies <= 0 || nbodies > 64) return fail(c, ALEBGK_EINVAL, "1..64 bodies");
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    for (int i = 0; i < c->sp.N; ++i)
+        if (c->bodyIdHost[i] >= nbodies)
+            return fail(c, ALEBGK_EINVAL, "a particle's body id exceeds nbodies");
+    CK(cudaSetDevice(c->cfg.device));
+    double *dc = nullptr;
+    CK(cudaMalloc(&dc, 4 * 64 * sizeof(double)));
+    cudaError_t e = cudaMemcpyAsync(dc, centre, 24 * (size_t)nbodies, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dc + 3 * 64, area, 8 * (size_t)nbodies, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = launchBodyLoads(c, nbodies, dc, dc + 3 * 64);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, c->d.bodyOut, 48 * (size_t)nbodies, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(dc);
+    if (e != cudaSuccess)
+        return fail(c, ALEBGK_ECUDA, std::string("body loads: ") + cudaGetErrorString(e));
+    return ALEBGK_OK;
+}
+
+int alebgk_body_set_surface_velocity(alebgk_ctx *c, int nbodies,
+                                     const double *centre, const double *state)
+{
+    if (!c || !centre || !state) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (nbodies <= 0 || nbodies > 64) return fail(c, ALEBGK_EINVAL, "1..64 bodies");
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    for (int i = 0; i < c->sp.N; ++i)
+        if (c->bodyIdHost[i] >= nbodies)
+            return fail(c, ALEBGK_EINVAL, "a particle's body id exceeds nbodies");
+    CK(cudaSetDevice(c->cfg.device));
+    double *dc = nullptr;
+    CK(cudaMalloc(&dc, 9 * 64 * sizeof(double)));
+    cudaError_t e = cudaMemcpyAsync(dc, centre, 24 * (size_t)nbodies, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dc + 3 * 64, state, 48 * (size_t)nbodies, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = launchSetSurfaceVelocity(c, nbodies, dc, dc + 3 * 64);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(dc);
+    if (e != cudaSuccess)
+        return fail(c, ALEBGK_ECUDA, std::string("surface velocity: ") + cudaGetErrorString(e));
+    return ALEBGK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Host-side coefficient tables
+// ---------------------------------------------------------------------------
+struct alebgk_coeffs
+{
+    CoeffTables t;
+    int N = 0;
+    int degenerateParticles = 0;
+};
+
+int alebgk_coeff_build(const alebgk_config *cfg, const alebgk_cloud *cl, double dt,
+                       alebgk_coeffs **out)
+{
+    if (!cfg || !cl || !out || !cl->xyz || !cl->meshv || !cl->wall || !cl->boundary ||
+        !cl->nnb || !cl->nbr)
+        return fail(nullptr, ALEBGK_EINVAL, "null argument");
+    *out = nullptr;
+    CoeffInput in;
+    in.dim = cfg->dim; in.N = cfg->N; in.Nv = cfg->Nv; in.mlsOrder = cfg->mls_order;
+    in.dt = dt; in.h = cfg->radius; in.vmin = cfg->vmin; in.dv = cfg->dv;
+    for (int a = 0; a < 3; ++a) { in.periodic[a] = cfg->periodic[a] != 0; in.L[a] = cfg->L[a]; }
+    in.xyz = cl->xyz; in.meshv = cl->meshv; in.wall = cl->wall;
+    in.boundary = cl->boundary; in.nnb = cl->nnb; in.nbr = cl->nbr;
+    in.maxNeigh = ALEBGK_MAX_NEIGH;
+    auto *t = new (std::nothrow) alebgk_coeffs();
+    if (!t) return fail(nullptr, ALEBGK_ENOMEM, "host allocation failed");
+    std::string err;
+    if (!buildCoefficients(in, t->t, &err))
+    {
+        delete t;
+        return fail(nullptr, ALEBGK_EINVAL, err);
+    }
+    t->N = cfg->N;
+    for (int k = 0; k < t->t.ncls; ++k)
+        if (t->t.degenerate[k]) t->degenerateParticles += t->t.members[k];
+    *out = t;
+    return ALEBGK_OK;
+}
+
+int alebgk_coeff_info(const alebgk_coeffs *t, int *info)
+{
+    if (!t || !info) return ALEBGK_EINVAL;
+    info[0] = t->t.ncls; info[1] = t->t.S; info[2] = t->t.V;
+    info[3] = t->degenerateParticles; info[4] = t->N;
+    return ALEBGK_OK;
+}
+
+int alebgk_coeff_get(const alebgk_coeffs *t, int *cls, int *nslot, int *slots,
+                     double *coef)
+{
+    if (!t) return ALEBGK_EINVAL;
+    if (cls) std::memcpy(cls, t->t.cls.data(), t->t.cls.size() * sizeof(int));
+    if (nslot) std::memcpy(nslot, t->t.nslot.data(), t->t.nslot.size() * sizeof(int));
+    if (slots) std::memcpy(slots, t->t.slots.data(), t->t.slots.size() * sizeof(int));
+    if (coef) std::memcpy(coef, t->t.coef.data(), t->t.coef.size() * sizeof(double));
+    return ALEBGK_OK;
+}
+
+void alebgk_coeff_free(alebgk_coeffs *t) { delete t; }
+
+// ---------------------------------------------------------------------------
+// Host case set-up
+// ---------------------------------------------------------------------------
+struct alebgk_case
+{
+    Cloud cloud;
+};
+
+int alebgk_case_build(const char *name, int Nx, int Nv, double dt, int mls_order,
+                      int fixed_body, double body_scale, alebgk_case **out)
+{
+    if (!name || !out) return fail(nullptr, ALEBGK_EINVAL, "null argument");
+    *out = nullptr;
+    int id = 0;
+    if (!caseByName(name, &id)) return fail(nullptr, ALEBGK_EINVAL, std::string("unknown case ") + name);
+    CaseParams prm;
+    if (!configureCase(id, Nx, Nv, dt, mls_order, fixed_body != 0, prm))
+        return fail(nullptr, ALEBGK_EINVAL, "configureCase failed");
+    auto *c = new (std::nothrow) alebgk_case();
+    if (!c) return fail(nullptr, ALEBGK_ENOMEM, "host allocation failed");
+    std::string err;
+    if (!buildCloud(prm, body_scale, c->cloud, &err))
+    {
+        delete c;
+        return fail(nullptr, ALEBGK_EINVAL, err);
+    }
+    *out = c;
+    return ALEBGK_OK;
+}
+
+void alebgk_case_free(alebgk_case *c) { delete c; }
+
+int alebgk_case_info(const alebgk_case *cs, int *info, double *prm)
+{
+    if (!cs) return ALEBGK_EINVAL;
+    const Cloud &c = cs->cloud;
+    const CaseParams &p = c.prm;
+    if (info)
+    {
+        info[0] = c.N; info[1] = p.dim; info[2] = p.Nv; info[3] = c.gStride;
+        info[4] = (int)c.bodies.size(); info[5] = p.mlsOrder; info[6] = p.Nx;
+        info[7] = p.movingBodies ? 1 : 0;
+    }
+    if (prm)
+    {
+        double v[24] = {p.dt, p.tau, p.R, p.dx, p.dy, p.dz, p.radius, p.minDist,
+                        p.dv, p.VMin, p.VMax, p.rho0, p.Tw, p.xleft, p.xright,
+                        p.ybottom, p.ytop, p.zfront, p.zback, p.dtRequested,
+                        p.tfinal, p.dHS, p.lidSpeed, (double)p.saveEvery};
+        std::memcpy(prm, v, sizeof v);
+    }
+    return ALEBGK_OK;
+}
+
+int alebgk_case_view(alebgk_case *cs, alebgk_cloud *v)
+{
+    if (!cs || !v) return ALEBGK_EINVAL;
+    Cloud &c = cs->cloud;
+    c.xyz.resize(3 * (size_t)c.N);
+    for (int i = 0; i < c.N; ++i)
+    {
+        c.xyz[3 * (size_t)i] = c.x[i];
+        c.xyz[3 * (size_t)i + 1] = c.y[i];
+        c.xyz[3 * (size_t)i + 2] = c.z[i];
+    }
+    v->xyz = c.xyz.data();
+    v->meshv = c.meshv.data();
+    v->wall = c.wall.data();
+    v->boundary = c.boundary.data();
+    v->body_id = c.bodyId.data();
+    v->nnb = c.nnb.data();
+    v->nbr = c.nbr.data();
+    v->g = c.g.data();
+    v->macro = c.macro.data();
+    return ALEBGK_OK;
+}
+
+int alebgk_case_bodies(const alebgk_case *cs, double *out)
+{
+    if (!cs || !out) return ALEBGK_EINVAL;
+    const Cloud &c = cs->cloud;
+    for (size_t b = 0; b < c.bodies.size(); ++b)
+    {
+        const Body &r = c.bodies[b];
+        double *o = out + 32 * b;
+        double v[22] = {r.cx, r.cy, r.cz, r.velx, r.vely, r.velz, r.angularVel,
+                        r.omx, r.omy, r.omz, r.forcex, r.forcey, r.forcez,
+                        r.torque, r.tqx, r.tqy, r.tqz, r.ox, r.oy, r.mass,
+                        r.inertia(), r.T};
+        std::memcpy(o, v, sizeof v);
+        for (int k = 0; k < 9; ++k) o[22 + k] = r.Rm[k];
+        o[31] = r.surfaceArea();
+    }
+    return ALEBGK_OK;
+}
+
+int alebgk_case_config(const alebgk_case *cs, int precision, int device,
+                       alebgk_config *cfg)
+{
+    if (!cs || !cfg) return ALEBGK_EINVAL;
+    const Cloud &c = cs->cloud;
+    const CaseParams &p = c.prm;
+    std::memset(cfg, 0, sizeof *cfg);
+    cfg->dim = p.dim; cfg->N = c.N; cfg->Nv = p.Nv; cfg->mls_order = p.mlsOrder;
+    cfg->precision = precision; cfg->limiter = 2; cfg->tau_variable = 0;
+    cfg->device = device; cfg->R = p.R; cfg->tau = p.tau; cfg->dHS = p.dHS;
+    cfg->vmin = p.VMin; cfg->dv = p.dv; cfg->radius = p.radius;
+    return ALEBGK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,59 @@
+// coeffs.h -- FP64 MLS stencil classes and transport coefficients (internal).
+//
+// The MLS transport of MLSTransport/MLSTransport.cpp:88-311 solves, for every
+// particle i and velocity node k, the weighted normal equations A(i,k) sol =
+// sum_j w_j b_j f_j[k] and keeps gt = sol[0].  The matrix, the weights and
+// the basis depend only on the geometry (neighbour offsets, foot point
+// x_i - (v_k - meshV_i) dt, support h), never on f; partial-pivot Gaussian
+// elimination with the reference's skip rule is a linear map of the
+// right-hand side once the pivots are chosen from A.  Hence
+//     gt[i][k] = sum_s c[class(i)][k][s] * f[nbr(i,s)][k]
+// with coefficients computed once in FP64.  Particles whose neighbour
+// offsets, wall state, mesh velocity and MLS order coincide share a class.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace alebgk {
+
+struct CoeffInput
+{
+    int dim = 3, N = 0, Nv = 0, mlsOrder = 2;
+    double dt = 0, h = 0, vmin = 0, dv = 0;
+    bool periodic[3] = {false, false, false};
+    double L[3] = {0, 0, 0};
+    const double *xyz = nullptr;    // N*3
+    const double *meshv = nullptr;  // N*3
+    const double *wall = nullptr;   // N*7
+    const int *boundary = nullptr;  // N
+    const int *nnb = nullptr;       // N
+    const int *nbr = nullptr;       // N*maxNeigh
+    int maxNeigh = 128;
+};
+
+struct CoeffTables
+{
+    int S = 0;                      // slot stride: 1 (self) + max neighbours
+    int V = 0;                      // velocity nodes per layer
+    int ncls = 0;
+    std::vector<int> cls;           // N: class of each particle
+    std::vector<int> nslot;         // N: 1 + neighbour count
+    std::vector<int> slots;         // N*S: slot 0 = self, then canonical order
+    std::vector<int> rep;           // ncls: representative particle
+    std::vector<double> coef;       // ncls*S*V, layout [class][slot][node]
+    std::vector<int> degenerate;    // ncls: nodes with a skipped pivot
+    std::vector<int> order;         // ncls: MLS order used
+    std::vector<int> members;       // ncls: particles in the class
+};
+
+// Builds classes and coefficients.  Returns false with *err on bad input.
+bool buildCoefficients(const CoeffInput &in, CoeffTables &out, std::string *err);
+
+// Partial-pivot Gaussian elimination with the reference's |pivot| < 1e-30
+// skip rule (MLSTransport/MLSTransport.cpp:20-62), applied to nrhs
+// right-hand sides at once: A is n x n row-major, B is n x nrhs row-major and
+// is overwritten with the solutions.  Returns the number of skipped pivots.
+int solveSkipGE(double *A, double *B, int n, int nrhs);
+
+}  // namespace alebgk

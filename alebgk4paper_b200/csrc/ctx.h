@@ -1,0 +1,86 @@
+// ctx.h -- device context of the ALE-BGK step (internal header).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/alebgk.h"
+
+namespace alebgk {
+
+// Per-step scalars kept on the device so that a step needs no host
+// synchronisation (the reference reads three masses back per step,
+// Solver/CudaBackend.cu:1384-1395).
+struct StepScalars
+{
+    double massOld;        // sumMass at the start of the step
+    double massNew;        // sumMass after transport + positivity + redo
+    double sigma;          // massOld / massNew
+    double massEnd;        // sumMass at the end of the step
+    int nflag;             // transport MOOD flags (length of the redo list)
+    int nfix;              // positivity repairs
+    int moodfail;          // post-collision moodCheck failed
+    int err;               // device error bits
+    long long steps;
+};
+
+struct DeviceBuffers
+{
+    void *f[2] = {nullptr, nullptr};   // ping-pong distribution, N x ldf
+    void *coef = nullptr;              // [class][slot][node]
+    double *pos = nullptr, *meshv = nullptr, *wall = nullptr;
+    int *boundary = nullptr, *bodyId = nullptr;
+    int *cls = nullptr, *nslot = nullptr, *slots = nullptr;
+    double *macro = nullptr;           // N x 6: rho ux uy uz T p
+    int *mood = nullptr, *flag = nullptr, *list = nullptr;
+    double *mass = nullptr, *dpx = nullptr;
+    double *bodyTmp = nullptr;         // N x 6 per-particle load contributions
+    double *bodyOut = nullptr;         // up to 64 bodies x 6
+    double *stage = nullptr;           // N x gs FP64 host-transfer staging
+    StepScalars *sc = nullptr;
+};
+
+struct StepParams
+{
+    int N = 0, dim = 3, Nv = 0, V = 0, L = 1, gs = 0, ldf = 0, S = 0;
+    int limiter = 2, tauVar = 0, mlsOrder = 2;
+    int periodic[3] = {0, 0, 0};
+    double Lp[3] = {0, 0, 0};
+    double R = 208, tau = 1, dHS = 0, vmin = 0, dv = 0, dvN = 0, h = 0, dt = 0;
+};
+
+}  // namespace alebgk
+
+struct alebgk_ctx
+{
+    alebgk_config cfg{};
+    alebgk::StepParams sp;
+    alebgk::DeviceBuffers d;
+    cudaStream_t stream = nullptr;
+    int cur = 0;                 // buffer holding the current g
+    bool uploaded = false;
+    int ncls = 0;
+    int degenerateParticles = 0;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    std::string err;
+    // host staging
+    std::vector<int> bodyIdHost;
+};
+
+namespace alebgk {
+
+// Launch wrappers (step.cu).
+cudaError_t prepareKernels(alebgk_ctx *c);
+cudaError_t launchStep(alebgk_ctx *c, int from, cudaEvent_t *ev = nullptr);
+cudaError_t launchMassInit(alebgk_ctx *c);
+cudaError_t launchBodyLoads(alebgk_ctx *c, int nbodies, const double *centreDev,
+                            const double *areaDev);
+cudaError_t launchSetSurfaceVelocity(alebgk_ctx *c, int nbodies,
+                                     const double *centreDev,
+                                     const double *stateDev);
+cudaError_t launchConvertIn(alebgk_ctx *c, const double *src, int buf);
+cudaError_t launchConvertOut(alebgk_ctx *c, double *dst, int buf);
+
+}  // namespace alebgk

@@ -1,0 +1,255 @@
+/*
+ * alebgk.h -- C-ABI of the B200-native ALE-BGK time step.
+ *
+ * This is the drop-in boundary for the solver-step interface of
+ * panchiittp/ALEBGK4Paper.  The reference's time loop (Solver/Solver.cpp:
+ * 253-578) drives its GPU backend through the C++ functions declared at
+ * Solver/Solver.cpp:67-89 and defined in Solver/CudaBackend.cu:1199-2082; they
+ * take std::vector<Particle> (Core/Types.hpp:213-261).  Each entry point below
+ * replaces one of them with plain pointers, sizes and an int status, so that
+ * a C, C++, Python (ctypes) or any other FFI caller can bind it; the
+ * reference-side C++ shim that maps the original symbols onto these calls is
+ * given in INTEGRATION.md.
+ *
+ * Conventions
+ *   - Every call returns ALEBGK_OK (0) or a negative ALEBGK_E* code; the
+ *     library never calls exit().  alebgk_last_error() returns the message.
+ *   - A context owns one device, one non-default CUDA stream and its device
+ *     buffers.  Calls on one context are not thread-safe; distinct contexts
+ *     are independent.  Work is enqueued on the context's stream; the
+ *     download_* calls synchronise that stream.
+ *   - Host arrays are plain, densely packed, row-major FP64/int32 arrays in
+ *     the reference's per-particle order.
+ */
+#ifndef ALEBGK_H
+#define ALEBGK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ALEBGK_OK 0
+#define ALEBGK_EINVAL (-1)   /* bad argument or configuration            */
+#define ALEBGK_ECUDA (-2)    /* a CUDA runtime call failed                */
+#define ALEBGK_ESTATE (-3)   /* call out of order (e.g. step before upload) */
+#define ALEBGK_ENOMEM (-4)   /* host or device allocation failed          */
+#define ALEBGK_EDEVICE (-5)  /* a device-side check failed (error word)   */
+
+#define ALEBGK_MAX_NEIGH 128 /* Core/Types.hpp:22 (MAX_NEIGH)             */
+
+typedef struct alebgk_ctx alebgk_ctx;
+typedef struct alebgk_case alebgk_case;
+
+/* Solver configuration: the subset of SimParameters / CalcParameters /
+ * GasConstants (Core/Types.hpp:110-208) that the step reads. */
+typedef struct alebgk_config
+{
+    int dim;          /* 2 (Chu-reduced g1/g2) or 3                          */
+    int N;            /* particles                                           */
+    int Nv;           /* velocity points per axis (uniform Fixed grid)       */
+    int mls_order;    /* 1 linear or 2 quadratic MLS for interior particles   */
+    int precision;    /* 32: FP32 f storage + FP32 reconstruction; 64: all FP64 */
+    int limiter;      /* 0 none, 2 MOOD (Core/Types.hpp:56-61)                */
+    int tau_variable; /* hard-sphere tau(rho,T) (MomentCalculations/Collision.cpp:87-96) */
+    int device;       /* CUDA device ordinal                                  */
+    double R;         /* gas constant, 208 for argon                          */
+    double tau;       /* BGK relaxation time                                  */
+    double dHS;       /* hard-sphere diameter (tau_variable only)             */
+    double vmin;      /* velocity grid lower end (VMin)                       */
+    double dv;        /* velocity grid spacing                                */
+    double radius;    /* MLS support h (CalcParameters::radius)               */
+    int periodic[3];  /* per-axis periodicity (minimum-image stencils)        */
+    double L[3];      /* periodic lengths                                     */
+} alebgk_config;
+
+/* The host cloud in SoA form.  Inputs for alebgk_upload; the download calls
+ * fill the non-NULL members of the same struct. */
+typedef struct alebgk_cloud
+{
+    double *xyz;      /* N*3 positions                                        */
+    double *meshv;    /* N*3 mesh velocity (meshVx/y/z)                       */
+    double *wall;     /* N*7 stored wall state: wnx wny wnz wUx wUy wUz wT    */
+    int *boundary;    /* N   wall-particle flag                               */
+    int *body_id;     /* N   -1 box wall / fluid, >=0 body surface            */
+    int *nnb;         /* N   neighbour count (<= ALEBGK_MAX_NEIGH)            */
+    int *nbr;         /* N*ALEBGK_MAX_NEIGH neighbour indices                 */
+    double *g;        /* N*gstride distribution (Nv^3, or g1[Nv^2] g2[Nv^2])  */
+    double *macro;    /* N*7: rho ux uy uz T p moodFlag                       */
+} alebgk_cloud;
+
+/* Counters after the last completed step (cudaLimiterCounts,
+ * cudaMlsCounts, cudaMassBudget, cudaTotalMass:
+ * Solver/CudaBackend.cu:1986-2030). */
+typedef struct alebgk_counters
+{
+    int64_t steps;            /* steps run since upload                       */
+    int transport_flags;      /* particles flagged by the transport MOOD screen */
+    int positivity_fixes;     /* particles whose positivity repair fired      */
+    int mood_fail;            /* 1 if the post-collision moodCheck failed     */
+    int mls_degenerate;       /* particles with a skipped (|pivot|<1e-30) MLS pivot */
+    double mass_before;       /* sumMass at the start of the step             */
+    double mass_after_transport; /* sumMass after transport (before rescale) */
+    double mass_scale;        /* global rescale factor applied               */
+    double mass_end;          /* sumMass at the end of the step               */
+    int error_word;           /* device-side error bits (0 = none)            */
+} alebgk_counters;
+
+/* ---- context --------------------------------------------------------- */
+
+/* Creates a context (no reference counterpart: the reference keeps one
+ * static DeviceCloud, Solver/CudaBackend.cu:69-115). */
+int alebgk_create(const alebgk_config *cfg, alebgk_ctx **out);
+
+/* Frees every device buffer and the context.
+ * Replaces cudaFreeCloud (Solver/CudaBackend.cu:1203-1221). */
+int alebgk_destroy(alebgk_ctx *ctx);
+
+/* Message of the last failed call on this context (or the last failed
+ * alebgk_create if ctx is NULL).  Copies at most len-1 bytes. */
+int alebgk_last_error(const alebgk_ctx *ctx, char *buf, size_t len);
+
+/* ---- state transfer -------------------------------------------------- */
+
+/* Copies the full host cloud to the device and (re)builds the MLS stencil
+ * classes and coefficient tables for the given dt.
+ * Replaces cudaUploadCloud (Solver/Solver.cpp:68,
+ * Solver/CudaBackend.cu:1223-1381); dt is the step the tables are built for
+ * (the reference passes it to every cudaStep instead). */
+int alebgk_upload(alebgk_ctx *ctx, const alebgk_cloud *cloud, double dt);
+
+/* Replaces only the distribution and macro fields (same geometry), e.g. a
+ * checkpoint restore.  No reference counterpart (cudaUploadCloud's
+ * layout-reuse path, Solver/CudaBackend.cu:1262-1263, covers it). */
+int alebgk_upload_state(alebgk_ctx *ctx, const double *g, const double *macro);
+
+/* Moments rho, u, T, p and moodFlag into macro (N*7).
+ * Replaces cudaDownloadMoments (Solver/Solver.cpp:71,
+ * Solver/CudaBackend.cu:1917-1972); p = rho*R*T as the CPU path computes it
+ * (MomentCalculations/Moments.cpp:94). */
+int alebgk_download_moments(alebgk_ctx *ctx, double *macro);
+
+/* Moments plus the full distribution g (N*gstride, FP64).
+ * Replaces cudaDownloadFull (Solver/Solver.cpp:72,
+ * Solver/CudaBackend.cu:2056-2082). */
+int alebgk_download_full(alebgk_ctx *ctx, double *g, double *macro);
+
+/* ---- the step ---------------------------------------------------------- */
+
+/* Enqueues nsteps full time steps with the dt given to alebgk_upload:
+ * transport, positivity + MOOD screen with linear redo, commit, global mass
+ * rescale, diffuse wall, moments, implicit BGK collision, moments, moodCheck
+ * (Solver/Solver.cpp:632-705).  No host synchronisation inside.
+ * Replaces cudaStep (Solver/Solver.cpp:69-70,
+ * Solver/CudaBackend.cu:1505-1870). */
+int alebgk_step(alebgk_ctx *ctx, int nsteps);
+
+/* Blocks until all work on the context's stream has finished and returns
+ * ALEBGK_EDEVICE if a device-side check set the error word. */
+int alebgk_sync(alebgk_ctx *ctx);
+
+/* Runs nsteps steps bracketed by CUDA events recorded on the context's own
+ * stream, synchronises, and returns the device time in *ms.  Replaces the
+ * reference's event-timed steady window ALEBGK_PROFILE_FROM/LEN
+ * (Solver/CudaBackend.cu:1518-1623). */
+int alebgk_step_timed(alebgk_ctx *ctx, int nsteps, float *ms);
+
+/* Runs nsteps steps kernel by kernel (no graph) with a CUDA event between
+ * every launch, and returns the summed device time of each stage in
+ * ms_per_stage[0..ALEBGK_NSTAGES-1] (transport, post_transport, redo,
+ * mass_after_transport, finalize, recollide, mass_end, step_begin).
+ * Replaces the one-shot [GPU-PROFILE] table of
+ * Solver/CudaBackend.cu:1518-1623. */
+#define ALEBGK_NSTAGES 8
+int alebgk_profile_steps(alebgk_ctx *ctx, int nsteps, float *ms_per_stage);
+
+/* ---- diagnostics ------------------------------------------------------- */
+
+/* Replaces cudaLimiterCounts, cudaMlsCounts, cudaMassBudget
+ * (Solver/CudaBackend.cu:1986-2030). */
+int alebgk_get_counters(alebgk_ctx *ctx, alebgk_counters *out);
+
+/* Total gas mass sum(g dv^d) on the device.
+ * Replaces cudaTotalMass (Solver/CudaBackend.cu:2018-2024). */
+int alebgk_total_mass(alebgk_ctx *ctx, double *mass);
+
+/* Per-particle x-momentum change applied by the last wall BC (N values,
+ * zero for interior particles).
+ * Replaces cudaWallMomentum (Solver/CudaBackend.cu:1977-1983). */
+int alebgk_wall_momentum(alebgk_ctx *ctx, double *dpx);
+
+/* Device pointers of the current distribution (row stride ldf elements,
+ * FP32 or FP64 per cfg.precision) for callers that keep data on the GPU.
+ * No reference counterpart. */
+int alebgk_device_state(alebgk_ctx *ctx, void **f, int *ldf, int *elem_bytes);
+
+/* ---- rigid bodies ------------------------------------------------------ */
+
+/* Surface-stress force and torque on each body from the current device g,
+ * relative to each surface particle's stored wall velocity:
+ * P_ab = sum f c_a c_b dv^3, t = -n.P, F += area t, T += area r x t.
+ * Restates computeBodyLoads (RigidBody/BodyDynamics.cpp:17-97).
+ * body_centre: nbodies*3; body_area: nbodies; out: nbodies*6 (F, T). */
+int alebgk_body_loads(alebgk_ctx *ctx, int nbodies, const double *body_centre,
+                      const double *body_area, double *out);
+
+/* Writes the surface wall velocity V + w x r of trial body states onto the
+ * surface particles on the device (RigidBody/BodyDynamics.cpp:103-125).
+ * state: nbodies*6 (V, w); body_centre: nbodies*3. */
+int alebgk_body_set_surface_velocity(alebgk_ctx *ctx, int nbodies,
+                                     const double *body_centre,
+                                     const double *state);
+
+/* ---- host-side MLS coefficient tables (no device work) -------------------
+ * The stencil classes and FP64 transport coefficients that alebgk_upload
+ * builds: gt[i][k] = sum_s coef[cls[i]][s][k] * g[slots[i][s]][k], slot 0 =
+ * the particle itself (coefficient 1 where the reference keeps the old value:
+ * outgoing wall nodes, MLSTransport/MLSTransport.cpp:144-150, and nodes
+ * without a weighted neighbour, :182).  No reference counterpart: the
+ * reference re-solves the normal equations for every node of every step
+ * (MLSTransport/MLSTransport.cpp:129-186). */
+typedef struct alebgk_coeffs alebgk_coeffs;
+int alebgk_coeff_build(const alebgk_config *cfg, const alebgk_cloud *cloud,
+                       double dt, alebgk_coeffs **out);
+/* info[0..4] = ncls, S (slot stride), V (nodes per layer),
+ *              particles with a skipped pivot, N */
+int alebgk_coeff_info(const alebgk_coeffs *t, int *info);
+/* cls: N, nslot: N, slots: N*S, coef: ncls*S*V (any may be NULL) */
+int alebgk_coeff_get(const alebgk_coeffs *t, int *cls, int *nslot, int *slots,
+                     double *coef);
+void alebgk_coeff_free(alebgk_coeffs *t);
+
+/* ---- host-side case set-up (no device work) -----------------------------
+ * Builds one of the reference's six cases (TestCases/TestCases.cpp:56-294,
+ * Initialization/*.cpp, TestCases/main.cpp:193-345) on the host.  Nx, Nv,
+ * dt <= 0 keep the case defaults; mls_order 1 or 2; fixed_body = --fixed. */
+int alebgk_case_build(const char *name, int Nx, int Nv, double dt,
+                      int mls_order, int fixed_body, double body_scale,
+                      alebgk_case **out);
+void alebgk_case_free(alebgk_case *c);
+
+/* info[0..7]  = N, dim, Nv, gstride, nbodies, mls_order, Nx, moving_bodies
+ * prm[0..23]  = dt, tau, R, dx, dy, dz, radius, minDist, dv, vmin, vmax,
+ *               rho0, Tw, xleft, xright, ybottom, ytop, zfront, zback,
+ *               dt_requested, tfinal, dHS, lid_speed, save_every */
+int alebgk_case_info(const alebgk_case *c, int *info, double *prm);
+
+/* Fills a cloud view whose members point into the case's own host arrays
+ * (valid until alebgk_case_free). */
+int alebgk_case_view(alebgk_case *c, alebgk_cloud *view);
+
+/* Body state: per body 32 doubles: cx cy cz velx vely velz angularVel omx omy
+ * omz forcex forcey forcez torque tqx tqy tqz ox oy mass I T Rm[9] area. */
+int alebgk_case_bodies(const alebgk_case *c, double *out);
+
+/* Fills a solver configuration from a case (precision 32 or 64). */
+int alebgk_case_config(const alebgk_case *c, int precision, int device,
+                       alebgk_config *cfg);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ALEBGK_H */
