@@ -3,7 +3,11 @@
 // Each function restates one piece of the reference's set-up so that the
 // cloud built here is the cloud the reference builds for the same case:
 // same particle order, positions, wall flags, wall state, neighbour sets and
-// initial distribution.
+// initial distribution.  The reference is built with -march=native, and GCC
+// contracts a*b + c into one rounding (an FMA) on any FMA-capable x86-64;
+// the expressions below spell those contractions out with std::fma so that
+// positions, voxel bins (floor at exact multiples of the box size) and hence
+// neighbour order come out bitwise identical to the reference's build.
 #include "cases.h"
 
 #include <algorithm>
@@ -48,8 +52,8 @@ double maxwellian3(double vx, double vy, double vz, double ux, double uy,
                    double uz, double T, double rho, double R)
 {
     double twoRT = 2.0 * R * T;
-    double e = -((vx - ux) * (vx - ux) + (vy - uy) * (vy - uy) +
-                 (vz - uz) * (vz - uz)) / twoRT;
+    double ax = vx - ux, ay = vy - uy, az = vz - uz;
+    double e = -std::fma(az, az, std::fma(ax, ax, ay * ay)) / twoRT;
     double norm = std::pow(kPi * twoRT, 1.5);
     return rho / norm * std::exp(e);
 }
@@ -59,7 +63,8 @@ double maxwellianG1(double vx, double vy, double ux, double uy, double T,
                     double rho, double R)
 {
     double twoRT = 2.0 * R * T;
-    double e = -((vx - ux) * (vx - ux) + (vy - uy) * (vy - uy)) / twoRT;
+    double ax = vx - ux, ay = vy - uy;
+    double e = -std::fma(ax, ax, ay * ay) / twoRT;
     return rho / (kPi * twoRT) * std::exp(e);
 }
 
@@ -105,19 +110,19 @@ bool Body::inside(double x, double y, double z) const
     case 1:
     {   // Geometry.hpp:233-237
         double dx = x - cx, dy = y - cy;
-        return dx * dx + dy * dy <= size * size;
+        return std::fma(dx, dx, dy * dy) <= size * size;
     }
     case 2:
     {   // Geometry.hpp:105-109
         double dx = x - cx, dy = y - cy, dz = z - cz;
-        return dx * dx + dy * dy + dz * dz <= size * size;
+        return std::fma(dz, dz, std::fma(dx, dx, dy * dy)) <= size * size;
     }
     default:
     {   // Geometry.hpp:275-293 (R^T applied to the offset)
         double dx = x - cx, dy = y - cy, dz = z - cz;
-        double bx = Rm[0] * dx + Rm[3] * dy + Rm[6] * dz;
-        double by = Rm[1] * dx + Rm[4] * dy + Rm[7] * dz;
-        double bz = Rm[2] * dx + Rm[5] * dy + Rm[8] * dz;
+        double bx = std::fma(Rm[6], dz, std::fma(Rm[0], dx, Rm[3] * dy));
+        double by = std::fma(Rm[7], dz, std::fma(Rm[1], dx, Rm[4] * dy));
+        double bz = std::fma(Rm[8], dz, std::fma(Rm[2], dx, Rm[5] * dy));
         return std::fabs(bx) <= size / 2 && std::fabs(by) <= size / 2 &&
                std::fabs(bz) <= size / 2;
     }
@@ -132,12 +137,13 @@ void Body::normal(double x, double y, double z, double *nx, double *ny,
     case 0:
     {   // Geometry.hpp:161-177: side whose outward normal is closest
         double xp = x - cx, yp = y - cy;
-        double n = std::sqrt(xp * xp + yp * yp);
+        double n = std::sqrt(std::fma(xp, xp, yp * yp));
+        double d1 = std::fma(xp, ox, yp * oy), d2 = std::fma(xp, oy, -(yp * ox));
         double dots[4][3] = {
-            {(xp * ox + yp * oy) / n, ox, oy},
-            {-(xp * ox + yp * oy) / n, -ox, -oy},
-            {(xp * oy - yp * ox) / n, oy, -ox},
-            {-(xp * oy - yp * ox) / n, -oy, ox},
+            {d1 / n, ox, oy},
+            {-d1 / n, -ox, -oy},
+            {d2 / n, oy, -ox},
+            {-d2 / n, -oy, ox},
         };
         int best = 0;
         for (int i = 1; i < 4; ++i)
@@ -148,23 +154,23 @@ void Body::normal(double x, double y, double z, double *nx, double *ny,
     case 1:
     {   // Geometry.hpp:225-231
         double dx = x - cx, dy = y - cy;
-        double n = std::sqrt(dx * dx + dy * dy);
+        double n = std::sqrt(std::fma(dx, dx, dy * dy));
         *nx = dx / n; *ny = dy / n; *nz = 0.0;
         return;
     }
     case 2:
     {   // Geometry.hpp:117-123
         double dx = x - cx, dy = y - cy, dz = z - cz;
-        double n = std::sqrt(dx * dx + dy * dy + dz * dz);
+        double n = std::sqrt(std::fma(dz, dz, std::fma(dx, dx, dy * dy)));
         *nx = dx / n; *ny = dy / n; *nz = dz / n;
         return;
     }
     default:
     {   // Geometry.hpp:298-309: dominant body-frame axis, column of Rm
         double dx = x - cx, dy = y - cy, dz = z - cz;
-        double b[3] = {Rm[0] * dx + Rm[3] * dy + Rm[6] * dz,
-                       Rm[1] * dx + Rm[4] * dy + Rm[7] * dz,
-                       Rm[2] * dx + Rm[5] * dy + Rm[8] * dz};
+        double b[3] = {std::fma(Rm[6], dz, std::fma(Rm[0], dx, Rm[3] * dy)),
+                       std::fma(Rm[7], dz, std::fma(Rm[1], dx, Rm[4] * dy)),
+                       std::fma(Rm[8], dz, std::fma(Rm[2], dx, Rm[5] * dy))};
         int f = 0;
         for (int i = 1; i < 3; ++i)
             if (std::fabs(b[i]) > std::fabs(b[f])) f = i;
@@ -188,21 +194,25 @@ void Body::surfacePoints(std::vector<double> &v) const
         double tlx = cx + size * (c - s) / 2, tly = cy + size * (s + c) / 2;
         double brx = cx + size * (s - c) / 2, bry = cy - size * (s + c) / 2;
         for (int i = 0; i < nSide; ++i)
-            v.insert(v.end(), {brx + dl * (i + 0.5) * c, bry + dl * (i + 0.5) * s, 0.0});
+            v.insert(v.end(), {std::fma(dl * (i + 0.5), c, brx),
+                               std::fma(dl * (i + 0.5), s, bry), 0.0});
         for (int i = 0; i < nSide; ++i)
-            v.insert(v.end(), {tlx - dl * (i + 0.5) * c, tly - dl * (i + 0.5) * s, 0.0});
+            v.insert(v.end(), {std::fma(-(dl * (i + 0.5)), c, tlx),
+                               std::fma(-(dl * (i + 0.5)), s, tly), 0.0});
         for (int i = 0; i < nSide; ++i)
-            v.insert(v.end(), {brx - dl * (i + 0.5) * s, bry + dl * (i + 0.5) * c, 0.0});
+            v.insert(v.end(), {std::fma(-(dl * (i + 0.5)), s, brx),
+                               std::fma(dl * (i + 0.5), c, bry), 0.0});
         for (int i = 0; i < nSide; ++i)
-            v.insert(v.end(), {tlx + dl * (i + 0.5) * s, tly - dl * (i + 0.5) * c, 0.0});
+            v.insert(v.end(), {std::fma(dl * (i + 0.5), s, tlx),
+                               std::fma(-(dl * (i + 0.5)), c, tly), 0.0});
         return;
     }
     case 1:
     {   // Geometry.hpp:239-246
         double dth = 2.0 * kPi / npts;
         for (int i = 0; i < npts; ++i)
-            v.insert(v.end(), {size * std::cos(i * dth) + cx,
-                               size * std::sin(i * dth) + cy, 0.0});
+            v.insert(v.end(), {std::fma(size, std::cos(i * dth), cx),
+                               std::fma(size, std::sin(i * dth), cy), 0.0});
         return;
     }
     case 2:
@@ -211,10 +221,11 @@ void Body::surfacePoints(std::vector<double> &v) const
         for (int i = 0; i < npts; ++i)
         {
             double zf = 1.0 - 2.0 * (i + 0.5) / npts;
-            double rf = std::sqrt(1.0 - zf * zf);
+            double rf = std::sqrt(std::fma(-zf, zf, 1.0));
             double th = ga * i;
-            v.insert(v.end(), {cx + size * rf * std::cos(th),
-                               cy + size * rf * std::sin(th), cz + size * zf});
+            v.insert(v.end(), {std::fma(size * rf, std::cos(th), cx),
+                               std::fma(size * rf, std::sin(th), cy),
+                               std::fma(size, zf, cz)});
         }
         return;
     }
@@ -229,12 +240,12 @@ void Body::surfacePoints(std::vector<double> &v) const
                     {
                         double b[3];
                         b[f] = sgn * size / 2.0;
-                        b[(f + 1) % 3] = (i + 0.5) * dl - size / 2.0;
-                        b[(f + 2) % 3] = (j + 0.5) * dl - size / 2.0;
+                        b[(f + 1) % 3] = std::fma(i + 0.5, dl, -(size / 2.0));
+                        b[(f + 2) % 3] = std::fma(j + 0.5, dl, -(size / 2.0));
                         v.insert(v.end(),
-                                 {cx + Rm[0] * b[0] + Rm[1] * b[1] + Rm[2] * b[2],
-                                  cy + Rm[3] * b[0] + Rm[4] * b[1] + Rm[5] * b[2],
-                                  cz + Rm[6] * b[0] + Rm[7] * b[1] + Rm[8] * b[2]});
+                                 {std::fma(Rm[2], b[2], std::fma(Rm[1], b[1], std::fma(Rm[0], b[0], cx))),
+                                  std::fma(Rm[5], b[2], std::fma(Rm[4], b[1], std::fma(Rm[3], b[0], cy))),
+                                  std::fma(Rm[8], b[2], std::fma(Rm[7], b[1], std::fma(Rm[6], b[0], cz)))});
                     }
         return;
     }
@@ -369,13 +380,13 @@ static void generateLattice(Cloud &c)
 
     for (int k = 0; k < Nz; k++)
     {
-        double z = (ndim == 3) ? p.zfront + k * p.dz : 0.0;
+        double z = (ndim == 3) ? std::fma((double)k, p.dz, p.zfront) : 0.0;
         for (int j = 0; j < Ny; j++)
         {
-            double y = p.ybottom + j * p.dy;
+            double y = std::fma((double)j, p.dy, p.ybottom);
             for (int i = 0; i < Nx; i++)
             {
-                double x = p.xleft + i * p.dx;
+                double x = std::fma((double)i, p.dx, p.xleft);
                 c.x.push_back(x); c.y.push_back(y); c.z.push_back(z);
                 bool bx = (i == 0 || i == Nx - 1);
                 bool by = (j == 0 || j == Ny - 1);
@@ -450,8 +461,8 @@ static void embedBodies(Cloud &c)
             for (size_t q = 0; q + 2 < s.size(); q += 3)
             {
                 double dx = c.x[i] - s[q], dy = c.y[i] - s[q + 1];
-                double d2 = dx * dx + dy * dy;
-                if (ndim == 3) { double dz = c.z[i] - s[q + 2]; d2 += dz * dz; }
+                double d2 = std::fma(dx, dx, dy * dy);
+                if (ndim == 3) { double dz = c.z[i] - s[q + 2]; d2 = std::fma(dz, dz, d2); }
                 if (d2 < hug2) { drop = true; break; }
             }
         }
@@ -535,7 +546,7 @@ void rebuildNeighbours(Cloud &c)
                         double ddx = c.x[j] - c.x[i];
                         double ddy = c.y[j] - c.y[i];
                         double ddz = (ndim == 3) ? c.z[j] - c.z[i] : 0.0;
-                        if (ddx * ddx + ddy * ddy + ddz * ddz < r2max)
+                        if (std::fma(ddz, ddz, std::fma(ddx, ddx, ddy * ddy)) < r2max)
                         {
                             out[cnt++] = j;
                             if (cnt >= kMaxNeigh) { done = true; break; }
@@ -579,7 +590,7 @@ static void wallState(Cloud &c)
             w[6] = Tsum;
             continue;
         }
-        double nlen = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        double nlen = std::sqrt(std::fma(n[2], n[2], std::fma(n[0], n[0], n[1] * n[1])));
         if (nlen > eps) { n[0] /= nlen; n[1] /= nlen; n[2] /= nlen; }
         for (int a = 0; a < 3; ++a) { w[a] = n[a]; w[3 + a] = U[a] / nHit; }
         w[6] = Tsum / nHit;
@@ -592,8 +603,8 @@ static void wallState(Cloud &c)
             if (!c.boundary[i] || c.bodyId[i] >= 0) continue;
             if (std::fabs(c.y[i] - p.ytop) > 1e-13) continue;
             const double s = c.x[i] / L;
-            c.wall[7 * i + 3] = p.lidSpeed * (2.0 * s) * (2.0 * s) *
-                                (2.0 - 2.0 * s) * (2.0 - 2.0 * s);
+            const double t = std::fma(-2.0, s, 2.0);
+            c.wall[7 * i + 3] = p.lidSpeed * (2.0 * s) * (2.0 * s) * t * t;
         }
     }
 }
@@ -615,16 +626,17 @@ static void initialState(Cloud &c)
             for (int jv = 0; jv < Nv; ++jv)
                 for (int iv = 0; iv < Nv; ++iv)
                     row[iv + Nv * (jv + Nv * kv)] =
-                        maxwellian3(p.VMin + iv * p.dv, p.VMin + jv * p.dv,
-                                    p.VMin + kv * p.dv, 0, 0, 0, T, rho, R);
+                        maxwellian3(std::fma((double)iv, p.dv, p.VMin),
+                                    std::fma((double)jv, p.dv, p.VMin),
+                                    std::fma((double)kv, p.dv, p.VMin), 0, 0, 0, T, rho, R);
     }
     else
     {
         for (int jv = 0; jv < Nv; ++jv)
             for (int iv = 0; iv < Nv; ++iv)
             {
-                double m = maxwellianG1(p.VMin + iv * p.dv, p.VMin + jv * p.dv,
-                                        0, 0, T, rho, R);
+                double m = maxwellianG1(std::fma((double)iv, p.dv, p.VMin),
+                                        std::fma((double)jv, p.dv, p.VMin), 0, 0, T, rho, R);
                 row[iv + Nv * jv] = m;
                 row[iv + Nv * jv + Nv2] = 0.5 * R * T * m;
             }

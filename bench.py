@@ -1,0 +1,377 @@
+"""Benchmark of the B200 ALE-BGK step: cavity3d Nx=40 Nv=10, quadratic MLS.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step is the full time step of the 64 000-particle x 1 000-velocity cloud
+(transport, positivity + MOOD screen, mass rescale, diffuse wall, moments, BGK
+collision, moments, moodCheck).  The metric is particle x velocity updates
+per second.  Under torchrun (N > 1) every rank advances its own independent
+cavity on its own GPU -- the cavities do not exchange data -- so per-GPU work
+is fixed and scaling is weak; the step time is the max over ranks.
+
+Rank 0 prints one JSON line.  ``--impl reference`` times the reference's own
+CPU implementation (compiled unmodified into oracle/_ref) on this host's cores
+instead.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(case="cavity3d", Nx=40, Nv=10, mls_order=2)
+METRIC = "cavity3d Nx40 Nv10 updates/s"
+BYTES_PER_UPDATE_FP32 = 8.0     # read f once + write f once, FP32
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--ncu", action="store_true",
+                    help="profiler mode: --warmup steps then --steps steps, no timing "
+                         "and no JSON (for ncu launch lists and captures)")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+            time.sleep(0.3)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def recorded_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        e = d[kernel]
+        return float(e["bytes_per_launch"]), e.get("source", "")
+    except (OSError, KeyError, ValueError):
+        return None, ""
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline_reference(seconds_budget: float = 40.0):
+    """One full reference CPU step of the same workload on all host cores."""
+    from oracle.oracle import RefCase, ref_library
+    if ref_library() is None:
+        return None
+    r = RefCase(WORKLOAD["case"], WORKLOAD["Nx"], WORKLOAD["Nv"], -1.0, WORKLOAD["mls_order"])
+    cores = os.cpu_count() or 1
+    r.set_threads(cores)
+    t0 = time.perf_counter()
+    r.step(1)
+    t = time.perf_counter() - t0
+    updates = r.N * r.Nv ** 3
+    return {"value": updates / t, "unit": "updates/s", "cores": cores, "kind": "reference",
+            "sample": f"1 full step of {WORKLOAD['case']} Nx40 Nv10 quadratic "
+                      f"({r.N} x {r.Nv ** 3} updates, {t:.1f} s), reference CPU build "
+                      f"{os.path.basename(r.path)}, OpenMP {cores} threads"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle.oracle import RefCase, ref_library
+    if ref_library() is None:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref (the compiled reference) is not built"}))
+        return
+    cores = os.cpu_count() or 1
+    r = RefCase(WORKLOAD["case"], WORKLOAD["Nx"], WORKLOAD["Nv"], -1.0, WORKLOAD["mls_order"])
+    r.set_threads(cores)
+    updates = r.N * r.Nv ** 3
+    # A bounded sample: the first warm-up step is timed to project the run;
+    # steps are capped so that the whole arm ends within a few minutes.
+    budget = float(os.environ.get("ALEBGK_REF_BUDGET_S", "150"))
+    t0 = time.perf_counter()
+    r.step(1)
+    t1 = time.perf_counter() - t0
+    warm = max(0, min(args.warmup, int(budget * 0.25 / max(t1, 1e-9))) - 1)
+    if warm:
+        r.step(warm)
+    k = max(1, min(args.steps, int(budget / max(t1, 1e-9))))
+    t0 = time.perf_counter()
+    r.step(k)
+    t = time.perf_counter() - t0
+    v = updates * k / t
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "updates/s",
+        "n_gpus": 0, "steps": k, "warmup": warm + 1, "ms_per_step": 1e3 * t / k,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: the reference's own cavity3d case set-up (start from rest)",
+        "config": {"workload": "cavity3d Nx=40 Nv=10 quadratic MLS, 64000 particles x "
+                               "1000 velocities, dt=1e-11", "mls_order": 2},
+        "cpu_baseline": {"value": v, "unit": "updates/s", "cores": cores, "kind": "reference",
+                         "sample": f"{k} timed full steps after {warm + 1} warm-up, reference "
+                                   f"CPU build {os.path.basename(r.path)}, {cores} OpenMP threads"},
+        "e2e": {"value": v, "unit": "updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }))
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    rank, world, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    import alebgk4paper_b200 as ab
+    from alebgk4paper_b200 import _abi
+
+    case = ab.Case(WORKLOAD["case"], WORKLOAD["Nx"], WORKLOAD["Nv"], -1.0, WORKLOAD["mls_order"])
+    N, V = case.N, case.Nv ** 3
+    updates = N * V
+    s = ab.Solver(case, precision=args.precision, device=local)
+    lib = s.lib
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    ms = ctypes.c_float()
+    with ClockSampler(local) as clk:
+        # warm-up (also captures the two step graphs), held for at least half
+        # a second so that the clock samples see the GPU under this load
+        s.cudaStep(max(3, args.warmup))
+        s.sync()
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < 0.5:
+            s.cudaStep(4)
+            s.sync()
+        barrier()
+        rc = lib.alebgk_step_timed(s.ctx, args.steps, ctypes.byref(ms))
+        if rc != 0:
+            raise RuntimeError(f"alebgk_step_timed failed ({rc})")
+        barrier()
+    t_ms = ms.value
+    if dist is not None:
+        tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    value = world * updates * args.steps / (t_ms / 1e3)
+
+    # per-stage device times (kernel by kernel, events on the launching stream)
+    prof = (ctypes.c_float * _abi.NSTAGES)()
+    nprof = 3
+    rc = lib.alebgk_profile_steps(s.ctx, nprof, prof)
+    if rc != 0:
+        raise RuntimeError("alebgk_profile_steps failed")
+    stage_ms = {name: prof[i] / nprof for i, name in enumerate(_abi.STAGES)}
+    dominant = max(stage_ms, key=stage_ms.get)
+    step_ms_prof = sum(stage_ms.values())
+    peak, peak_src = measured_peak()
+    es = 4 if args.precision == 32 else 8
+    alg_bytes = {"transport": 2 * es, "post_transport": 2 * es, "finalize": 2 * es,
+                 "recollide": 2 * es, "redo": 2 * es}
+    per_update = alg_bytes.get(dominant, 2 * es)
+    achieved = per_update * updates / (stage_ms[dominant] / 1e3) / 1e9
+    kern_name = {"transport": "k_transport", "post_transport": "k_post_transport",
+                 "finalize": "k_finalize"}.get(dominant, dominant)
+    traffic, traffic_src = recorded_traffic(kern_name)
+
+    # end to end through the C-ABI with host buffers: every step uploads the
+    # full FP64 state from pinned host memory (alebgk_upload_state, the
+    # cudaUploadCloud of the reference's hybrid loop), runs one step and reads
+    # the moment field back (alebgk_download_moments).
+    g_host = torch.empty((N, case.gstride), dtype=torch.float64, pin_memory=True)
+    mac_host = torch.empty((N, 7), dtype=torch.float64, pin_memory=True)
+    gd, md = s.cudaDownloadFull()
+    g_host.copy_(torch.from_numpy(gd))
+    mac_host.copy_(torch.from_numpy(md))
+    gp = ctypes.cast(g_host.data_ptr(), _abi.c_double_p)
+    mp = ctypes.cast(mac_host.data_ptr(), _abi.c_double_p)
+
+    def e2e_step():
+        r1 = lib.alebgk_upload_state(s.ctx, gp, mp)
+        r2 = lib.alebgk_step(s.ctx, 1)
+        r3 = lib.alebgk_download_moments(s.ctx, mp)
+        if r1 or r2 or r3:
+            raise RuntimeError("e2e step failed")
+
+    e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    barrier()
+    te = time.perf_counter() - t0
+    if dist is not None:
+        tt = torch.tensor([te], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te = float(tt.item())
+    e2e_value = world * updates * args.e2e_steps / te
+    h2d = N * case.gstride * 8 + N * 7 * 8
+    d2h = N * 7 * 8
+
+    cnt = s.counters()
+    s.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_reference()
+        except Exception as exc:  # reported, never gating
+            cpu = {"value": None, "unit": "updates/s", "cores": os.cpu_count(),
+                   "kind": "reference", "sample": f"not run: {exc}"}
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(3, args.warmup),
+        "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if args.precision == 32 else "f64",
+        "data": "synthetic: the reference's cavity3d case set-up, gas at rest at t=0",
+        "config": {"workload": "cavity3d Nx=40 Nv=10 quadratic MLS, 64000 particles x 1000 "
+                               "velocities, dt=1e-11, FP32 f storage + FP32 MLS "
+                               "reconstruction, FP64 sums",
+                   "particles": N, "velocities": V, "mls_order": 2,
+                   "parallelism": f"{world} independent cavities, one per GPU",
+                   "l2": "inputs larger than L2: two 256 MB distribution buffers "
+                         "ping-pong, no flush needed"},
+        "gpu_launches": 8 * args.steps,
+        "stage_ms": {k: round(v, 5) for k, v in stage_ms.items()},
+        "roofline": {"bound": "hbm", "kernel": kern_name, "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_src, "traffic": traffic,
+                     "traffic_source": traffic_src,
+                     "algorithmic_bytes_per_launch": per_update * updates},
+        "step_roofline": {"achieved": BYTES_PER_UPDATE_FP32 * (es / 4) * updates /
+                                      (t_ms / args.steps / 1e3) / 1e9,
+                          "peak": peak, "unit": "GB/s",
+                          "frac": BYTES_PER_UPDATE_FP32 * (es / 4) * updates /
+                                  (t_ms / args.steps / 1e3) / 1e9 / peak,
+                          "note": "whole step against 8 B/update (FP32) algorithmic bytes"},
+        "e2e": {"value": e2e_value, "unit": "updates/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
+                "path": "alebgk_upload_state + alebgk_step + alebgk_download_moments, "
+                        "pinned host buffers, wall clock"},
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+        "counters": {"transport_flags": cnt["transport_flags"],
+                     "mood_fail": cnt["mood_fail"]},
+    }
+    print(json.dumps(out))
+
+
+def run_ncu(args):
+    import alebgk4paper_b200 as ab
+    case = ab.Case(WORKLOAD["case"], WORKLOAD["Nx"], WORKLOAD["Nv"], -1.0, WORKLOAD["mls_order"])
+    s = ab.Solver(case, precision=args.precision)
+    s.cudaStep(args.warmup)
+    s.cudaStep(args.steps)
+    s.sync()
+    s.close()
+
+
+def main():
+    args = parse()
+    if args.ncu:
+        run_ncu(args)
+    elif args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,96 @@
+"""Generates the golden fixtures in this folder from the reference itself.
+
+The reference ships no tests or golden vectors, so every fixture here is the
+output of the reference's own CPU code (compiled unmodified by
+``oracle/Makefile`` into ``oracle/_ref/``), run through ``oracle/ref_driver.cpp``
+with the reference's set-up and step order.  Re-run after rebuilding
+``oracle/_ref``::
+
+    make -C oracle ref && python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle.oracle import RefCase  # noqa: E402
+
+# (case, Nx, Nv, mls_order, fixed body)
+SETUPS = [
+    ("cavity2d", 12, 8, 2, True),
+    ("cavity3d", 6, 4, 2, True),
+    ("cavity2d-square", 24, 8, 2, True),
+    ("cavity2d-circle", 20, 8, 2, True),
+    ("cavity3d-sphere", 12, 4, 2, True),
+    ("cavity3d-cube", 12, 4, 2, True),
+]
+
+# (tag, case, Nx, Nv, mls_order, steps, keep full g)
+STEPS = [
+    ("c2d_n8_v8_q_s5", "cavity2d", 8, 8, 2, 5, True),
+    ("c2d_n20_v16_q_s20", "cavity2d", 20, 16, 2, 20, False),
+    ("c2d_n20_v16_l_s20", "cavity2d", 20, 16, 1, 20, False),
+    ("c3d_n6_v4_q_s3", "cavity3d", 6, 4, 2, 3, True),
+    ("c3d_n10_v6_q_s3", "cavity3d", 10, 6, 2, 3, False),
+    ("c3d_n9_v5_q_s3", "cavity3d", 9, 5, 2, 3, False),
+    ("cube_n12_v4_q_s2", "cavity3d-cube", 12, 4, 2, 2, False),
+    ("square_n24_v8_q_s4", "cavity2d-square", 24, 8, 2, 4, False),
+]
+
+
+def nbr_hash(nbr: np.ndarray, nnb: np.ndarray) -> np.ndarray:
+    """Order-sensitive per-particle hash of the neighbour list."""
+    out = np.zeros(len(nnb), np.int64)
+    for i, n in enumerate(nnb):
+        h = 1469598103934665603
+        for j in nbr[i, :n]:
+            h = ((h ^ int(j)) * 1099511628211) & 0x7FFFFFFFFFFFFFFF
+        out[i] = h
+    return out
+
+
+def main():
+    for case, Nx, Nv, order, fixed in SETUPS:
+        r = RefCase(case, Nx, Nv, -1.0, order, fixed_body=fixed)
+        c = r.cloud()
+        np.savez_compressed(
+            os.path.join(HERE, f"setup_{case}_n{Nx}_v{Nv}.npz"),
+            xyz=c["xyz"], wall=c["wall"], boundary=c["boundary"], body_id=c["body_id"],
+            nnb=c["nnb"], nbr_hash=nbr_hash(c["nbr"], c["nnb"]), g0=r.g()[:4],
+            params=np.array([r.params[k] for k in ("dt", "tau", "R", "dx", "radius", "dv",
+                                                   "vmin", "rho0", "Tw")]))
+    for tag, case, Nx, Nv, order, steps, full in STEPS:
+        r = RefCase(case, Nx, Nv, -1.0, order, fixed_body=True)
+        flags = []
+        for _ in range(steps):
+            st = r.step(1)
+            flags.append([st["transport_flags"], st["mood_fail"]])
+        g = r.g()
+        d = dict(case=case, Nx=Nx, Nv=Nv, order=order, steps=steps, macro=r.macro(),
+                 gsum=g.sum(axis=1), gabs=np.abs(g).sum(axis=1), flags=np.array(flags),
+                 mass=r.sum_mass())
+        if full:
+            d["g"] = g
+        np.savez_compressed(os.path.join(HERE, f"step_{tag}.npz"), **d)
+    # Free cube: one step of the reference's moving-body path
+    # (RigidBody/BodyDynamics.cpp:143-711) -> body state after the Heun update.
+    r = RefCase("cavity3d-cube", 12, 4, -1.0, 2, fixed_body=False)
+    b0 = r.bodies().copy()
+    g0 = r.g()
+    m0 = r.macro()
+    c0 = r.cloud()
+    r.step(1)
+    np.savez_compressed(os.path.join(HERE, "body_cube_n12_v4_free_s1.npz"),
+                        bodies_before=b0, bodies_after=r.bodies(), N_after=r.N,
+                        mass_after=r.sum_mass(), g0_sum=g0.sum(), m0=m0[:, 0].sum(),
+                        nsurf=int((c0["body_id"] >= 0).sum()))
+    print("fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()
