@@ -12,8 +12,8 @@ c_double_p = ctypes.POINTER(ctypes.c_double)
 
 MAX_NEIGH = 128
 NSTAGES = 8
-STAGES = ("transport", "post_transport", "redo", "mass_after_transport",
-          "finalize", "recollide", "mass_end", "step_begin")
+STAGES = ("transport", "particle", "sigma", "scale_mood", "recollide", "mass_end",
+          "step_begin", "unused")
 OK, EINVAL, ECUDA, ESTATE, ENOMEM, EDEVICE = 0, -1, -2, -3, -4, -5
 
 

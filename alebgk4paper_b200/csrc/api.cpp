@@ -41,9 +41,10 @@ cudaError_t dalloc(P **p, size_t n)
 void freeBuffers(alebgk_ctx *c)
 {
     DeviceBuffers &d = c->d;
-    void *ptrs[] = {d.f[0], d.f[1], d.coef, d.pos, d.meshv, d.wall, d.boundary,
-                    d.bodyId, d.cls, d.nslot, d.slots, d.macro, d.mood, d.flag,
-                    d.list, d.mass, d.dpx, d.bodyTmp, d.bodyOut, d.stage, d.sc};
+    void *ptrs[] = {d.f[0], d.f[1], d.coef, d.coefLin, d.pos, d.meshv, d.wall,
+                    d.boundary, d.bodyId, d.cls, d.nslot, d.slots, d.macro[0],
+                    d.macro[1], d.mood, d.flag, d.massPos, d.massEnd, d.minG,
+                    d.dpx, d.bodyTmp, d.bodyOut, d.stage, d.sc};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     d = DeviceBuffers();
@@ -166,9 +167,19 @@ int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
     in.xyz = cl->xyz; in.meshv = cl->meshv; in.wall = cl->wall;
     in.boundary = cl->boundary; in.nnb = cl->nnb; in.nbr = cl->nbr;
     in.maxNeigh = ALEBGK_MAX_NEIGH;
-    CoeffTables tb;
+    CoeffTables tb, tl;
     std::string err;
     if (!buildCoefficients(in, tb, &err)) return fail(c, ALEBGK_EINVAL, err);
+    // Linear tables for the MOOD redo (mlsTransportCompute(..., 1, true)),
+    // on the same classes and slot order.
+    CoeffInput inLin = in;
+    inLin.mlsOrder = 1;
+    if (p.limiter == 2)
+    {
+        if (!buildCoefficients(inLin, tl, &err)) return fail(c, ALEBGK_EINVAL, err);
+        if (tl.cls != tb.cls || tl.slots != tb.slots || tl.S != tb.S)
+            return fail(c, ALEBGK_EINVAL, "linear and quadratic stencil classes differ");
+    }
     p.S = tb.S;
     c->ncls = tb.ncls;
     c->degenerateParticles = 0;
@@ -184,15 +195,16 @@ int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
     CK(cudaMemsetAsync(d.f[0], 0, fBytes, c->stream));
     CK(cudaMemsetAsync(d.f[1], 0, fBytes, c->stream));
     const size_t ncoef = (size_t)tb.ncls * tb.S * tb.V;
-    CK(cudaMalloc(&d.coef, std::max<size_t>(ncoef, 1) * es));
-    if (f64)
-        CK(cudaMemcpy(d.coef, tb.coef.data(), ncoef * 8, cudaMemcpyHostToDevice));
-    else
-    {
+    auto putTable = [&](void **dst, const std::vector<double> &src) -> cudaError_t {
+        cudaError_t e = cudaMalloc(dst, std::max<size_t>(ncoef, 1) * es);
+        if (e != cudaSuccess || src.empty()) return e;
+        if (f64) return cudaMemcpy(*dst, src.data(), ncoef * 8, cudaMemcpyHostToDevice);
         std::vector<float> cf(ncoef);
-        for (size_t q = 0; q < ncoef; ++q) cf[q] = (float)tb.coef[q];
-        CK(cudaMemcpy(d.coef, cf.data(), ncoef * 4, cudaMemcpyHostToDevice));
-    }
+        for (size_t q = 0; q < ncoef; ++q) cf[q] = (float)src[q];
+        return cudaMemcpy(*dst, cf.data(), ncoef * 4, cudaMemcpyHostToDevice);
+    };
+    CK(putTable(&d.coef, tb.coef));
+    CK(putTable(&d.coefLin, p.limiter == 2 ? tl.coef : tb.coef));
     CK(dalloc(&d.pos, 3 * (size_t)N));
     CK(dalloc(&d.meshv, 3 * (size_t)N));
     CK(dalloc(&d.wall, 7 * (size_t)N));
@@ -201,11 +213,13 @@ int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
     CK(dalloc(&d.cls, N));
     CK(dalloc(&d.nslot, N));
     CK(dalloc(&d.slots, (size_t)N * tb.S));
-    CK(dalloc(&d.macro, 6 * (size_t)N));
+    CK(dalloc(&d.macro[0], 6 * (size_t)N));
+    CK(dalloc(&d.macro[1], 6 * (size_t)N));
     CK(dalloc(&d.mood, N));
     CK(dalloc(&d.flag, N));
-    CK(dalloc(&d.list, N));
-    CK(dalloc(&d.mass, N));
+    CK(dalloc(&d.massPos, N));
+    CK(dalloc(&d.massEnd, N));
+    CK(dalloc(&d.minG, N));
     CK(dalloc(&d.dpx, N));
     CK(dalloc(&d.bodyTmp, 6 * (size_t)N));
     CK(dalloc(&d.bodyOut, 64 * 6));
@@ -242,7 +256,7 @@ int alebgk_upload_state(alebgk_ctx *c, const double *g, const double *macro)
         for (int q = 0; q < 6; ++q) mac[6 * (size_t)i + q] = macro[7 * (size_t)i + q];
         mood[i] = macro[7 * (size_t)i + 6] != 0.0;
     }
-    CK(cudaMemcpy(c->d.macro, mac.data(), mac.size() * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d.macro[c->cur], mac.data(), mac.size() * 8, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c->d.mood, mood.data(), 4 * (size_t)N, cudaMemcpyHostToDevice));
     cudaError_t e = cudaMemcpyAsync(c->d.stage, g, (size_t)N * p.gs * 8,
                                     cudaMemcpyHostToDevice, c->stream);
@@ -334,7 +348,7 @@ int alebgk_profile_steps(alebgk_ctx *c, int nsteps, float *ms)
     if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
     CK(cudaSetDevice(c->cfg.device));
     // launch order -> stage index of include/alebgk.h
-    static const int stageOf[ALEBGK_NSTAGES] = {7, 0, 1, 2, 3, 4, 5, 6};
+    static const int stageOf[ALEBGK_NSTAGES] = {6, 0, 1, 2, 3, 4, 5, 7};
     cudaEvent_t ev[ALEBGK_NSTAGES + 1];
     for (auto &e : ev) CK(cudaEventCreate(&e));
     for (int q = 0; q < ALEBGK_NSTAGES; ++q) ms[q] = 0.0f;
@@ -368,7 +382,8 @@ int alebgk_download_moments(alebgk_ctx *c, double *macro)
     const int N = c->sp.N;
     std::vector<double> mac(6 * (size_t)N);
     std::vector<int> mood(N);
-    CK(cudaMemcpyAsync(mac.data(), c->d.macro, mac.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(mac.data(), c->d.macro[c->cur], mac.size() * 8, cudaMemcpyDeviceToHost,
+                       c->stream));
     CK(cudaMemcpyAsync(mood.data(), c->d.mood, 4 * (size_t)N, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     for (int i = 0; i < N; ++i)
@@ -412,7 +427,7 @@ int alebgk_get_counters(alebgk_ctx *c, alebgk_counters *out)
     out->mass_after_transport = s.massNew;
     out->mass_scale = s.sigma;
     out->mass_end = s.massEnd;
-    out->mass_before = (s.sigma != 0.0) ? s.sigma * s.massNew : s.massOld;
+    out->mass_before = s.sigma * s.massNew;
     out->error_word = s.err;
     return ALEBGK_OK;
 }

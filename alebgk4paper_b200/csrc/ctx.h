@@ -13,13 +13,20 @@ namespace alebgk {
 // Per-step scalars kept on the device so that a step needs no host
 // synchronisation (the reference reads three masses back per step,
 // Solver/CudaBackend.cu:1384-1395).
+//
+// The stored distribution h is the true one divided by `scale`: the global
+// mass rescale of a step (Solver/Solver.cpp:650-655) is a uniform factor, and
+// everything after it in the step is homogeneous of degree one in g, so the
+// factor is applied to the macros at once and to h lazily, by the next
+// transport (which is linear) and by every download.
 struct StepScalars
 {
-    double massOld;        // sumMass at the start of the step
-    double massNew;        // sumMass after transport + positivity + redo
-    double sigma;          // massOld / massNew
-    double massEnd;        // sumMass at the end of the step
-    int nflag;             // transport MOOD flags (length of the redo list)
+    double massOld;        // true sumMass at the start of the step
+    double massNew;        // true sumMass after transport + positivity + redo
+    double sigma;          // massOld / massNew of the last step
+    double massEnd;        // true sumMass at the end of the step
+    double scale;          // true g = scale * stored h
+    int nflag;             // transport MOOD flags
     int nfix;              // positivity repairs
     int moodfail;          // post-collision moodCheck failed
     int err;               // device error bits
@@ -29,13 +36,17 @@ struct StepScalars
 struct DeviceBuffers
 {
     void *f[2] = {nullptr, nullptr};   // ping-pong distribution, N x ldf
-    void *coef = nullptr;              // [class][slot][node]
+    void *coef = nullptr;              // [class][slot][node], MLS order of the cloud
+    void *coefLin = nullptr;           // same, linear MLS (MOOD redo)
     double *pos = nullptr, *meshv = nullptr, *wall = nullptr;
     int *boundary = nullptr, *bodyId = nullptr;
     int *cls = nullptr, *nslot = nullptr, *slots = nullptr;
-    double *macro = nullptr;           // N x 6: rho ux uy uz T p
-    int *mood = nullptr, *flag = nullptr, *list = nullptr;
-    double *mass = nullptr, *dpx = nullptr;
+    double *macro[2] = {nullptr, nullptr};   // N x 6: rho ux uy uz T p (true)
+    int *mood = nullptr, *flag = nullptr;
+    double *massPos = nullptr;         // per particle: mass after positivity (true)
+    double *massEnd = nullptr;         // per particle: mass of h at step end
+    double *minG = nullptr;            // per particle: min of h over the mass layer
+    double *dpx = nullptr;
     double *bodyTmp = nullptr;         // N x 6 per-particle load contributions
     double *bodyOut = nullptr;         // up to 64 bodies x 6
     double *stage = nullptr;           // N x gs FP64 host-transfer staging
@@ -59,13 +70,12 @@ struct alebgk_ctx
     alebgk::StepParams sp;
     alebgk::DeviceBuffers d;
     cudaStream_t stream = nullptr;
-    int cur = 0;                 // buffer holding the current g
+    int cur = 0;                 // buffer holding the current h and macros
     bool uploaded = false;
     int ncls = 0;
     int degenerateParticles = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     std::string err;
-    // host staging
     std::vector<int> bodyIdHost;
 };
 

@@ -158,8 +158,8 @@ int alebgk_step_timed(alebgk_ctx *ctx, int nsteps, float *ms);
 
 /* Runs nsteps steps kernel by kernel (no graph) with a CUDA event between
  * every launch, and returns the summed device time of each stage in
- * ms_per_stage[0..ALEBGK_NSTAGES-1] (transport, post_transport, redo,
- * mass_after_transport, finalize, recollide, mass_end, step_begin).
+ * ms_per_stage[0..ALEBGK_NSTAGES-1] (transport, particle, sigma, scale_mood,
+ * recollide, mass_end, step_begin, unused).
  * Replaces the one-shot [GPU-PROFILE] table of
  * Solver/CudaBackend.cu:1518-1623. */
 #define ALEBGK_NSTAGES 8
