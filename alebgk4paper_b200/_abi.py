@@ -11,9 +11,9 @@ c_int_p = ctypes.POINTER(ctypes.c_int)
 c_double_p = ctypes.POINTER(ctypes.c_double)
 
 MAX_NEIGH = 128
-NSTAGES = 8
-STAGES = ("transport", "particle", "sigma", "scale_mood", "recollide", "mass_end",
-          "step_begin", "unused")
+NSTAGES = 10
+STAGES = ("transport", "particle", "redo", "sigma", "fixup", "mass_sum", "scale_mood",
+          "recollide", "mass_end", "step_begin")
 OK, EINVAL, ECUDA, ESTATE, ENOMEM, EDEVICE = 0, -1, -2, -3, -4, -5
 
 
@@ -26,6 +26,7 @@ class Config(ctypes.Structure):
         ("R", ctypes.c_double), ("tau", ctypes.c_double), ("dHS", ctypes.c_double),
         ("vmin", ctypes.c_double), ("dv", ctypes.c_double), ("radius", ctypes.c_double),
         ("periodic", ctypes.c_int * 3), ("L", ctypes.c_double * 3),
+        ("transport", ctypes.c_int),
     ]
 
 
@@ -44,7 +45,7 @@ class Counters(ctypes.Structure):
         ("mls_degenerate", ctypes.c_int),
         ("mass_before", ctypes.c_double), ("mass_after_transport", ctypes.c_double),
         ("mass_scale", ctypes.c_double), ("mass_end", ctypes.c_double),
-        ("error_word", ctypes.c_int),
+        ("error_word", ctypes.c_int), ("transport_kernel", ctypes.c_int),
     ]
 
 

@@ -11,6 +11,7 @@
 #include "cases.h"
 #include "coeffs.h"
 #include "ctx.h"
+#include "march.h"
 
 using namespace alebgk;
 
@@ -43,11 +44,14 @@ void freeBuffers(alebgk_ctx *c)
     DeviceBuffers &d = c->d;
     void *ptrs[] = {d.f[0], d.f[1], d.coef, d.coefLin, d.pos, d.meshv, d.wall,
                     d.boundary, d.bodyId, d.cls, d.nslot, d.slots, d.macro[0],
-                    d.macro[1], d.mood, d.flag, d.massPos, d.massEnd, d.minG,
+                    d.macro[1], d.mood, d.flag, d.flagList, d.degList, d.massPos, d.massEnd, d.minG,
                     d.dpx, d.bodyTmp, d.bodyOut, d.stage, d.sc};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     d = DeviceBuffers();
+    if (c->march.units) cudaFree(c->march.units);
+    if (c->march.coefT) cudaFree(c->march.coefT);
+    c->march = MarchState();
     for (auto &g : c->graph)
         if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     c->uploaded = false;
@@ -75,10 +79,10 @@ int alebgk_create(const alebgk_config *cfg, alebgk_ctx **out)
     if (!(cfg->tau > 0) || !(cfg->R > 0) || !(cfg->dv > 0) || !(cfg->radius > 0))
         return fail(nullptr, ALEBGK_EINVAL, "tau, R, dv and radius must be > 0");
     const int gs = (cfg->dim == 3) ? cfg->Nv * cfg->Nv * cfg->Nv : 2 * cfg->Nv * cfg->Nv;
-    if ((size_t)gs * sizeof(double) > 200 * 1024)
+    if ((size_t)gs * (cfg->precision == 64 ? 8 : 4) > 160 * 1024)
         return fail(nullptr, ALEBGK_EINVAL,
-                    "a particle's distribution exceeds the 200 KB per-particle "
-                    "shared-memory row of the finalize kernel");
+                    "a particle's distribution exceeds the 160 KB shared-memory row "
+                    "of the particle kernel");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return fail(nullptr, ALEBGK_ECUDA, "no CUDA device available");
@@ -217,6 +221,8 @@ int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
     CK(dalloc(&d.macro[1], 6 * (size_t)N));
     CK(dalloc(&d.mood, N));
     CK(dalloc(&d.flag, N));
+    CK(dalloc(&d.flagList, N));
+    CK(dalloc(&d.degList, N));
     CK(dalloc(&d.massPos, N));
     CK(dalloc(&d.massEnd, N));
     CK(dalloc(&d.minG, N));
@@ -236,6 +242,33 @@ int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
     CK(cudaMemset(d.dpx, 0, 8 * (size_t)N));
     CK(cudaMemset(d.sc, 0, sizeof(StepScalars)));
     CK(prepareKernels(c));
+    // Lattice-marching transport (FP32, complete 3-D lattice).
+    if (!f64 && c->cfg.transport != 1)
+    {
+        MarchPlan plan;
+        buildMarchPlan(cl->xyz, N, p.dim, cl->nnb, cl->nbr, ALEBGK_MAX_NEIGH, tb,
+                       nullptr, plan);
+        if (plan.ok)
+        {
+            MarchState &m = c->march;
+            m.nunits = (int)plan.units.size();
+            m.Vpad = plan.Vpad; m.Nx = plan.Nx; m.Ny = plan.Ny; m.Nz = plan.Nz;
+            CK(cudaMalloc(&m.units, sizeof(MarchUnit) * m.nunits));
+            CK(cudaMemcpy(m.units, plan.units.data(), sizeof(MarchUnit) * m.nunits,
+                          cudaMemcpyHostToDevice));
+            CK(cudaMalloc(&m.coefT, plan.coefT.size() * 4));
+            CK(cudaMemcpy(m.coefT, plan.coefT.data(), plan.coefT.size() * 4,
+                          cudaMemcpyHostToDevice));
+            for (int b = 0; b < 2; ++b)
+                if (!encodeMarchMap(m.tmap[b], d.f[b], p.V, m.Nx, m.Ny, m.Nz, p.ldf, &err))
+                    return fail(c, ALEBGK_ECUDA, err);
+            CK(prepareMarch());
+            m.enabled = true;
+        }
+    }
+    if (c->cfg.transport == 2 && !c->march.enabled)
+        return fail(c, ALEBGK_EINVAL,
+                    "the lattice march needs FP32 and a complete 3-D lattice cloud");
     c->bodyIdHost.assign(cl->body_id, cl->body_id + N);
     c->cur = 0;
     c->uploaded = true;
@@ -348,7 +381,7 @@ int alebgk_profile_steps(alebgk_ctx *c, int nsteps, float *ms)
     if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
     CK(cudaSetDevice(c->cfg.device));
     // launch order -> stage index of include/alebgk.h
-    static const int stageOf[ALEBGK_NSTAGES] = {6, 0, 1, 2, 3, 4, 5, 7};
+    static const int stageOf[ALEBGK_NSTAGES] = {9, 0, 1, 2, 3, 4, 5, 6, 7, 8};
     cudaEvent_t ev[ALEBGK_NSTAGES + 1];
     for (auto &e : ev) CK(cudaEventCreate(&e));
     for (int q = 0; q < ALEBGK_NSTAGES; ++q) ms[q] = 0.0f;
@@ -429,6 +462,7 @@ int alebgk_get_counters(alebgk_ctx *c, alebgk_counters *out)
     out->mass_end = s.massEnd;
     out->mass_before = s.sigma * s.massNew;
     out->error_word = s.err;
+    out->transport_kernel = c->march.enabled ? 2 : 1;
     return ALEBGK_OK;
 }
 

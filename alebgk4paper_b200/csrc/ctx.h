@@ -10,6 +10,18 @@
 
 namespace alebgk {
 
+struct MarchUnit;
+
+// Device state of the lattice-marching transport (march.cu).
+struct MarchState
+{
+    bool enabled = false;
+    int nunits = 0, Vpad = 0, Nx = 0, Ny = 0, Nz = 0;
+    MarchUnit *units = nullptr;
+    float *coefT = nullptr;
+    alignas(64) unsigned char tmap[2][128];   // CUtensorMap per source buffer
+};
+
 // Per-step scalars kept on the device so that a step needs no host
 // synchronisation (the reference reads three masses back per step,
 // Solver/CudaBackend.cu:1384-1395).
@@ -26,7 +38,8 @@ struct StepScalars
     double sigma;          // massOld / massNew of the last step
     double massEnd;        // true sumMass at the end of the step
     double scale;          // true g = scale * stored h
-    int nflag;             // transport MOOD flags
+    int nflag;             // transport MOOD flags (length of the redo list)
+    int ndeg;              // particles finished after sigma (k_fixup list)
     int nfix;              // positivity repairs
     int moodfail;          // post-collision moodCheck failed
     int err;               // device error bits
@@ -43,6 +56,7 @@ struct DeviceBuffers
     int *cls = nullptr, *nslot = nullptr, *slots = nullptr;
     double *macro[2] = {nullptr, nullptr};   // N x 6: rho ux uy uz T p (true)
     int *mood = nullptr, *flag = nullptr;
+    int *flagList = nullptr, *degList = nullptr;
     double *massPos = nullptr;         // per particle: mass after positivity (true)
     double *massEnd = nullptr;         // per particle: mass of h at step end
     double *minG = nullptr;            // per particle: min of h over the mass layer
@@ -69,6 +83,7 @@ struct alebgk_ctx
     alebgk_config cfg{};
     alebgk::StepParams sp;
     alebgk::DeviceBuffers d;
+    alebgk::MarchState march;
     cudaStream_t stream = nullptr;
     int cur = 0;                 // buffer holding the current h and macros
     bool uploaded = false;
@@ -92,5 +107,9 @@ cudaError_t launchSetSurfaceVelocity(alebgk_ctx *c, int nbodies,
                                      const double *stateDev);
 cudaError_t launchConvertIn(alebgk_ctx *c, const double *src, int buf);
 cudaError_t launchConvertOut(alebgk_ctx *c, double *dst, int buf);
+cudaError_t launchMarch(alebgk_ctx *c, const void *tmap, float *outBuf, cudaStream_t st);
+cudaError_t prepareMarch();
+bool encodeMarchMap(void *tmapOut, void *f, int V, int Nx, int Ny, int Nz, int ldf,
+                    std::string *err);
 
 }  // namespace alebgk

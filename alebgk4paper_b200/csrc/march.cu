@@ -1,0 +1,316 @@
+// march.cu -- lattice-marching MLS transport for sm_100a (FP32).
+//
+// gt(x,y,z;k) = scale * sum_o C[class][o][k] * h(x+o;k) over the 81 lattice
+// offsets |o|^2 <= 6, for a cloud that is a complete lattice (march.h).
+//
+// CTA = one work unit (an 8x4 tile of lattice columns, output planes
+// [za, zb)) x one chunk of 32 velocities, lane = velocity.  The CTA marches
+// through z: every input plane of the tile plus a two-column halo (12x8
+// particles x 32 velocities, 12 KB) is brought into a four-slot shared-
+// memory ring by one TMA tensor load (cp.async.bulk.tensor.4d, completion on
+// an mbarrier; zero fill outside the lattice).  Each warp owns one
+// class-uniform 2x2 block of columns; its 81 coefficients for its lane's
+// velocity stay in registers for the whole march, and every staged value
+// feeds the FMAs of up to four columns and five output planes, held in a
+// 4 x 5 register queue.  An output plane is complete two input planes after
+// its own and is stored straight from the queue.  Every wait is bounded; a
+// timeout sets the step's error word instead of hanging.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <utility>
+
+#include "ctx.h"
+#include "march.h"
+
+namespace alebgk {
+
+namespace {
+
+constexpr int kPW = kMarchTileX + 4;      // staged plane: 12 x 8 particles
+constexpr int kPH = kMarchTileY + 4;
+constexpr int kRing = 4;
+constexpr uint32_t kPlaneBytes = kPW * kPH * kMarchChunk * 4;
+constexpr long long kSpinLimit = 1ll << 20;
+
+__host__ __device__ constexpr int tidx(int dx, int dy, int dz)
+{
+    int n = 0;
+    for (int z = -2; z <= 2; ++z)
+        for (int y = -2; y <= 2; ++y)
+            for (int x = -2; x <= 2; ++x)
+            {
+                if (x * x + y * y + z * z > 6) continue;
+                if (x == dx && y == dy && z == dz) return n;
+                ++n;
+            }
+    return -1;
+}
+static_assert(tidx(2, 1, 1) >= 0 && tidx(2, 2, 0) < 0, "template");
+
+template <int... I, typename F>
+__device__ __forceinline__ void unrollImpl(std::integer_sequence<int, I...>, F &&f)
+{
+    (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, typename F>
+__device__ __forceinline__ void unroll(F &&f)
+{
+    unrollImpl(std::make_integer_sequence<int, N>{}, f);
+}
+
+__device__ __forceinline__ uint32_t smemAddr(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbarInit(uint64_t *bar, int count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbarExpectTx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbarArrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smemAddr(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbarTryWait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smemAddr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait on an mbarrier phase.  After kSpinLimit polls the wait gives
+// up and marks the CTA dead; a dead CTA does not wait again, so a broken
+// pipeline costs one timeout, not one per plane.
+__device__ __forceinline__ bool mbarWait(uint64_t *bar, uint32_t parity, bool &dead)
+{
+    if (dead) return false;
+    for (long long it = 0; it < kSpinLimit; ++it)
+        if (mbarTryWait(bar, parity)) return true;
+    dead = true;
+    return false;
+}
+
+__device__ __forceinline__ void tmaLoadPlane(void *dst, const CUtensorMap *map, uint64_t *bar,
+                                             int c0, int c1, int c2, int c3)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smemAddr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
+        "r"(smemAddr(bar))
+        : "memory");
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kMarchWarps * 32, 2)
+k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ units,
+        const float *__restrict__ coefT, float *__restrict__ out, int Nx, int Ny, int V,
+        int Vpad, int ldf, StepScalars *sc)
+{
+    extern __shared__ __align__(128) unsigned char marchSmem[];
+    typedef float Plane[kPH][kPW][kMarchChunk];
+    Plane *ring = reinterpret_cast<Plane *>(marchSmem);
+    __shared__ __align__(8) uint64_t full[kRing], empty[kRing];
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const MarchUnit &u = units[blockIdx.x];
+    const int ux0 = u.x0, uy0 = u.y0, za = u.za, zb = u.zb;
+    const int k0 = blockIdx.y * kMarchChunk;
+    const int k = k0 + lane;
+    const int nin = zb - za + 4;                 // input planes za-2 .. zb+1
+    const bool active = warp < u.nsub;
+    const int sub = active ? __ldg(&u.sub[warp]) : 0;
+    const int bx = sub & 15, by = (sub >> 4) & 15, mask = (sub >> 8) & 15, cls = sub >> 12;
+    if (*(volatile int *)&sc->err) return;      // an earlier CTA gave up
+
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < kRing; ++s)
+        {
+            mbarInit(&full[s], 1);
+            mbarInit(&empty[s], kMarchWarps);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int n = 0; n < kRing && n < nin; ++n)
+        {
+            mbarExpectTx(&full[n], kPlaneBytes);
+            tmaLoadPlane(&ring[n][0][0][0], &tmap, &full[n], k0, ux0 - 2, uy0 - 2,
+                         za - 2 + n);
+        }
+
+    float coef[kTmplOffsets];
+    if (active)
+    {
+        const float *cb = coefT + (size_t)cls * kTmplOffsets * Vpad + k;
+#pragma unroll
+        for (int o = 0; o < kTmplOffsets; ++o) coef[o] = __ldg(cb + (size_t)o * Vpad);
+    }
+    float acc[4][5];
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int r = 0; r < 5; ++r) acc[c][r] = 0.0f;
+    const float scale = (float)sc->scale;
+    bool dead = false;
+
+    for (int n = 0; n < nin; ++n)
+    {
+        const int s = n % kRing;
+        const uint32_t par = (uint32_t)(n / kRing) & 1u;
+        mbarWait(&full[s], par, dead);
+        const int zi = za - 2 + n;
+        if (active)
+        {
+            // output plane of queue slot r: zo = zi - 2 + r
+            bool rv[5];
+#pragma unroll
+            for (int r = 0; r < 5; ++r)
+            {
+                const int zo = zi - 2 + r;
+                rv[r] = zo >= za && zo < zb;
+            }
+            const float *P = &ring[s][0][0][0];
+            unroll<6>([&](auto DY) {
+                constexpr int dy = decltype(DY)::value - 2;
+                float v[6];
+                unroll<6>([&](auto DX) {
+                    constexpr int dx = decltype(DX)::value - 2;
+                    constexpr bool need = tidx(dx, dy, 0) >= 0 || tidx(dx - 1, dy, 0) >= 0 ||
+                                          tidx(dx, dy - 1, 0) >= 0 ||
+                                          tidx(dx - 1, dy - 1, 0) >= 0;
+                    if constexpr (need)
+                        v[dx + 2] = P[((by + dy + 2) * kPW + (bx + dx + 2)) * kMarchChunk + lane];
+                });
+                unroll<5>([&](auto R) {
+                    constexpr int r = decltype(R)::value;
+                    constexpr int dz = 2 - r;
+                    if (rv[r])
+                    {
+                        unroll<6>([&](auto DX) {
+                            constexpr int dx = decltype(DX)::value - 2;
+                            unroll<4>([&](auto C) {
+                                constexpr int c = decltype(C)::value;
+                                constexpr int o = tidx(dx - (c & 1), dy - (c >> 1), dz);
+                                if constexpr (o >= 0)
+                                    acc[c][r] = fmaf(coef[o], v[dx + 2], acc[c][r]);
+                            });
+                        });
+                    }
+                });
+            });
+            // queue slot 0 (zo = zi - 2) is complete
+            if (rv[0] && k < V)
+            {
+                const int zo = zi - 2;
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                {
+                    if (!(mask >> c & 1)) continue;
+                    const int x = ux0 + bx + (c & 1), y = uy0 + by + (c >> 1);
+                    const size_t i = (size_t)x + (size_t)Nx * (y + (size_t)Ny * zo);
+                    out[i * ldf + k] = acc[c][0] * scale;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+#pragma unroll
+                for (int r = 0; r < 4; ++r) acc[c][r] = acc[c][r + 1];
+                acc[c][4] = 0.0f;
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbarArrive(&empty[s]);
+        if (threadIdx.x == 0 && n + kRing < nin)
+        {
+            mbarWait(&empty[s], par, dead);
+            mbarExpectTx(&full[s], kPlaneBytes);
+            tmaLoadPlane(&ring[s][0][0][0], &tmap, &full[s], k0, ux0 - 2, uy0 - 2,
+                         zi + kRing);
+        }
+    }
+    if (dead) atomicOr(&sc->err, 2);
+}
+
+// ---------------------------------------------------------------------------
+// Host side: tensor map over the distribution (dims: velocity, x, y, z).
+// ---------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+
+bool encodeMarchMap(void *tmapOut, void *f, int V, int Nx, int Ny, int Nz, int ldf,
+                    std::string *err)
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn)
+    {
+        cudaDriverEntryPointQueryResult q;
+        void *p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !p)
+        {
+            if (err) *err = "cuTensorMapEncodeTiled is not available";
+            return false;
+        }
+        fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    const cuuint64_t dims[4] = {(cuuint64_t)V, (cuuint64_t)Nx, (cuuint64_t)Ny, (cuuint64_t)Nz};
+    const cuuint64_t strides[3] = {(cuuint64_t)ldf * 4, (cuuint64_t)ldf * 4 * Nx,
+                                   (cuuint64_t)ldf * 4 * Nx * Ny};
+    const cuuint32_t box[4] = {kMarchChunk, kPW, kPH, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = fn(reinterpret_cast<CUtensorMap *>(tmapOut), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                    f, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+    {
+        if (err) *err = "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
+        return false;
+    }
+    return true;
+}
+
+cudaError_t prepareMarch()
+{
+    return cudaFuncSetAttribute(k_march, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(kRing * kPlaneBytes));
+}
+
+cudaError_t launchMarch(alebgk_ctx *c, const void *tmap, float *outBuf, cudaStream_t st)
+{
+    const StepParams &p = c->sp;
+    const CUtensorMap *m = static_cast<const CUtensorMap *>(tmap);
+    dim3 grid(c->march.nunits, c->march.Vpad / kMarchChunk);
+    k_march<<<grid, kMarchWarps * 32, kRing * kPlaneBytes, st>>>(*m, c->march.units,
+                                                                 c->march.coefT, outBuf,
+                                               c->march.Nx, c->march.Ny, p.V, c->march.Vpad,
+                                               p.ldf, c->d.sc);
+    return cudaGetLastError();
+}
+
+}  // namespace alebgk

@@ -1,0 +1,50 @@
+// march.h -- lattice-marching transport plan (internal header).
+//
+// When the cloud is a complete Cartesian lattice in the reference's particle
+// order (i = x + Nx (y + Ny z), Initialization/ParticleGeneration.cpp:119-184)
+// and every neighbour lies within two lattice steps, the transport is a
+// stencil over lattice positions: gt(x,y,z;k) = sum_o C[class][o][k] f(x+o;k)
+// over the 81 offsets |o|^2 <= 6 (self included).  The plan groups lattice
+// columns into work units of class-uniform 2x2 column blocks that march
+// through z.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "coeffs.h"
+
+namespace alebgk {
+
+constexpr int kTmplOffsets = 81;    // (dx,dy,dz) in [-2,2]^3 with |d|^2 <= 6
+constexpr int kMarchTileX = 8;      // CTA column tile
+constexpr int kMarchTileY = 4;
+constexpr int kMarchWarps = 8;      // one 2x2 column block per warp
+constexpr int kMarchChunk = 32;     // velocities per CTA (one per lane)
+
+// Canonical template offset index of (dx, dy, dz), or -1 if outside.
+int templateIndex(int dx, int dy, int dz);
+
+struct MarchUnit
+{
+    int x0, y0, za, zb;   // tile origin (columns) and output planes [za, zb)
+    int nsub;             // active warps
+    int sub[kMarchWarps]; // bx | by << 4 | mask << 8 | class << 12
+};
+
+struct MarchPlan
+{
+    bool ok = false;
+    int Nx = 0, Ny = 0, Nz = 0;
+    int ncls = 0, Vpad = 0;
+    std::vector<MarchUnit> units;
+    std::vector<float> coefT;        // [class][81][Vpad]
+    std::vector<float> coefTLin;     // same, linear MLS
+};
+
+// Detects the lattice and builds the plan; plan.ok is false when the cloud
+// is not a complete lattice with two-step stencils.
+void buildMarchPlan(const double *xyz, int N, int dim, const int *nnb,
+                    const int *nbr, int maxNeigh, const CoeffTables &tb,
+                    const CoeffTables *tl, MarchPlan &plan);
+
+}  // namespace alebgk

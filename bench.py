@@ -257,12 +257,10 @@ def run_ours(args):
     step_ms_prof = sum(stage_ms.values())
     peak, peak_src = measured_peak()
     es = 4 if args.precision == 32 else 8
-    alg_bytes = {"transport": 2 * es, "post_transport": 2 * es, "finalize": 2 * es,
-                 "recollide": 2 * es, "redo": 2 * es}
+    alg_bytes = {"transport": 2 * es, "particle": 2 * es}
     per_update = alg_bytes.get(dominant, 2 * es)
     achieved = per_update * updates / (stage_ms[dominant] / 1e3) / 1e9
-    kern_name = {"transport": "k_transport", "post_transport": "k_post_transport",
-                 "finalize": "k_finalize"}.get(dominant, dominant)
+    kern_name = {"transport": "k_transport", "particle": "k_particle"}.get(dominant, dominant)
     traffic, traffic_src = recorded_traffic(kern_name)
 
     # end to end through the C-ABI with host buffers: every step uploads the
@@ -328,7 +326,7 @@ def run_ours(args):
                    "parallelism": f"{world} independent cavities, one per GPU",
                    "l2": "inputs larger than L2: two 256 MB distribution buffers "
                          "ping-pong, no flush needed"},
-        "gpu_launches": 8 * args.steps,
+        "gpu_launches": 10 * args.steps,
         "stage_ms": {k: round(v, 5) for k, v in stage_ms.items()},
         "roofline": {"bound": "hbm", "kernel": kern_name, "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak,

@@ -63,6 +63,9 @@ typedef struct alebgk_config
     double radius;    /* MLS support h (CalcParameters::radius)               */
     int periodic[3];  /* per-axis periodicity (minimum-image stencils)        */
     double L[3];      /* periodic lengths                                     */
+    int transport;    /* 0 auto (lattice march when the cloud is a complete
+                         lattice and precision is 32, else coefficient
+                         gather), 1 always gather, 2 require the march       */
 } alebgk_config;
 
 /* The host cloud in SoA form.  Inputs for alebgk_upload; the download calls
@@ -95,6 +98,8 @@ typedef struct alebgk_counters
     double mass_scale;        /* global rescale factor applied               */
     double mass_end;          /* sumMass at the end of the step               */
     int error_word;           /* device-side error bits (0 = none)            */
+    int transport_kernel;     /* transport in use: 1 coefficient gather,
+                                 2 lattice march                              */
 } alebgk_counters;
 
 /* ---- context --------------------------------------------------------- */
@@ -158,11 +163,11 @@ int alebgk_step_timed(alebgk_ctx *ctx, int nsteps, float *ms);
 
 /* Runs nsteps steps kernel by kernel (no graph) with a CUDA event between
  * every launch, and returns the summed device time of each stage in
- * ms_per_stage[0..ALEBGK_NSTAGES-1] (transport, particle, sigma, scale_mood,
- * recollide, mass_end, step_begin, unused).
+ * ms_per_stage[0..ALEBGK_NSTAGES-1] (transport, particle, redo, sigma,
+ * fixup, mass_sum, scale_mood, recollide, mass_end, step_begin).
  * Replaces the one-shot [GPU-PROFILE] table of
  * Solver/CudaBackend.cu:1518-1623. */
-#define ALEBGK_NSTAGES 8
+#define ALEBGK_NSTAGES 10
 int alebgk_profile_steps(alebgk_ctx *ctx, int nsteps, float *ms_per_stage);
 
 /* ---- diagnostics ------------------------------------------------------- */
