@@ -6,15 +6,18 @@
 // CTA = one work unit (an 8x4 tile of lattice columns, output planes
 // [za, zb)) x one chunk of 32 velocities, lane = velocity.  The CTA marches
 // through z: every input plane of the tile plus a two-column halo (12x8
-// particles x 32 velocities, 12 KB) is brought into a four-slot shared-
+// particles x 32 velocities, 12 KB) is brought into a six-slot shared-
 // memory ring by one TMA tensor load (cp.async.bulk.tensor.4d, completion on
 // an mbarrier; zero fill outside the lattice).  Each warp owns one
 // class-uniform 2x2 block of columns; its 81 coefficients for its lane's
 // velocity stay in registers for the whole march, and every staged value
 // feeds the FMAs of up to four columns and five output planes, held in a
 // 4 x 5 register queue.  An output plane is complete two input planes after
-// its own and is stored straight from the queue.  Every wait is bounded; a
-// timeout sets the step's error word instead of hanging.
+// its own and is stored straight from the queue.  Thread 0 refills a ring
+// slot two planes after the warps released it, so the warps of a CTA may
+// drift apart by two planes without stalling the loads, which run four
+// planes ahead.  Every wait is bounded; a timeout sets the step's error
+// word instead of hanging.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -30,7 +33,9 @@ namespace {
 
 constexpr int kPW = kMarchTileX + 4;      // staged plane: 12 x 8 particles
 constexpr int kPH = kMarchTileY + 4;
-constexpr int kRing = 4;
+constexpr int kRing = 6;                  // staged planes
+constexpr int kLag = 2;                   // refill lag behind the consumers
+static_assert(kLag < kRing, "ring");
 constexpr uint32_t kPlaneBytes = kPW * kPH * kMarchChunk * 4;
 constexpr long long kSpinLimit = 1ll << 20;
 
@@ -128,6 +133,7 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
     typedef float Plane[kPH][kPW][kMarchChunk];
     Plane *ring = reinterpret_cast<Plane *>(marchSmem);
     __shared__ __align__(8) uint64_t full[kRing], empty[kRing];
+    __shared__ int giveUp;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const MarchUnit &u = units[blockIdx.x];
@@ -138,10 +144,11 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
     const bool active = warp < u.nsub;
     const int sub = active ? __ldg(&u.sub[warp]) : 0;
     const int bx = sub & 15, by = (sub >> 4) & 15, mask = (sub >> 8) & 15, cls = sub >> 12;
-    if (*(volatile int *)&sc->err) return;      // an earlier CTA gave up
-
     if (threadIdx.x == 0)
     {
+        // An earlier CTA that timed out set the error word: skip the work.
+        // Read once and shared, so that every thread of the CTA agrees.
+        giveUp = *(volatile int *)&sc->err;
         for (int s = 0; s < kRing; ++s)
         {
             mbarInit(&full[s], 1);
@@ -150,6 +157,7 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    if (giveUp) return;
     if (threadIdx.x == 0)
         for (int n = 0; n < kRing && n < nin; ++n)
         {
@@ -241,12 +249,15 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
         }
         __syncwarp();
         if (lane == 0) mbarArrive(&empty[s]);
-        if (threadIdx.x == 0 && n + kRing < nin)
+        // Refill the slot of plane m = n - kLag with plane m + kRing.
+        const int m = n - kLag;
+        if (threadIdx.x == 0 && m >= 0 && m + kRing < nin)
         {
-            mbarWait(&empty[s], par, dead);
-            mbarExpectTx(&full[s], kPlaneBytes);
-            tmaLoadPlane(&ring[s][0][0][0], &tmap, &full[s], k0, ux0 - 2, uy0 - 2,
-                         zi + kRing);
+            const int sm = m % kRing;
+            mbarWait(&empty[sm], (uint32_t)(m / kRing) & 1u, dead);
+            mbarExpectTx(&full[sm], kPlaneBytes);
+            tmaLoadPlane(&ring[sm][0][0][0], &tmap, &full[sm], k0, ux0 - 2, uy0 - 2,
+                         za - 2 + m + kRing);
         }
     }
     if (dead) atomicOr(&sc->err, 2);
