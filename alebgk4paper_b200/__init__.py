@@ -206,6 +206,18 @@ class Solver:
         _check(self.lib.alebgk_body_loads(self.ctx, nb, _dp(c), _dp(a), _dp(out)), self.ctx)
         return out
 
+    def body_loads_noalloc(self, centres: np.ndarray, areas: np.ndarray) -> np.ndarray:
+        """Same loads as :meth:`body_loads` from a fixed device scratch, with no
+        device allocation (at most ``_abi.NOALLOC_MAX_BODIES`` bodies; calls that
+        overlap on one device race on the shared scratch)."""
+        nb = len(areas)
+        c = np.ascontiguousarray(centres, np.float64).reshape(nb, 3)
+        a = np.ascontiguousarray(areas, np.float64)
+        out = np.zeros((nb, 6))
+        _check(self.lib.alebgk_body_loads_noalloc(self.ctx, nb, _dp(c), _dp(a), _dp(out)),
+               self.ctx)
+        return out
+
     def cudaFreeCloud(self):
         if getattr(self, "ctx", None):
             self.lib.alebgk_destroy(self.ctx)

@@ -11,6 +11,7 @@ c_int_p = ctypes.POINTER(ctypes.c_int)
 c_double_p = ctypes.POINTER(ctypes.c_double)
 
 MAX_NEIGH = 128
+NOALLOC_MAX_BODIES = 16        # ALEBGK_NOALLOC_MAX_BODIES
 NSTAGES = 10
 STAGES = ("transport", "particle", "redo", "sigma", "fixup", "mass_sum", "scale_mood",
           "recollide", "mass_end", "step_begin")
@@ -77,6 +78,8 @@ SIGNATURES = {
                                            c_int_p, c_int_p]),
     "alebgk_body_loads": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p,
                                          c_double_p, c_double_p]),
+    "alebgk_body_loads_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p,
+                                                 c_double_p, c_double_p]),
     "alebgk_body_set_surface_velocity": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
                                                         c_double_p, c_double_p]),
     "alebgk_case_build": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int,

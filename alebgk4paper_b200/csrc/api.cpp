@@ -523,6 +523,26 @@ int alebgk_body_loads(alebgk_ctx *c, int nbodies, const double *centre,
     return ALEBGK_OK;
 }
 
+int alebgk_body_loads_noalloc(alebgk_ctx *c, int nbodies, const double *centre,
+                              const double *area, double *out)
+{
+    if (!c || !centre || !area || !out) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (nbodies <= 0 || nbodies > ALEBGK_NOALLOC_MAX_BODIES)
+        return fail(c, ALEBGK_EINVAL,
+                    "body loads without allocation take 1.." +
+                        std::to_string(ALEBGK_NOALLOC_MAX_BODIES) + " bodies, got " +
+                        std::to_string(nbodies));
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    for (int i = 0; i < c->sp.N; ++i)
+        if (c->bodyIdHost[i] >= nbodies)
+            return fail(c, ALEBGK_EINVAL, "a particle's body id exceeds nbodies");
+    CK(cudaSetDevice(c->cfg.device));
+    std::string err;
+    if (alebgk::bodyLoadsNoAlloc(c, nbodies, centre, area, out, &err) != cudaSuccess)
+        return fail(c, ALEBGK_ECUDA, err);
+    return ALEBGK_OK;
+}
+
 int alebgk_body_set_surface_velocity(alebgk_ctx *c, int nbodies,
                                      const double *centre, const double *state)
 {

@@ -105,6 +105,10 @@ cudaError_t launchBodyLoads(alebgk_ctx *c, int nbodies, const double *centreDev,
 cudaError_t launchSetSurfaceVelocity(alebgk_ctx *c, int nbodies,
                                      const double *centreDev,
                                      const double *stateDev);
+// Body loads on the fixed device scratch of body_noalloc.cu (no allocation).
+constexpr int kNoAllocMaxBodies = ALEBGK_NOALLOC_MAX_BODIES;
+cudaError_t bodyLoadsNoAlloc(alebgk_ctx *c, int nbodies, const double *centre,
+                             const double *area, double *out, std::string *err);
 cudaError_t launchConvertIn(alebgk_ctx *c, const double *src, int buf);
 cudaError_t launchConvertOut(alebgk_ctx *c, double *dst, int buf);
 cudaError_t launchMarch(alebgk_ctx *c, const void *tmap, float *outBuf, cudaStream_t st);

@@ -200,6 +200,22 @@ int alebgk_device_state(alebgk_ctx *ctx, void **f, int *ldf, int *elem_bytes);
 int alebgk_body_loads(alebgk_ctx *ctx, int nbodies, const double *body_centre,
                       const double *body_area, double *out);
 
+/* The loads of alebgk_body_loads without any device allocation.  No
+ * counterpart in the reference.  For callers that must not allocate: one
+ * that advances several cavities on separate streams of a device (the
+ * cudaFree of the allocating call synchronises the whole device and stalls
+ * every other stream), and one that has reserved the device memory for its
+ * own pools (an allocation could fail mid-run).  Sums run per block and then
+ * over blocks, so results match alebgk_body_loads to rounding, not bitwise.
+ * Limits: 1..ALEBGK_NOALLOC_MAX_BODIES bodies; larger counts return
+ * ALEBGK_EINVAL.  Scratch: one fixed 114,432-byte device array per device,
+ * shared by all contexts on it, so overlapping calls on one device race and
+ * must be serialised by the caller.  The first call on a device looks the
+ * array up and should come before any stream capture. */
+#define ALEBGK_NOALLOC_MAX_BODIES 16
+int alebgk_body_loads_noalloc(alebgk_ctx *ctx, int nbodies, const double *body_centre,
+                              const double *body_area, double *out);
+
 /* Writes the surface wall velocity V + w x r of trial body states onto the
  * surface particles on the device (RigidBody/BodyDynamics.cpp:103-125).
  * state: nbodies*6 (V, w); body_centre: nbodies*3. */
