@@ -102,9 +102,11 @@ class Case:
         finally:
             lib.alebgk_case_free(h)
 
-    def config(self, precision: int = 32, device: int = 0, transport: int = 0) -> _abi.Config:
+    def config(self, precision: int = 32, device: int = 0, transport: int = 0,
+               particle: int = 0) -> _abi.Config:
         cfg = _abi.Config()
         cfg.transport = transport
+        cfg.particle = particle
         cfg.dim, cfg.N, cfg.Nv = self.dim, self.N, self.Nv
         cfg.mls_order, cfg.precision, cfg.limiter = self.mls_order, precision, 2
         cfg.tau_variable, cfg.device = 0, device
@@ -134,13 +136,14 @@ class Solver:
 
     def __init__(self, case: Case, precision: int = 32, device: int = 0,
                  dt: float | None = None, config: _abi.Config | None = None,
-                 transport: int = 0):
+                 transport: int = 0, particle: int = 0):
         self.lib = _abi.load()
         self.case = case
         self.N, self.gstride, self.dim = case.N, case.gstride, case.dim
         self.precision = precision
         self.dt = float(dt if dt is not None else case.dt)
-        cfg = config if config is not None else case.config(precision, device, transport)
+        cfg = config if config is not None else case.config(precision, device, transport,
+                                                              particle)
         self.cfg = cfg
         h = ctypes.c_void_p()
         _check(self.lib.alebgk_create(ctypes.byref(cfg), ctypes.byref(h)))

@@ -27,7 +27,7 @@ class Config(ctypes.Structure):
         ("R", ctypes.c_double), ("tau", ctypes.c_double), ("dHS", ctypes.c_double),
         ("vmin", ctypes.c_double), ("dv", ctypes.c_double), ("radius", ctypes.c_double),
         ("periodic", ctypes.c_int * 3), ("L", ctypes.c_double * 3),
-        ("transport", ctypes.c_int),
+        ("transport", ctypes.c_int), ("particle", ctypes.c_int),
     ]
 
 
@@ -47,6 +47,7 @@ class Counters(ctypes.Structure):
         ("mass_before", ctypes.c_double), ("mass_after_transport", ctypes.c_double),
         ("mass_scale", ctypes.c_double), ("mass_end", ctypes.c_double),
         ("error_word", ctypes.c_int), ("transport_kernel", ctypes.c_int),
+        ("particle_kernel", ctypes.c_int),
     ]
 
 

@@ -20,7 +20,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libalebgk_b200.so")
 
 SOURCES = ["step.cu", "march.cu", "body_noalloc.cu", "api.cpp", "coeffs.cpp", "cases.cpp", "march_plan.cpp"]
-HEADERS = ["ctx.h", "coeffs.h", "cases.h", "march.h"]
+HEADERS = ["ctx.h", "coeffs.h", "cases.h", "march.h", "mbar.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

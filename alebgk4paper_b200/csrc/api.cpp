@@ -44,7 +44,7 @@ void freeBuffers(alebgk_ctx *c)
     DeviceBuffers &d = c->d;
     void *ptrs[] = {d.f[0], d.f[1], d.coef, d.coefLin, d.pos, d.meshv, d.wall,
                     d.boundary, d.bodyId, d.cls, d.nslot, d.slots, d.macro[0],
-                    d.macro[1], d.mood, d.flag, d.flagList, d.degList, d.massPos, d.massEnd, d.minG,
+                    d.macro[1], d.mood, d.flag, d.flagList, d.degList, d.massPos, d.massEnd, d.minG, d.nad,
                     d.dpx, d.bodyTmp, d.bodyOut, d.stage, d.sc};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -76,6 +76,8 @@ int alebgk_create(const alebgk_config *cfg, alebgk_ctx **out)
         return fail(nullptr, ALEBGK_EINVAL, "mls_order must be 1 or 2");
     if (cfg->limiter != 0 && cfg->limiter != 2)
         return fail(nullptr, ALEBGK_EINVAL, "limiter must be 0 (none) or 2 (MOOD)");
+    if (cfg->transport < 0 || cfg->transport > 2 || cfg->particle < 0 || cfg->particle > 2)
+        return fail(nullptr, ALEBGK_EINVAL, "transport and particle selectors are 0, 1 or 2");
     if (!(cfg->tau > 0) || !(cfg->R > 0) || !(cfg->dv > 0) || !(cfg->radius > 0))
         return fail(nullptr, ALEBGK_EINVAL, "tau, R, dv and radius must be > 0");
     const int gs = (cfg->dim == 3) ? cfg->Nv * cfg->Nv * cfg->Nv : 2 * cfg->Nv * cfg->Nv;
@@ -150,6 +152,9 @@ int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
     freeBuffers(c);
     StepParams &p = c->sp;
     p.dt = dt;
+    p.lam = dt / p.tau;
+    p.c1 = 1.0 / (1.0 + p.lam);
+    p.inv3R = 1.0 / (3.0 * p.R);
     const int N = p.N;
     for (int i = 0; i < N; ++i)
     {
@@ -226,6 +231,7 @@ int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
     CK(dalloc(&d.massPos, N));
     CK(dalloc(&d.massEnd, N));
     CK(dalloc(&d.minG, N));
+    CK(dalloc(&d.nad, 2 * (size_t)N));
     CK(dalloc(&d.dpx, N));
     CK(dalloc(&d.bodyTmp, 6 * (size_t)N));
     CK(dalloc(&d.bodyOut, 64 * 6));
@@ -242,6 +248,10 @@ int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
     CK(cudaMemset(d.dpx, 0, 8 * (size_t)N));
     CK(cudaMemset(d.sc, 0, sizeof(StepScalars)));
     CK(prepareKernels(c));
+    if (c->cfg.particle == 2 && !c->pStream)
+        return fail(c, ALEBGK_EINVAL,
+                    "the streamed particle kernel needs a 3-D cloud whose rows fit in "
+                    "shared memory");
     // Lattice-marching transport (FP32, complete 3-D lattice).
     if (!f64 && c->cfg.transport != 1)
     {
@@ -463,6 +473,7 @@ int alebgk_get_counters(alebgk_ctx *c, alebgk_counters *out)
     out->mass_before = s.sigma * s.massNew;
     out->error_word = s.err;
     out->transport_kernel = c->march.enabled ? 2 : 1;
+    out->particle_kernel = c->pStream ? 2 : 1;
     return ALEBGK_OK;
 }
 

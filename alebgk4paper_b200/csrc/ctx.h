@@ -60,6 +60,7 @@ struct DeviceBuffers
     double *massPos = nullptr;         // per particle: mass after positivity (true)
     double *massEnd = nullptr;         // per particle: mass of h at step end
     double *minG = nullptr;            // per particle: min of h over the mass layer
+    double *nad = nullptr;             // per particle: NAD neighbour density range (lo, hi)
     double *dpx = nullptr;
     double *bodyTmp = nullptr;         // N x 6 per-particle load contributions
     double *bodyOut = nullptr;         // up to 64 bodies x 6
@@ -74,6 +75,7 @@ struct StepParams
     int periodic[3] = {0, 0, 0};
     double Lp[3] = {0, 0, 0};
     double R = 208, tau = 1, dHS = 0, vmin = 0, dv = 0, dvN = 0, h = 0, dt = 0;
+    double lam = 0, c1 = 1, inv3R = 0;   // dt/tau, 1/(1+lam), 1/(3R) for this dt
 };
 
 }  // namespace alebgk
@@ -90,6 +92,10 @@ struct alebgk_ctx
     int ncls = 0;
     int degenerateParticles = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    // Streamed particle kernel: on, warps per block, blocks, dynamic smem.
+    bool pStream = false;
+    int pStreamWpb = 0, pStreamBlocks = 0;
+    size_t pStreamSmem = 0;
     std::string err;
     std::vector<int> bodyIdHost;
 };

@@ -26,6 +26,7 @@
 
 #include "ctx.h"
 #include "march.h"
+#include "mbar.cuh"
 
 namespace alebgk {
 
@@ -37,7 +38,6 @@ constexpr int kRing = 6;                  // staged planes
 constexpr int kLag = 2;                   // refill lag behind the consumers
 static_assert(kLag < kRing, "ring");
 constexpr uint32_t kPlaneBytes = kPW * kPH * kMarchChunk * 4;
-constexpr long long kSpinLimit = 1ll << 20;
 
 __host__ __device__ constexpr int tidx(int dx, int dy, int dz)
 {
@@ -63,52 +63,6 @@ template <int N, typename F>
 __device__ __forceinline__ void unroll(F &&f)
 {
     unrollImpl(std::make_integer_sequence<int, N>{}, f);
-}
-
-__device__ __forceinline__ uint32_t smemAddr(const void *p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbarInit(uint64_t *bar, int count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbarExpectTx(uint64_t *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void mbarArrive(uint64_t *bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smemAddr(bar)) : "memory");
-}
-
-__device__ __forceinline__ bool mbarTryWait(uint64_t *bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smemAddr(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait on an mbarrier phase.  After kSpinLimit polls the wait gives
-// up and marks the CTA dead; a dead CTA does not wait again, so a broken
-// pipeline costs one timeout, not one per plane.
-__device__ __forceinline__ bool mbarWait(uint64_t *bar, uint32_t parity, bool &dead)
-{
-    if (dead) return false;
-    for (long long it = 0; it < kSpinLimit; ++it)
-        if (mbarTryWait(bar, parity)) return true;
-    dead = true;
-    return false;
 }
 
 __device__ __forceinline__ void tmaLoadPlane(void *dst, const CUtensorMap *map, uint64_t *bar,
@@ -154,7 +108,7 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
             mbarInit(&full[s], 1);
             mbarInit(&empty[s], kMarchWarps);
         }
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        mbarInitFence();
     }
     __syncthreads();
     if (giveUp) return;

@@ -1,9 +1,11 @@
 // step.cu -- device kernels of the ALE-BGK time step for sm_100a.
 //
 // One step (the CPU step order of Solver/Solver.cpp:632-705):
-//   k_step_begin      reset the step's counters
+//   k_step_begin      reset the step's counters (and the NAD neighbour ranges
+//                     of the streamed particle kernel)
 //   k_transport       gt[i][k] = scale * sum_s coef[class][s][k] * h[slot s][k]
-//   k_particle        per particle (one warp): positivity repair, MOOD PAD/NAD
+//   k_particle        per particle (one warp; k_particle_stream for 3-D clouds):
+//                     positivity repair, MOOD PAD/NAD
 //                     screen with linear redo, diffuse wall or moments + BGK
 //                     collision + moments, without the global rescale
 //   k_sigma           deterministic mass sums -> global rescale sigma
@@ -18,6 +20,7 @@
 #include <cmath>
 
 #include "ctx.h"
+#include "mbar.cuh"
 
 namespace alebgk {
 
@@ -219,6 +222,7 @@ struct ParticleArgs
     const int *boundary, *cls, *nslot, *slots;
     const double *wall, *macPrev;
     double *macNew, *massPos, *massEnd, *minG, *dpx;
+    const double *nad;        // NAD neighbour density range (lo, hi) per particle
     int *flag, *flagList, *degList;
     StepScalars *sc;
 };
@@ -240,6 +244,11 @@ struct RowRegs
 #pragma unroll 8
         for (int k = lane; k < n; k += 32) buf[k] = row[k];
         __syncwarp();
+    }
+    // Over a copy that is already staged in buf.
+    __device__ RowRegs(T *row_, T *buf_, const StepParams &p, int lane_, bool)
+        : buf(buf_), row(row_), V(p.V), lane(lane_)
+    {
     }
     // Calls f(k, iv, jv, kv, g1&, g2&) for every node of the row.
     template <typename F>
@@ -483,6 +492,451 @@ k_particle(ParticleArgs<T> a, StepParams p, int warpsPerBlock)
     }
     if (flagged) return;
     finishParticle(a, p, i, r, pv, tab[warp]);
+}
+
+// ---------------------------------------------------------------------------
+// The same stages for a 3-D single-layer cloud, streamed: persistent warps
+// take particles i = w, w + W, ...; each warp double-buffers its particles'
+// rows in shared memory with one bulk copy per row (the next row is in
+// flight while the current one is processed).  Per node the velocity
+// (vx, vy, vz, |v|^2) and the grid indices come from tables built once per
+// block, and the NAD neighbour density range comes from k_step_begin.  An
+// interior row takes two passes:
+//   1. positivity sums and the moments of the row,
+//   2. the implicit BGK collision h = (g + lam M) / (1 + lam), written out.
+// The post-collision moments are not summed over the row: by linearity they
+// are c1 (moments of g + lam * moments of M), and the moments of the
+// separable discrete Maxwellian are products of per-axis sums over Nv nodes
+// (Collision.cpp:70-139 then Moments.cpp:17-97 give the same numbers up to
+// rounding).  Each lane sums its nodes in the storage type T -- at most
+// ceil(V/32) terms -- and the lanes' sums are combined in FP64.  Wall
+// particles take finishParticle on the staged row.
+// ---------------------------------------------------------------------------
+
+// Node velocity table of the streamed kernel, in the storage type.
+template <typename T> struct VelNode;
+template <> struct __align__(16) VelNode<float>
+{
+    float vx, vy, vz, v2;
+};
+template <> struct __align__(16) VelNode<double>
+{
+    double vx, vy, vz, v2;
+};
+
+// Shared-memory layout of k_particle_stream: velocity table, node index
+// table, then two rows per warp.
+template <typename T>
+__host__ __device__ inline size_t streamRowsOffset(int V)
+{
+    return ((size_t)V * (sizeof(VelNode<T>) + sizeof(int)) + 127) / 128 * 128;
+}
+
+template <typename T>
+__host__ __device__ inline size_t streamSmemBytes(int V, int ldf, int wpb)
+{
+    return streamRowsOffset<T>(V) + (size_t)wpb * 2 * ldf * sizeof(T);
+}
+
+// Sums K <= 8 values over the warp with 9 shuffle rounds instead of 5K:
+// each round halves the set a lane keeps and adds its partner's other half.
+// Every lane receives all K totals.
+template <int K>
+__device__ __forceinline__ void warpSumMany(double (&v)[K], int lane)
+{
+    static_assert(K >= 1 && K <= 8, "up to eight values");
+    double w[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) w[q] = q < K ? v[q] : 0.0;
+#pragma unroll
+    for (int half = 4, bit = 16; half >= 1; half >>= 1, bit >>= 1)
+    {
+        const bool up = (lane & bit) != 0;
+#pragma unroll
+        for (int q = 0; q < half; ++q)
+        {
+            const double keep = up ? w[q + half] : w[q];
+            const double give = up ? w[q] : w[q + half];
+            w[q] = keep + __shfl_xor_sync(0xffffffffu, give, bit);
+        }
+    }
+    // w[0] now holds value index (b4 b3 b2 of the lane) summed over the lanes
+    // that share those bits; finish over bits 1 and 0.
+    w[0] += __shfl_xor_sync(0xffffffffu, w[0], 2);
+    w[0] += __shfl_xor_sync(0xffffffffu, w[0], 1);
+#pragma unroll
+    for (int q = 0; q < K; ++q)
+    {
+        const int src = ((q >> 2) & 1) << 4 | ((q >> 1) & 1) << 3 | (q & 1) << 2;
+        v[q] = __shfl_sync(0xffffffffu, w[0], src);
+    }
+}
+
+// NAD neighbour density range of every interior particle
+// (MLSTransport.cpp:325-379) from the previous step's macros, one warp per
+// particle; the streamed particle kernel reads it instead of gathering.
+__device__ void nadRanges(const double *__restrict__ macPrev, const int *__restrict__ boundary,
+                          const int *__restrict__ nslot, const int *__restrict__ slots,
+                          int S, int N, double *__restrict__ nad)
+{
+    const int lane = threadIdx.x & 31;
+    const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int i = w0; i < N; i += nw)
+    {
+        if (boundary[i]) continue;
+        double lo = INFINITY, hi = -INFINITY;
+        const int ns = nslot[i];
+        const int *sl = slots + (size_t)i * S;
+        for (int s = 1 + lane; s < ns; s += 32)
+        {
+            const double rr = macPrev[6 * (size_t)sl[s]];
+            lo = fmin(lo, rr);
+            hi = fmax(hi, rr);
+        }
+        lo = warpMin(lo);
+        hi = warpMax(hi);
+        if (lane == 0)
+        {
+            nad[2 * (size_t)i] = lo;
+            nad[2 * (size_t)i + 1] = hi;
+        }
+    }
+}
+
+// Diffuse wall (BoundaryConditions/DiffuseWall.cpp:19-154) of a staged 3-D
+// row, as finishParticle's wall branch computes it, with the node velocities
+// read from the exact FP64 per-axis table velD and no divergent branches.
+// The wall-normal velocity keeps the reference's contracted form (bcCn),
+// which decides the cn = 0 ties.
+template <typename T>
+__device__ __forceinline__ void finishWallStream(const ParticleArgs<T> &a, const StepParams &p,
+                                                 int i, const T *row, const int *idxT,
+                                                 const double *velD, const Positivity &pv,
+                                                 double (*tb)[kMaxNv], int lane)
+{
+    const double *w = a.wall + 7 * (size_t)i;
+    const double Ux = w[3], Uy = w[4], Uz = w[5], Tw = w[6];
+    const double RT2w = 2.0 * p.R * Tw;
+    const double norm = pow(kPi * RT2w, 1.5);
+    const double dvN = p.dvN;
+    for (int q = lane; q < p.Nv; q += 32)
+    {
+        const double va = velD[q];
+        tb[0][q] = exp(-(va - Ux) * (va - Ux) / RT2w) / norm;
+        tb[1][q] = exp(-(va - Uy) * (va - Uy) / RT2w);
+        tb[2][q] = exp(-(va - Uz) * (va - Uz) / RT2w);
+    }
+    __syncwarp();
+    double iM[2] = {0, 0}, iP[2] = {0, 0};
+    auto passA = [&](int u, int k) {
+        const int id = idxT[k];
+        const int iv = id & 255, jv = (id >> 8) & 255, kv = id >> 16;
+        const double cn = bcCn(3, velD[iv], velD[jv], velD[kv], w);
+        const double x = pv.v1((double)row[k]);
+        const double mw = tb[0][iv] * tb[1][jv] * tb[2][kv];
+        iM[u] += cn < 0.0 ? cn * x * dvN : 0.0;
+        iP[u] += cn > 0.0 ? cn * mw * dvN : 0.0;
+    };
+    int k1 = lane;
+#pragma unroll 2
+    for (; k1 + 32 < p.V; k1 += 64)
+    {
+        passA(0, k1);
+        passA(1, k1 + 32);
+    }
+    if (k1 < p.V) passA(0, k1);
+    double r[2] = {iM[0] + iM[1], iP[0] + iP[1]};
+    warpSumMany<2>(r, lane);
+    const double rhow = (r[1] > 1.0e-30) ? (-r[0] / r[1]) : 1.0;
+    T *gout = a.g + (size_t)i * p.ldf;
+    double dp[2] = {0, 0}, ms[2] = {0, 0};
+    auto passB = [&](int u, int k) {
+        const int id = idxT[k];
+        const int iv = id & 255, jv = (id >> 8) & 255, kv = id >> 16;
+        const double vx = velD[iv];
+        const double cn = bcCn(3, vx, velD[jv], velD[kv], w);
+        const double h1 = pv.v1((double)row[k]);
+        const double Mw = rhow * (tb[0][iv] * tb[1][jv] * tb[2][kv]);
+        dp[u] += cn > 0.0 ? vx * (Mw - h1) * dvN : 0.0;
+        const T g1 = T(cn > 0.0 ? Mw : h1);
+        gout[k] = g1;
+        ms[u] += (double)g1;
+    };
+    k1 = lane;
+#pragma unroll 2
+    for (; k1 + 32 < p.V; k1 += 64)
+    {
+        passB(0, k1);
+        passB(1, k1 + 32);
+    }
+    if (k1 < p.V) passB(0, k1);
+    double r2[2] = {dp[0] + dp[1], ms[0] + ms[1]};
+    warpSumMany<2>(r2, lane);
+    if (lane == 0)
+    {
+        double *mac = a.macNew + 6 * (size_t)i;
+        mac[0] = rhow; mac[1] = Ux; mac[2] = Uy; mac[3] = Uz;
+        mac[4] = Tw; mac[5] = rhow * p.R * Tw;
+        a.dpx[i] = r2[0];
+        a.massEnd[i] = r2[1] * dvN;
+        a.minG[i] = 0.0;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kNT)
+k_particle_stream(ParticleArgs<T> a, StepParams p, int wpb)
+{
+    __shared__ double tab[kNT / 32][3][kMaxNv];
+    __shared__ float tabF[kNT / 32][sizeof(T) == 4 ? 3 : 1][kMaxNv];
+    __shared__ double velD[kMaxNv];
+    __shared__ __align__(8) uint64_t full[kNT / 32][2];
+    extern __shared__ __align__(128) unsigned char streamSmem[];
+    VelNode<T> *velT = reinterpret_cast<VelNode<T> *>(streamSmem);
+    int *idxT = reinterpret_cast<int *>(velT + p.V);
+    T *rows = reinterpret_cast<T *>(streamSmem + streamRowsOffset<T>(p.V));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int V = p.V, Nv = p.Nv;
+
+    for (int k = threadIdx.x; k < V; k += blockDim.x)
+    {
+        const int iv = k % Nv, jv = (k / Nv) % Nv, kv = k / (Nv * Nv);
+        const double vx = fma((double)iv, p.dv, p.vmin);
+        const double vy = fma((double)jv, p.dv, p.vmin);
+        const double vz = fma((double)kv, p.dv, p.vmin);
+        velT[k] = VelNode<T>{T(vx), T(vy), T(vz), T(vx * vx + vy * vy + vz * vz)};
+        idxT[k] = iv | jv << 8 | kv << 16;
+    }
+    for (int q = threadIdx.x; q < Nv; q += blockDim.x) velD[q] = fma((double)q, p.dv, p.vmin);
+    if (lane == 0 && warp < wpb)
+    {
+        mbarInit(&full[warp][0], 1);
+        mbarInit(&full[warp][1], 1);
+        mbarInitFence();
+    }
+    __syncthreads();
+    if (warp >= wpb) return;
+
+    const int W = gridDim.x * wpb;
+    int i = blockIdx.x * wpb + warp;
+    auto rb = [&](int b) { return rows + (size_t)(2 * warp + b) * p.ldf; };
+    const uint32_t rowBytes = (uint32_t)(p.ldf * sizeof(T));
+    if (lane == 0 && i < p.N)
+    {
+        mbarExpectTx(&full[warp][0], rowBytes);
+        bulkLoad(rb(0), a.g + (size_t)i * p.ldf, rowBytes, &full[warp][0]);
+    }
+    double(*tb)[kMaxNv] = tab[warp];
+    // Maxwellian factors in T for the node loop: the double table itself,
+    // or the warp's single-precision copy.
+    T(*tt)[kMaxNv] = sizeof(T) == 4 ? reinterpret_cast<T(*)[kMaxNv]>(&tabF[warp][0][0])
+                                    : reinterpret_cast<T(*)[kMaxNv]>(&tb[0][0]);
+    const double dvN = p.dvN;
+    bool dead = false;
+
+    for (int it = 0; i < p.N; ++it, i += W)
+    {
+        const int b = it & 1;
+        const int inext = i + W;
+        if (lane == 0 && inext < p.N)
+        {
+            fenceProxyAsync();     // the warp's accesses to rb(b ^ 1) are done
+            mbarExpectTx(&full[warp][b ^ 1], rowBytes);
+            bulkLoad(rb(b ^ 1), a.g + (size_t)inext * p.ldf, rowBytes, &full[warp][b ^ 1]);
+        }
+        // Independent loads, first used after pass 1.
+        const int wallI = a.boundary[i];
+        const double2 nadI = p.limiter == 2 ? reinterpret_cast<const double2 *>(a.nad)[i]
+                                            : make_double2(INFINITY, -INFINITY);
+
+        mbarWait(&full[warp][b], (uint32_t)(it >> 1) & 1u, dead);
+        if (__any_sync(0xffffffffu, dead))
+        {
+            // The row never arrived: report, let the other copy land, stop.
+            if (lane == 0)
+            {
+                atomicOr(&a.sc->err, 4);
+                bool d2 = false;
+                if (inext < p.N) mbarWait(&full[warp][b ^ 1], (uint32_t)((it + 1) >> 1) & 1u, d2);
+            }
+            __syncwarp();
+            return;
+        }
+        const T *row = rb(b);
+
+        // Pass 1: positivity sums and moments of the transported row, two
+        // interleaved partial sums per quantity.
+        T s0[4] = {0, 0, 0, 0}, sn[4] = {0, 0, 0, 0}, mx[4] = {0, 0, 0, 0},
+          my[4] = {0, 0, 0, 0}, mz[4] = {0, 0, 0, 0}, me[4] = {0, 0, 0, 0};
+        auto acc = [&](int u, int k) {
+            const T x = row[k];
+            const VelNode<T> v = velT[k];
+            s0[u] += x;
+            sn[u] += x < T(0) ? x : T(0);
+            mx[u] = fma(v.vx, x, mx[u]);
+            my[u] = fma(v.vy, x, my[u]);
+            mz[u] = fma(v.vz, x, mz[u]);
+            me[u] = fma(v.v2, x, me[u]);
+        };
+        int k1 = lane;
+        for (; k1 + 96 < V; k1 += 128)
+        {
+            acc(0, k1);
+            acc(1, k1 + 32);
+            acc(2, k1 + 64);
+            acc(3, k1 + 96);
+        }
+        if (k1 < V) acc(0, k1);
+        if (k1 + 32 < V) acc(1, k1 + 32);
+        if (k1 + 64 < V) acc(2, k1 + 64);
+        auto sum4 = [](const T (&v)[4]) {
+            return ((double)v[0] + (double)v[1]) + ((double)v[2] + (double)v[3]);
+        };
+        double r1[6] = {sum4(s0), sum4(sn), sum4(mx), sum4(my), sum4(mz), sum4(me)};
+        warpSumMany<6>(r1, lane);
+        const bool wallP = wallI != 0;
+        const bool screenP = p.limiter == 2 && !wallP;
+        const double lo = nadI.x, hi = nadI.y;
+        const bool bad = !isfinite(r1[0]) || !isfinite(r1[1]);
+        const double pos = r1[0] - r1[1], neg = r1[1];
+        const double m = pos + neg;
+        const Positivity pv(pos, neg);
+        int flagged = 0;
+        if (screenP)
+        {
+            if (bad || m <= 0.0) flagged = 1;
+            else if (isfinite(lo) && isfinite(hi))
+            {
+                const double rn = m * dvN;
+                const double slack = 0.1 * fmax(hi - lo, 1.0e-12) + 1.0e-9;
+                flagged = (rn < lo - slack || rn > hi + slack);
+            }
+        }
+        if (lane == 0)
+        {
+            a.flag[i] = flagged;
+            if (pv.fix) atomicAdd(&a.sc->nfix, 1);
+            if (flagged) a.flagList[atomicAdd(&a.sc->nflag, 1)] = i;
+            else a.massPos[i] = m * dvN;
+        }
+        if (flagged)
+        {
+            __syncwarp();
+            continue;
+        }
+        if (wallP)
+        {
+            finishWallStream(a, p, i, row, idxT, velD, pv, tb, lane);
+            __syncwarp();
+            continue;
+        }
+
+        // Moments of the repaired row (Moments.cpp:17-97).
+        double M0 = r1[0] * dvN, Mx = r1[2] * dvN, My = r1[3] * dvN, Mz = r1[4] * dvN,
+               ME = r1[5] * dvN;
+        if (pv.fix)
+        {
+            // Rare: the repair zeroes the negative nodes and scales the rest,
+            // so the repaired moments are s times those of the positive part.
+            T q[5] = {0, 0, 0, 0, 0};
+            for (int k = lane; k < V; k += 32)
+            {
+                const T x = row[k] < T(0) ? T(0) : row[k];
+                const VelNode<T> v = velT[k];
+                q[0] += x;
+                q[1] = fma(v.vx, x, q[1]);
+                q[2] = fma(v.vy, x, q[2]);
+                q[3] = fma(v.vz, x, q[3]);
+                q[4] = fma(v.v2, x, q[4]);
+            }
+            double r2[5] = {(double)q[0], (double)q[1], (double)q[2], (double)q[3], (double)q[4]};
+            warpSumMany<5>(r2, lane);
+            const double f = pv.s * dvN;
+            M0 = r2[0] * f; Mx = r2[1] * f; My = r2[2] * f; Mz = r2[3] * f; ME = r2[4] * f;
+        }
+        if (!(M0 > 1.0e-30) || p.tauVar)
+        {
+            if (lane == 0) a.degList[atomicAdd(&a.sc->ndeg, 1)] = i;
+            __syncwarp();
+            continue;
+        }
+        const double iM0 = 1.0 / M0;
+        const double rho = M0, ux = Mx * iM0, uy = My * iM0, uz = Mz * iM0;
+        const double Tt = fmax((ME * iM0 - (ux * ux + uy * uy + uz * uz)) * p.inv3R, 1.0e-6);
+        const double lam = p.lam, c1 = p.c1;
+        const double twoRT = 2.0 * p.R * Tt;
+        const double piT = kPi * twoRT;
+        const double A = rho / (piT * sqrt(piT));
+        const double i2RT = 1.0 / twoRT;
+
+        // Per-axis Maxwellian factors, one (axis, node) per lane, in FP64 and
+        // in T for the node loop; then lane 3d + m sums velocity^m times the
+        // axis-d factors over the Nv nodes.
+        for (int j = lane; j < 3 * Nv; j += 32)
+        {
+            const int d = j / Nv, q = j - d * Nv;
+            const double va = velD[q];
+            const double u = d == 0 ? ux : (d == 1 ? uy : uz);
+            const double e = (d == 0 ? lam * A : 1.0) * exp(-(va - u) * (va - u) * i2RT);
+            tb[d][q] = e;
+            tt[d][q] = T(e);
+        }
+        __syncwarp();
+        double Sl = 0.0;
+        if (lane < 9)
+        {
+            const int d = lane / 3, mom = lane - 3 * d;
+            for (int q = 0; q < Nv; ++q)
+            {
+                const double va = velD[q], e = tb[d][q];
+                Sl += mom == 0 ? e : (mom == 1 ? va * e : va * va * e);
+            }
+        }
+        double S[9];
+#pragma unroll
+        for (int j = 0; j < 9; ++j) S[j] = __shfl_sync(0xffffffffu, Sl, j);
+
+        // Pass 2: collision, written straight to the distribution.
+        T *gout = a.g + (size_t)i * p.ldf;
+        const T c1t = T(c1), st = T(pv.s);
+        T mn = T(INFINITY);
+#pragma unroll 8
+        for (int k = lane; k < V; k += 32)
+        {
+            const int id = idxT[k];
+            const T lM = tt[0][id & 255] * tt[1][(id >> 8) & 255] * tt[2][id >> 16];
+            T x = row[k];
+            if (pv.fix) x = x < T(0) ? T(0) : x * st;
+            const T h = c1t * (x + lM);
+            mn = mn < h ? mn : h;
+            gout[k] = h;
+        }
+        const double mnd = warpMin((double)mn);
+        if (lane == 0)
+        {
+            const double N0 = c1 * (M0 + dvN * S[0] * S[3] * S[6]);
+            const double Nx = c1 * (Mx + dvN * S[1] * S[3] * S[6]);
+            const double Ny = c1 * (My + dvN * S[0] * S[4] * S[6]);
+            const double Nz = c1 * (Mz + dvN * S[0] * S[3] * S[7]);
+            const double NE = c1 * (ME + dvN * (S[2] * S[3] * S[6] + S[0] * S[5] * S[6] +
+                                                S[0] * S[3] * S[8]));
+            double r2 = rho, x2 = ux, y2 = uy, z2 = uz, T2 = Tt;
+            if (N0 > 1.0e-30)
+            {
+                const double iN0 = 1.0 / N0;
+                r2 = N0; x2 = Nx * iN0; y2 = Ny * iN0; z2 = Nz * iN0;
+                T2 = fmax((NE * iN0 - (x2 * x2 + y2 * y2 + z2 * z2)) * p.inv3R, 1.0e-6);
+            }
+            double *mac = a.macNew + 6 * (size_t)i;
+            mac[0] = r2; mac[1] = x2; mac[2] = y2; mac[3] = z2; mac[4] = T2;
+            mac[5] = r2 * p.R * T2;
+            a.dpx[i] = 0.0;
+            a.massEnd[i] = N0;
+            a.minG[i] = mnd;
+        }
+        __syncwarp();
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -789,12 +1243,21 @@ k_mass_end(const double *__restrict__ massEnd, int N, StepScalars *sc)
     }
 }
 
-__global__ void k_step_begin(StepScalars *sc)
+// Resets the step's counters; with a NAD range buffer also computes the
+// neighbour density ranges of the streamed particle kernel.
+__global__ void __launch_bounds__(kNT)
+k_step_begin(StepScalars *sc, const double *__restrict__ macPrev,
+             const int *__restrict__ boundary, const int *__restrict__ nslot,
+             const int *__restrict__ slots, int S, int N, double *__restrict__ nad)
 {
-    sc->nflag = 0;
-    sc->ndeg = 0;
-    sc->nfix = 0;
-    sc->moodfail = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+    {
+        sc->nflag = 0;
+        sc->ndeg = 0;
+        sc->nfix = 0;
+        sc->moodfail = 0;
+    }
+    if (nad) nadRanges(macPrev, boundary, nslot, slots, S, N, nad);
 }
 
 // Particle masses of an uploaded state (scale 1).
@@ -977,12 +1440,15 @@ static cudaError_t stepT(alebgk_ctx *c, int from, cudaEvent_t *ev)
     pa.wall = d.wall; pa.macPrev = macA; pa.macNew = macB;
     pa.massPos = d.massPos; pa.massEnd = d.massEnd; pa.minG = d.minG; pa.dpx = d.dpx;
     pa.flag = d.flag; pa.flagList = d.flagList; pa.degList = d.degList; pa.sc = d.sc;
+    pa.nad = d.nad;
     int q = 0;
     auto mark = [&]() { if (ev) cudaEventRecord(ev[q++], st); };
     const int pBlocks = (p.N + kNT / 32 - 1) / (kNT / 32);
     const int listBlocks = min(p.N, 1184);
     mark();
-    k_step_begin<<<1, 1, 0, st>>>(d.sc);
+    const bool nadOn = c->pStream && p.limiter == 2;
+    k_step_begin<<<nadOn ? min((p.N + kNT / 32 - 1) / (kNT / 32), 1184) : 1, kNT, 0, st>>>(
+        d.sc, macA, d.boundary, d.nslot, d.slots, p.S, p.N, nadOn ? d.nad : nullptr);
     mark();
     if (sizeof(T) == 4 && c->march.enabled)
     {
@@ -1000,7 +1466,10 @@ static cudaError_t stepT(alebgk_ctx *c, int from, cudaEvent_t *ev)
     const size_t rowBytes = (size_t)p.L * p.V * sizeof(T);
     const int wpb = particleWarpsPerBlock(p, sizeof(T));
     const int ppBlocks = (p.N + wpb - 1) / wpb;
-    if (p.L == 2) k_particle<T, 2><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
+    if (c->pStream)
+        k_particle_stream<T><<<c->pStreamBlocks, kNT, c->pStreamSmem, st>>>(pa, p,
+                                                                          c->pStreamWpb);
+    else if (p.L == 2) k_particle<T, 2><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
     else k_particle<T, 1><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
     mark();
     if (p.L == 2) k_redo<T, 2><<<listBlocks, kNT, rowBytes, st>>>(pa, p);
@@ -1037,6 +1506,35 @@ static cudaError_t prepareT(alebgk_ctx *c)
     set((const void *)k_particle<T, 2>, wpb * rowBytes);
     set((const void *)k_redo<T, 1>, rowBytes);
     set((const void *)k_redo<T, 2>, rowBytes);
+
+    // Streamed particle kernel: 3-D single layer, two rows per warp, at
+    // least four warps per block in 200 KB of shared memory.
+    c->pStream = false;
+    if (e == cudaSuccess && p.dim == 3 && p.L == 1 && p.Nv <= 255 && c->cfg.particle != 1)
+    {
+        int w = kNT / 32;
+        while (w >= 4 && streamSmemBytes<T>(p.V, p.ldf, w) > 200u * 1024u) --w;
+        if (w >= 4)
+        {
+            const size_t smem = streamSmemBytes<T>(p.V, p.ldf, w);
+            set((const void *)k_particle_stream<T>, smem);
+            int occ = 0, sms = 0, dev = 0;
+            if (e == cudaSuccess) e = cudaGetDevice(&dev);
+            if (e == cudaSuccess)
+                e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (e == cudaSuccess)
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &occ, k_particle_stream<T>, kNT, smem);
+            if (e == cudaSuccess && occ > 0)
+            {
+                const int need = (p.N + w - 1) / w;
+                c->pStream = true;
+                c->pStreamWpb = w;
+                c->pStreamSmem = smem;
+                c->pStreamBlocks = need < sms * occ ? need : sms * occ;
+            }
+        }
+    }
     return e;
 }
 

@@ -66,6 +66,9 @@ typedef struct alebgk_config
     int transport;    /* 0 auto (lattice march when the cloud is a complete
                          lattice and precision is 32, else coefficient
                          gather), 1 always gather, 2 require the march       */
+    int particle;     /* 0 auto (streamed rows for a 3-D cloud whose rows fit,
+                         else one warp per particle), 1 always the general
+                         kernel, 2 require the streamed kernel                */
 } alebgk_config;
 
 /* The host cloud in SoA form.  Inputs for alebgk_upload; the download calls
@@ -100,6 +103,8 @@ typedef struct alebgk_counters
     int error_word;           /* device-side error bits (0 = none)            */
     int transport_kernel;     /* transport in use: 1 coefficient gather,
                                  2 lattice march                              */
+    int particle_kernel;      /* particle stage in use: 1 warp per particle,
+                                 2 streamed rows                              */
 } alebgk_counters;
 
 /* ---- context --------------------------------------------------------- */
