@@ -115,6 +115,7 @@ int alebgk_create(const alebgk_config *cfg, alebgk_ctx **out)
     p.vmin = cfg->vmin; p.dv = cfg->dv;
     p.dvN = (cfg->dim == 3) ? cfg->dv * cfg->dv * cfg->dv : cfg->dv * cfg->dv;
     p.h = cfg->radius;
+    p.nadNoise = (cfg->precision == 32) ? 64.0 * 0x1p-24 : 0.0;
     *out = c;
     return ALEBGK_OK;
 }

@@ -455,7 +455,8 @@ __device__ int screen(const ParticleArgs<T> &a, const StepParams &p, int i, int 
     if (isfinite(lo) && isfinite(hi))
     {
         double rn = m * p.dvN;
-        double slack = 0.1 * fmax(hi - lo, 1.0e-12) + 1.0e-9;
+        double slack = 0.1 * fmax(hi - lo, 1.0e-12) + 1.0e-9 +
+                       p.nadNoise * fmax(fabs(lo), fabs(hi));
         if (rn < lo - slack || rn > hi + slack) return 1;
     }
     return 0;
@@ -809,7 +810,8 @@ k_particle_stream(ParticleArgs<T> a, StepParams p, int wpb)
             else if (isfinite(lo) && isfinite(hi))
             {
                 const double rn = m * dvN;
-                const double slack = 0.1 * fmax(hi - lo, 1.0e-12) + 1.0e-9;
+                const double slack = 0.1 * fmax(hi - lo, 1.0e-12) + 1.0e-9 +
+                                     p.nadNoise * fmax(fabs(lo), fabs(hi));
                 flagged = (rn < lo - slack || rn > hi + slack);
             }
         }

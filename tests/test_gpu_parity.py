@@ -249,6 +249,30 @@ def test_streamed_particle_kernel_positivity_repair(gpu):
     s.close()
 
 
+def test_fp32_screen_ignores_rounding_noise(gpu):
+    """FP32 cannot resolve density extrema below its own rounding, so its NAD
+    screen adds a floor of 64 FP32 ulps of the neighbour range to the
+    reference's slack (MLSTransport.cpp:370).  Step 1, where the screen fires
+    on every interior particle of the rest state, matches FP64; later FP32
+    flags at most what FP64 flags, instead of the thousands of particles
+    whose transported density differs from its neighbours' only by
+    rounding."""
+    c = ab.Case("cavity3d", 16, 10, -1.0, 2)
+    s32 = ab.Solver(c, precision=32)
+    s64 = ab.Solver(c, precision=64)
+    for step in range(6):
+        s32.cudaStep(1)
+        s64.cudaStep(1)
+        f32 = s32.counters()["transport_flags"]
+        f64 = s64.counters()["transport_flags"]
+        if step == 0:
+            assert f32 == f64 == 14 ** 3
+        else:
+            assert f32 <= f64
+    s32.close()
+    s64.close()
+
+
 def test_full_size_cavity3d_properties(gpu):
     """cavity3d Nx=40 Nv=10 (64 000 x 1 000): properties that hold at any
     size -- FP32 tracks FP64 on the device, the run is finite, and the mass
