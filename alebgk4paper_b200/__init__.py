@@ -99,6 +99,13 @@ class Case:
             bodies = np.zeros(32 * max(1, self.nbodies))
             _check(lib.alebgk_case_bodies(h, _dp(bodies)))
             self.bodies = bodies.reshape(-1, 32)[: self.nbodies].copy()
+            kind = np.zeros(max(1, self.nbodies), np.int32)
+            rot = np.zeros(max(1, self.nbodies), np.int32)
+            size = np.zeros(max(1, self.nbodies))
+            _check(lib.alebgk_case_body_shapes(h, _ip(kind), _ip(rot), _dp(size)))
+            self.body_kind = kind[: self.nbodies].copy()
+            self.body_rotates = rot[: self.nbodies].copy()
+            self.body_size = size[: self.nbodies].copy()
         finally:
             lib.alebgk_case_free(h)
 
@@ -220,6 +227,53 @@ class Solver:
         _check(self.lib.alebgk_body_loads_noalloc(self.ctx, nb, _dp(c), _dp(a), _dp(out)),
                self.ctx)
         return out
+
+    def body_step(self, state: np.ndarray | None = None, dt: float | None = None) -> np.ndarray:
+        """One Heun Newton-Euler step of the case's bodies after a completed
+        step (moveRigidBodies, RigidBody/BodyDynamics.cpp:352-638).  ``state``
+        (nbodies x 32, the layout of :attr:`Case.bodies`) defaults to the
+        case's; the updated state is returned.  The surface particles move,
+        so the next :meth:`cudaStep` needs the cloud uploaded again."""
+        c = self.case
+        st = np.ascontiguousarray(c.bodies if state is None else state, np.float64)
+        nb = st.shape[0]
+        arr = (_abi.Body * nb)()
+        for b in range(nb):
+            arr[b].kind = int(c.body_kind[b])
+            arr[b].rotates = int(c.body_rotates[b])
+            arr[b].size = float(c.body_size[b])
+            for k in range(32):
+                arr[b].state[k] = float(st[b, k])
+        p = c.params
+        box = np.array([p["xleft"], p["xright"], p["ybottom"], p["ytop"], p["zfront"],
+                        p["zback"]])
+        _check(self.lib.alebgk_body_step(self.ctx, nb, arr, _dp(box), float(p["dx"]),
+                                         float(self.dt if dt is None else dt)), self.ctx)
+        return np.array([[arr[b].state[k] for k in range(32)] for b in range(nb)])
+
+    def refresh_geometry(self):
+        """Uploads the cloud again after :meth:`body_step` moved the surface:
+        positions, mesh velocities and wall state as the device holds them,
+        with the current distribution and macros, and the neighbour lists
+        kept.  The reference instead runs its cloud management here
+        (manageRemove, mergeCloseParticles, manageRefill and a neighbour
+        rebuild, Solver.cpp:373-401); this keeps the particle set, which is
+        what those routines leave while the body stays clear of the fluid
+        particles."""
+        c = self.case
+        xyz, mv, wall = self.download_geometry()
+        g, macro = self.cudaDownloadFull()
+        c.xyz, c.meshv, c.wall, c.g, c.macro = xyz, mv, wall, g, macro
+        self.cudaUploadCloud(c)
+
+    def download_geometry(self):
+        """(xyz N x 3, meshv N x 3, wall N x 7) as stored on the device."""
+        xyz = np.zeros((self.N, 3))
+        mv = np.zeros((self.N, 3))
+        wall = np.zeros((self.N, 7))
+        _check(self.lib.alebgk_download_geometry(self.ctx, _dp(xyz), _dp(mv), _dp(wall)),
+               self.ctx)
+        return xyz, mv, wall
 
     def cudaFreeCloud(self):
         if getattr(self, "ctx", None):

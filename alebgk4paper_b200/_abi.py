@@ -39,6 +39,11 @@ class Cloud(ctypes.Structure):
     ]
 
 
+class Body(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("rotates", ctypes.c_int), ("size", ctypes.c_double),
+                ("state", ctypes.c_double * 32)]
+
+
 class Counters(ctypes.Structure):
     _fields_ = [
         ("steps", ctypes.c_int64), ("transport_flags", ctypes.c_int),
@@ -81,6 +86,11 @@ SIGNATURES = {
                                          c_double_p, c_double_p]),
     "alebgk_body_loads_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p,
                                                  c_double_p, c_double_p]),
+    "alebgk_body_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(Body),
+                                        c_double_p, ctypes.c_double, ctypes.c_double]),
+    "alebgk_download_geometry": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p,
+                                                c_double_p]),
+    "alebgk_case_body_shapes": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p, c_double_p]),
     "alebgk_body_set_surface_velocity": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
                                                         c_double_p, c_double_p]),
     "alebgk_case_build": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int,

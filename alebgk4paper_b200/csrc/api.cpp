@@ -45,7 +45,7 @@ void freeBuffers(alebgk_ctx *c)
     void *ptrs[] = {d.f[0], d.f[1], d.coef, d.coefLin, d.pos, d.meshv, d.wall,
                     d.boundary, d.bodyId, d.cls, d.nslot, d.slots, d.macro[0],
                     d.macro[1], d.mood, d.flag, d.flagList, d.degList, d.massPos, d.massEnd, d.minG, d.nad,
-                    d.dpx, d.bodyTmp, d.bodyOut, d.stage, d.sc};
+                    d.dpx, d.bodyTmp, d.bodyOut, d.stage, d.surfList, d.bodyIO, d.sc};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     d = DeviceBuffers();
@@ -238,6 +238,15 @@ int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
     CK(dalloc(&d.bodyOut, 64 * 6));
     CK(dalloc(&d.sc, 1));
     CK(dalloc(&d.stage, (size_t)N * p.gs));
+    c->surfHost.clear();
+    for (int i = 0; i < N; ++i)
+        if (cl->boundary[i] && cl->body_id[i] >= 0) c->surfHost.push_back(i);
+    CK(dalloc(&d.surfList, c->surfHost.size()));
+    CK(dalloc(&d.bodyIO, (size_t)kBodyIOHead + 13 * c->surfHost.size()));
+    if (!c->surfHost.empty())
+        CK(cudaMemcpy(d.surfList, c->surfHost.data(), 4 * c->surfHost.size(),
+                      cudaMemcpyHostToDevice));
+    c->geometryDirty = false;
     CK(cudaMemcpy(d.pos, cl->xyz, 24 * (size_t)N, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d.meshv, cl->meshv, 24 * (size_t)N, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d.wall, cl->wall, 56 * (size_t)N, cudaMemcpyHostToDevice));
@@ -317,6 +326,9 @@ int alebgk_step(alebgk_ctx *c, int nsteps)
     if (!c) return ALEBGK_EINVAL;
     if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
     if (nsteps < 0) return fail(c, ALEBGK_EINVAL, "nsteps must be >= 0");
+    if (c->geometryDirty)
+        return fail(c, ALEBGK_ESTATE,
+                    "a body step moved the surface particles: upload the cloud again");
     CK(cudaSetDevice(c->cfg.device));
     for (int n = 0; n < nsteps; ++n)
     {
@@ -578,6 +590,46 @@ int alebgk_body_set_surface_velocity(alebgk_ctx *c, int nbodies,
     return ALEBGK_OK;
 }
 
+int alebgk_body_step(alebgk_ctx *c, int nbodies, alebgk_body *bodies, const double *box,
+                     double dx, double dt)
+{
+    if (!c || !bodies || !box) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (nbodies <= 0 || nbodies > kMaxBodyIO) return fail(c, ALEBGK_EINVAL, "1..64 bodies");
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    if (!(dt > 0)) return fail(c, ALEBGK_EINVAL, "dt must be > 0");
+    for (int b = 0; b < nbodies; ++b)
+    {
+        const alebgk_body &B = bodies[b];
+        if (B.kind < 0 || B.kind > 3 || (B.kind >= 2) != (c->sp.dim == 3))
+            return fail(c, ALEBGK_EINVAL, "body kind does not match the cloud's dimension");
+        if (!(B.state[19] > 0) || !(B.state[20] > 0))
+            return fail(c, ALEBGK_EINVAL, "body mass and moment of inertia must be > 0");
+    }
+    for (int i = 0; i < c->sp.N; ++i)
+        if (c->bodyIdHost[i] >= nbodies)
+            return fail(c, ALEBGK_EINVAL, "a particle's body id exceeds nbodies");
+    CK(cudaSetDevice(c->cfg.device));
+    std::string err;
+    const cudaError_t e = bodyStep(c, nbodies, bodies, box, dx, dt, &err);
+    if (e != cudaSuccess)
+        return fail(c, ALEBGK_ECUDA, "body step: " + err + ": " + cudaGetErrorString(e));
+    c->geometryDirty = !c->surfHost.empty();
+    return ALEBGK_OK;
+}
+
+int alebgk_download_geometry(alebgk_ctx *c, double *xyz, double *meshv, double *wall)
+{
+    if (!c) return ALEBGK_EINVAL;
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    const size_t N = c->sp.N;
+    if (xyz) CK(cudaMemcpy(xyz, c->d.pos, 24 * N, cudaMemcpyDeviceToHost));
+    if (meshv) CK(cudaMemcpy(meshv, c->d.meshv, 24 * N, cudaMemcpyDeviceToHost));
+    if (wall) CK(cudaMemcpy(wall, c->d.wall, 56 * N, cudaMemcpyDeviceToHost));
+    return ALEBGK_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Host-side coefficient tables
 // ---------------------------------------------------------------------------
@@ -730,6 +782,19 @@ int alebgk_case_bodies(const alebgk_case *cs, double *out)
         std::memcpy(o, v, sizeof v);
         for (int k = 0; k < 9; ++k) o[22 + k] = r.Rm[k];
         o[31] = r.surfaceArea();
+    }
+    return ALEBGK_OK;
+}
+
+int alebgk_case_body_shapes(const alebgk_case *cs, int *kind, int *rotates, double *size)
+{
+    if (!cs || !kind || !rotates || !size) return ALEBGK_EINVAL;
+    const Cloud &c = cs->cloud;
+    for (size_t b = 0; b < c.bodies.size(); ++b)
+    {
+        kind[b] = c.bodies[b].kind;
+        rotates[b] = c.bodies[b].rotates ? 1 : 0;
+        size[b] = c.bodies[b].size;
     }
     return ALEBGK_OK;
 }

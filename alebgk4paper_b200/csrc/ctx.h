@@ -65,6 +65,8 @@ struct DeviceBuffers
     double *bodyTmp = nullptr;         // N x 6 per-particle load contributions
     double *bodyOut = nullptr;         // up to 64 bodies x 6
     double *stage = nullptr;           // N x gs FP64 host-transfer staging
+    int *surfList = nullptr;           // body-surface particles (boundary, bodyId >= 0)
+    double *bodyIO = nullptr;          // body-step staging: kBodyIOHead + 13 per surface particle
     StepScalars *sc = nullptr;
 };
 
@@ -103,6 +105,8 @@ struct alebgk_ctx
     size_t pStreamSmem = 0;
     std::string err;
     std::vector<int> bodyIdHost;
+    std::vector<int> surfHost;   // body-surface particle indices, ascending
+    bool geometryDirty = false;  // a body step moved the surface since the upload
 };
 
 namespace alebgk {
@@ -116,6 +120,11 @@ cudaError_t launchBodyLoads(alebgk_ctx *c, int nbodies, const double *centreDev,
 cudaError_t launchSetSurfaceVelocity(alebgk_ctx *c, int nbodies,
                                      const double *centreDev,
                                      const double *stateDev);
+// Heun Newton-Euler step of the rigid bodies (body_step.cu).
+constexpr int kMaxBodyIO = 64;                 // bodies per body call
+constexpr int kBodyIOHead = 13 * kMaxBodyIO;   // doubles before the surface rows
+cudaError_t bodyStep(alebgk_ctx *c, int nbodies, alebgk_body *bodies, const double *box,
+                     double dx, double dt, std::string *err);
 // Body loads on the fixed device scratch of body_noalloc.cu (no allocation).
 constexpr int kNoAllocMaxBodies = ALEBGK_NOALLOC_MAX_BODIES;
 cudaError_t bodyLoadsNoAlloc(alebgk_ctx *c, int nbodies, const double *centre,

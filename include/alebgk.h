@@ -221,6 +221,39 @@ int alebgk_body_loads(alebgk_ctx *ctx, int nbodies, const double *body_centre,
 int alebgk_body_loads_noalloc(alebgk_ctx *ctx, int nbodies, const double *body_centre,
                               const double *body_area, double *out);
 
+/* One rigid body: shape and the 32-double state of alebgk_case_bodies
+ * (centre 0-2, velocity 3-5, 2-D spin 6, angular velocity 7-9, force
+ * 10-12, 2-D torque 13, torque 14-16, 2-D orientation 17-18, mass 19,
+ * moment of inertia 20, temperature 21, body-to-world rotation 22-30,
+ * surface area per surface point 31).  RigidBody/Geometry.hpp:19-362. */
+typedef struct alebgk_body
+{
+    int kind;          /* 0 square, 1 circle (2-D); 2 sphere, 3 cube (3-D) */
+    int rotates;       /* free to spin under the hydrodynamic torque        */
+    double size;       /* side (square, cube) or radius (circle, sphere)    */
+    double state[32];
+} alebgk_body;
+
+/* One Heun Newton-Euler step of the bodies after a completed alebgk_step
+ * (moveRigidBodies, RigidBody/BodyDynamics.cpp:352-638): loads at the
+ * stored wall state and at the predicted one (on the device, FP64), rigid
+ * motion of the surface particles with the old body state, Newton-Euler
+ * with the averaged loads, box-wall contact with a gap of 0.4 dx, and the
+ * surface particles' new normal, wall velocity and mesh velocity.  bodies
+ * is read and updated in place; box = xleft, xright, ybottom, ytop, zfront,
+ * zback (DomainBoundary, Core/Types.hpp:73).  The surface particles move,
+ * so the next alebgk_step returns ALEBGK_ESTATE until the cloud is uploaded
+ * again (alebgk_download_geometry gives the moved geometry; the reference
+ * runs its cloud management in between, Solver.cpp:373-401). */
+int alebgk_body_step(alebgk_ctx *ctx, int nbodies, alebgk_body *bodies,
+                     const double *box, double dx, double dt);
+
+/* Positions (N*3), mesh velocities (N*3) and wall state (N*7) as stored on
+ * the device; any pointer may be NULL.  No reference counterpart (the
+ * reference's device state is never read back; cudaSyncBodies,
+ * Solver/CudaBackend.cu:1884-1916, writes it). */
+int alebgk_download_geometry(alebgk_ctx *ctx, double *xyz, double *meshv, double *wall);
+
 /* Writes the surface wall velocity V + w x r of trial body states onto the
  * surface particles on the device (RigidBody/BodyDynamics.cpp:103-125).
  * state: nbodies*6 (V, w); body_centre: nbodies*3. */
@@ -269,6 +302,9 @@ int alebgk_case_view(alebgk_case *c, alebgk_cloud *view);
 /* Body state: per body 32 doubles: cx cy cz velx vely velz angularVel omx omy
  * omz forcex forcey forcez torque tqx tqy tqz ox oy mass I T Rm[9] area. */
 int alebgk_case_bodies(const alebgk_case *c, double *out);
+
+/* Shape of every body of the case: kind (alebgk_body), rotates, size. */
+int alebgk_case_body_shapes(const alebgk_case *c, int *kind, int *rotates, double *size);
 
 /* Fills a solver configuration from a case (precision 32 or 64). */
 int alebgk_case_config(const alebgk_case *c, int precision, int device,

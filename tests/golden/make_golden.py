@@ -42,6 +42,13 @@ STEPS = [
     ("square_n24_v8_q_s4", "cavity2d-square", 24, 8, 2, 4, False),
 ]
 
+# Free-body runs: (tag, case, Nx, Nv), BODY_STEPS steps each.
+BODY_RUNS = [
+    ("cube_n12_v4_free", "cavity3d-cube", 12, 4),
+    ("square_n24_v8_free", "cavity2d-square", 24, 8),
+]
+BODY_STEPS = 8
+
 
 def nbr_hash(nbr: np.ndarray, nnb: np.ndarray) -> np.ndarray:
     """Order-sensitive per-particle hash of the neighbour list."""
@@ -77,18 +84,19 @@ def main():
         if full:
             d["g"] = g
         np.savez_compressed(os.path.join(HERE, f"step_{tag}.npz"), **d)
-    # Free cube: one step of the reference's moving-body path
-    # (RigidBody/BodyDynamics.cpp:143-711) -> body state after the Heun update.
-    r = RefCase("cavity3d-cube", 12, 4, -1.0, 2, fixed_body=False)
-    b0 = r.bodies().copy()
-    g0 = r.g()
-    m0 = r.macro()
-    c0 = r.cloud()
-    r.step(1)
-    np.savez_compressed(os.path.join(HERE, "body_cube_n12_v4_free_s1.npz"),
-                        bodies_before=b0, bodies_after=r.bodies(), N_after=r.N,
-                        mass_after=r.sum_mass(), g0_sum=g0.sum(), m0=m0[:, 0].sum(),
-                        nsurf=int((c0["body_id"] >= 0).sum()))
+    # Free bodies: the reference's moving-body path (fluid step, then
+    # moveRigidBodies, RigidBody/BodyDynamics.cpp:143-711, then its cloud
+    # management) -> body state and particle count after every step.
+    for tag, case, Nx, Nv in BODY_RUNS:
+        r = RefCase(case, Nx, Nv, -1.0, 2, fixed_body=False)
+        b0 = r.bodies().copy()
+        hist, counts = [], []
+        for _ in range(BODY_STEPS):
+            r.step(1)
+            hist.append(r.bodies().copy())
+            counts.append(r.N)
+        np.savez_compressed(os.path.join(HERE, f"body_{tag}.npz"), bodies_before=b0,
+                            bodies=np.array(hist), N=np.array(counts))
     print("fixtures written to", HERE)
 
 
