@@ -56,6 +56,23 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest of every rank's x (a step time): the job is as fast as
+    its slowest cavity.  Every rank must call it, in the same order."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def weak_value(world: int, updates_per_rank: int, steps: int, seconds: float) -> float:
+    """Whole-job updates/s: every rank advances its own cavity of the same
+    size, so the job does world x updates x steps in the max-over-ranks time."""
+    return world * updates_per_rank * steps / seconds
+
+
 # ---------------------------------------------------------------------------
 class ClockSampler:
     """Samples nvidia-smi clocks and throttle reasons during the timed region."""
@@ -240,12 +257,8 @@ def run_ours(args):
         if rc != 0:
             raise RuntimeError(f"alebgk_step_timed failed ({rc})")
         barrier()
-    t_ms = ms.value
-    if dist is not None:
-        tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
-    value = world * updates * args.steps / (t_ms / 1e3)
+    t_ms = max_over_ranks(ms.value, dist, "cuda")
+    value = weak_value(world, updates, args.steps, t_ms / 1e3)
 
     # per-stage device times (kernel by kernel, events on the launching stream)
     prof = (ctypes.c_float * _abi.NSTAGES)()
@@ -300,12 +313,8 @@ def run_ours(args):
     for _ in range(args.e2e_steps):
         e2e_step()
     barrier()
-    te = time.perf_counter() - t0
-    if dist is not None:
-        tt = torch.tensor([te], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        te = float(tt.item())
-    e2e_value = world * updates * args.e2e_steps / te
+    te = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
+    e2e_value = weak_value(world, updates, args.e2e_steps, te)
     h2d = N * case.gstride * 8 + N * 7 * 8
     d2h = N * 7 * 8
 
