@@ -44,7 +44,7 @@ void freeBuffers(alebgk_ctx *c)
     DeviceBuffers &d = c->d;
     void *ptrs[] = {d.f[0], d.f[1], d.coef, d.coefLin, d.pos, d.meshv, d.wall,
                     d.boundary, d.bodyId, d.cls, d.nslot, d.slots, d.macro[0],
-                    d.macro[1], d.mood, d.flag, d.flagList, d.degList, d.massPos, d.massEnd, d.minG, d.nad,
+                    d.macro[1], d.mood, d.flag, d.flagList, d.degList, d.massPos, d.massEnd, d.minG, d.nad, d.redPartial,
                     d.dpx, d.bodyTmp, d.bodyOut, d.stage, d.surfList, d.bodyIO, d.sc};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -95,9 +95,15 @@ int alebgk_create(const alebgk_config *cfg, alebgk_ctx **out)
     c->cfg = *cfg;
     cudaError_t e = cudaSetDevice(cfg->device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->evFork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->evJoin, cudaEventDisableTiming);
     if (e != cudaSuccess)
     {
         gCreateError = std::string("stream creation: ") + cudaGetErrorString(e);
+        if (c->stream) cudaStreamDestroy(c->stream);
+        if (c->stream2) cudaStreamDestroy(c->stream2);
+        if (c->evFork) cudaEventDestroy(c->evFork);
         delete c;
         return ALEBGK_ECUDA;
     }
@@ -127,6 +133,9 @@ int alebgk_destroy(alebgk_ctx *c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     freeBuffers(c);
     if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->stream2) cudaStreamDestroy(c->stream2);
+    if (c->evFork) cudaEventDestroy(c->evFork);
+    if (c->evJoin) cudaEventDestroy(c->evJoin);
     delete c;
     return ALEBGK_OK;
 }
@@ -233,6 +242,7 @@ int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
     CK(dalloc(&d.massEnd, N));
     CK(dalloc(&d.minG, N));
     CK(dalloc(&d.nad, 2 * (size_t)N));
+    CK(dalloc(&d.redPartial, 256));
     CK(dalloc(&d.dpx, N));
     CK(dalloc(&d.bodyTmp, 6 * (size_t)N));
     CK(dalloc(&d.bodyOut, 64 * 6));

@@ -43,6 +43,7 @@ struct StepScalars
     int nfix;              // positivity repairs
     int moodfail;          // post-collision moodCheck failed
     int err;               // device error bits
+    unsigned redCount;     // ticket of the grid sums (zero between kernels)
     long long steps;
 };
 
@@ -61,6 +62,7 @@ struct DeviceBuffers
     double *massEnd = nullptr;         // per particle: mass of h at step end
     double *minG = nullptr;            // per particle: min of h over the mass layer
     double *nad = nullptr;             // per particle: NAD neighbour density range (lo, hi)
+    double *redPartial = nullptr;      // per-block partials of the grid sums
     double *dpx = nullptr;
     double *bodyTmp = nullptr;         // N x 6 per-particle load contributions
     double *bodyOut = nullptr;         // up to 64 bodies x 6
@@ -94,6 +96,8 @@ struct alebgk_ctx
     alebgk::DeviceBuffers d;
     alebgk::MarchState march;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;          // side stream of the step graph
+    cudaEvent_t evFork = nullptr, evJoin = nullptr;
     int cur = 0;                 // buffer holding the current h and macros
     bool uploaded = false;
     int ncls = 0;

@@ -1088,55 +1088,97 @@ k_fixup(ParticleArgs<T> a, StepParams p)
     }
 }
 
-// Deterministic single-block sums; thread t sums a contiguous chunk.
+// Deterministic single-block sums: thread t sums elements t, t + nt, ...
+// (coalesced) into four interleaved partial sums, combined in a fixed order.
 template <int K>
 __device__ void blockReduceArrays(const double *const (&a)[K], int N, double (&out)[K],
                                   double *sh)
 {
     const int t = threadIdx.x, nt = blockDim.x;
-    const int chunk = (N + nt - 1) / nt;
-    const int lo = t * chunk, hi = min(N, lo + chunk);
     double v[K];
 #pragma unroll
     for (int q = 0; q < K; ++q)
     {
-        double s = 0.0;
-        for (int i = lo; i < hi; ++i) s += a[q][i];
-        v[q] = s;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int i = t;
+        for (; i + 3 * nt < N; i += 4 * nt)
+        {
+            s0 += a[q][i];
+            s1 += a[q][i + nt];
+            s2 += a[q][i + 2 * nt];
+            s3 += a[q][i + 3 * nt];
+        }
+        for (; i < N; i += nt) s0 += a[q][i];
+        v[q] = (s0 + s1) + (s2 + s3);
     }
     blockSums<K>(v, sh);
 #pragma unroll
     for (int q = 0; q < K; ++q) out[q] = v[q];
 }
 
-// Global mass rescale (Solver/Solver.cpp:650-655): sigma = massOld/massNew.
-__global__ void __launch_bounds__(1024)
-k_sigma(const double *__restrict__ massPos, int N, StepScalars *sc)
+// Deterministic grid sum of a[0..N) over kRedBlocks blocks: block b sums the
+// fixed strided subset b*nt + t + k*stride into partial[b]; the last block to
+// finish (ticket on sc->redCount) adds the partials in block order and
+// resets the ticket.  Returns true in thread 0 of that block, with *total.
+constexpr int kRedBlocks = 64;
+constexpr int kRedThreads = 256;
+
+__device__ bool gridSumLast(const double *__restrict__ a, int N, double *partial,
+                            StepScalars *sc, double *total)
 {
     __shared__ double sh[32];
-    const double *const a[1] = {massPos};
-    double out[1];
-    blockReduceArrays<1>(a, N, out, sh);
-    if (threadIdx.x == 0)
+    __shared__ bool last;
+    const int t = threadIdx.x, stride = gridDim.x * blockDim.x;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    int i = blockIdx.x * blockDim.x + t;
+    for (; i + 3 * stride < N; i += 4 * stride)
     {
-        sc->massNew = out[0];
-        sc->sigma = (out[0] > 1.0e-30) ? sc->massOld / out[0] : 1.0;
+        s0 += a[i];
+        s1 += a[i + stride];
+        s2 += a[i + 2 * stride];
+        s3 += a[i + 3 * stride];
+    }
+    for (; i < N; i += stride) s0 += a[i];
+    double v[1] = {(s0 + s1) + (s2 + s3)};
+    blockSums<1>(v, sh);
+    if (t == 0)
+    {
+        partial[blockIdx.x] = v[0];
+        __threadfence();
+        last = atomicAdd(&sc->redCount, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || t != 0) return false;
+    __threadfence();
+    double s = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) s += ((volatile double *)partial)[b];
+    sc->redCount = 0;
+    *total = s;
+    return true;
+}
+
+// Global mass rescale (Solver/Solver.cpp:650-655): sigma = massOld/massNew.
+__global__ void __launch_bounds__(kRedThreads)
+k_sigma(const double *__restrict__ massPos, int N, double *partial, StepScalars *sc)
+{
+    double m;
+    if (gridSumLast(massPos, N, partial, sc, &m))
+    {
+        sc->massNew = m;
+        sc->sigma = (m > 1.0e-30) ? sc->massOld / m : 1.0;
     }
 }
 
 // Mass at the end of the step (the next step's massOld); the stored state
 // now carries the scale sigma.
-__global__ void __launch_bounds__(1024)
-k_mass_sum(const double *__restrict__ massEnd, int N, StepScalars *sc)
+__global__ void __launch_bounds__(kRedThreads)
+k_mass_sum(const double *__restrict__ massEnd, int N, double *partial, StepScalars *sc)
 {
-    __shared__ double sh[32];
-    const double *const a[1] = {massEnd};
-    double out[1];
-    blockReduceArrays<1>(a, N, out, sh);
-    if (threadIdx.x == 0)
+    double m;
+    if (gridSumLast(massEnd, N, partial, sc, &m))
     {
         const double sigma = sc->sigma;
-        sc->massEnd = sigma * out[0];
+        sc->massEnd = sigma * m;
         sc->massOld = sc->massEnd;
         sc->scale = sigma;
         sc->steps += 1;
@@ -1171,8 +1213,9 @@ k_recollide(T *__restrict__ g, StepParams p, const int *__restrict__ boundary,
 {
     if (sc->moodfail == 0) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int i = blockIdx.x * (kNT / 32) + warp;
-    if (i >= p.N || boundary[i]) return;
+    for (int i = blockIdx.x * (kNT / 32) + warp; i < p.N; i += gridDim.x * (kNT / 32))
+    {
+    if (boundary[i]) continue;
     const double sigma = sc->sigma;
     T *row = g + (size_t)i * p.ldf;
     double *mac = macNew + 6 * (size_t)i;
@@ -1227,20 +1270,18 @@ k_recollide(T *__restrict__ g, StepParams p, const int *__restrict__ boundary,
         }
         massEnd[i] = N0 / sigma;
     }
+    }
 }
 
 // Mass at the end of a step whose moodCheck failed (after k_recollide).
-__global__ void __launch_bounds__(1024)
-k_mass_end(const double *__restrict__ massEnd, int N, StepScalars *sc)
+__global__ void __launch_bounds__(kRedThreads)
+k_mass_end(const double *__restrict__ massEnd, int N, double *partial, StepScalars *sc)
 {
     if (sc->moodfail == 0) return;
-    __shared__ double sh[32];
-    const double *const a[1] = {massEnd};
-    double out[1];
-    blockReduceArrays<1>(a, N, out, sh);
-    if (threadIdx.x == 0)
+    double m;
+    if (gridSumLast(massEnd, N, partial, sc, &m))
     {
-        sc->massEnd = sc->sigma * out[0];
+        sc->massEnd = sc->sigma * m;
         sc->massOld = sc->massEnd;
     }
 }
@@ -1248,11 +1289,11 @@ k_mass_end(const double *__restrict__ massEnd, int N, StepScalars *sc)
 // Resets the step's counters; with a NAD range buffer also computes the
 // neighbour density ranges of the streamed particle kernel.
 __global__ void __launch_bounds__(kNT)
-k_step_begin(StepScalars *sc, const double *__restrict__ macPrev,
+k_step_begin(StepScalars *sc, int reset, const double *__restrict__ macPrev,
              const int *__restrict__ boundary, const int *__restrict__ nslot,
              const int *__restrict__ slots, int S, int N, double *__restrict__ nad)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0)
+    if (reset && blockIdx.x == 0 && threadIdx.x == 0)
     {
         sc->nflag = 0;
         sc->ndeg = 0;
@@ -1277,17 +1318,14 @@ k_particle_mass(const T *g, StepParams p, double *massEnd)
     if (lane == 0) massEnd[i] = s * p.dvN;
 }
 
-__global__ void __launch_bounds__(1024)
-k_mass_init(const double *__restrict__ massEnd, int N, StepScalars *sc)
+__global__ void __launch_bounds__(kRedThreads)
+k_mass_init(const double *__restrict__ massEnd, int N, double *partial, StepScalars *sc)
 {
-    __shared__ double sh[32];
-    const double *const a[1] = {massEnd};
-    double out[1];
-    blockReduceArrays<1>(a, N, out, sh);
-    if (threadIdx.x == 0)
+    double m;
+    if (gridSumLast(massEnd, N, partial, sc, &m))
     {
-        sc->massOld = out[0];
-        sc->massEnd = out[0];
+        sc->massOld = m;
+        sc->massEnd = m;
         sc->scale = 1.0;
         sc->sigma = 1.0;
     }
@@ -1446,11 +1484,27 @@ static cudaError_t stepT(alebgk_ctx *c, int from, cudaEvent_t *ev)
     int q = 0;
     auto mark = [&]() { if (ev) cudaEventRecord(ev[q++], st); };
     const int pBlocks = (p.N + kNT / 32 - 1) / (kNT / 32);
-    const int listBlocks = min(p.N, 1184);
+    const int listBlocks = min(p.N, 296);
     mark();
     const bool nadOn = c->pStream && p.limiter == 2;
-    k_step_begin<<<nadOn ? min((p.N + kNT / 32 - 1) / (kNT / 32), 1184) : 1, kNT, 0, st>>>(
-        d.sc, macA, d.boundary, d.nslot, d.slots, p.S, p.N, nadOn ? d.nad : nullptr);
+    const int nadBlocks = min((p.N + kNT / 32 - 1) / (kNT / 32), 1184);
+    // The NAD ranges depend only on the previous step's macros: in a step
+    // graph they run on a side stream beside the transport; when stages are
+    // timed they run in step_begin.
+    const bool fork = nadOn && !ev && c->stream2;
+    if (fork)
+    {
+        k_step_begin<<<1, kNT, 0, st>>>(d.sc, 1, macA, d.boundary, d.nslot, d.slots, p.S, p.N,
+                                        nullptr);
+        cudaEventRecord(c->evFork, st);
+        cudaStreamWaitEvent(c->stream2, c->evFork, 0);
+        k_step_begin<<<nadBlocks, kNT, 0, c->stream2>>>(d.sc, 0, macA, d.boundary, d.nslot,
+                                                        d.slots, p.S, p.N, d.nad);
+        cudaEventRecord(c->evJoin, c->stream2);
+    }
+    else
+        k_step_begin<<<nadOn ? nadBlocks : 1, kNT, 0, st>>>(
+            d.sc, 1, macA, d.boundary, d.nslot, d.slots, p.S, p.N, nadOn ? d.nad : nullptr);
     mark();
     if (sizeof(T) == 4 && c->march.enabled)
     {
@@ -1465,6 +1519,7 @@ static cudaError_t stepT(alebgk_ctx *c, int from, cudaEvent_t *ev)
                                            p.ldf, d.sc);
     }
     mark();
+    if (fork) cudaStreamWaitEvent(st, c->evJoin, 0);
     const size_t rowBytes = (size_t)p.L * p.V * sizeof(T);
     const int wpb = particleWarpsPerBlock(p, sizeof(T));
     const int ppBlocks = (p.N + wpb - 1) / wpb;
@@ -1477,18 +1532,20 @@ static cudaError_t stepT(alebgk_ctx *c, int from, cudaEvent_t *ev)
     if (p.L == 2) k_redo<T, 2><<<listBlocks, kNT, rowBytes, st>>>(pa, p);
     else k_redo<T, 1><<<listBlocks, kNT, rowBytes, st>>>(pa, p);
     mark();
-    k_sigma<<<1, 1024, 0, st>>>(d.massPos, p.N, d.sc);
+    k_sigma<<<kRedBlocks, kRedThreads, 0, st>>>(d.massPos, p.N, d.redPartial, d.sc);
     mark();
     k_fixup<T><<<min(pBlocks, 296), kNT, 0, st>>>(pa, p);
     mark();
-    k_mass_sum<<<1, 1024, 0, st>>>(d.massEnd, p.N, d.sc);
+    k_mass_sum<<<kRedBlocks, kRedThreads, 0, st>>>(d.massEnd, p.N, d.redPartial, d.sc);
     mark();
     k_scale_mood<<<(p.N + 255) / 256, 256, 0, st>>>(p, d.boundary, macB, d.minG, d.mood, d.sc);
     mark();
     if (p.limiter == 2)
-        k_recollide<T><<<pBlocks, kNT, 0, st>>>(fb, p, d.boundary, macB, d.massEnd, d.sc);
+        k_recollide<T><<<min(pBlocks, 592), kNT, 0, st>>>(fb, p, d.boundary, macB, d.massEnd,
+                                                         d.sc);
     mark();
-    if (p.limiter == 2) k_mass_end<<<1, 1024, 0, st>>>(d.massEnd, p.N, d.sc);
+    if (p.limiter == 2)
+        k_mass_end<<<kRedBlocks, kRedThreads, 0, st>>>(d.massEnd, p.N, d.redPartial, d.sc);
     mark();
     return cudaGetLastError();
 }
@@ -1558,7 +1615,8 @@ static cudaError_t massInitT(alebgk_ctx *c)
     const int pBlocks = (p.N + kNT / 32 - 1) / (kNT / 32);
     k_particle_mass<T><<<pBlocks, kNT, 0, c->stream>>>(
         static_cast<const T *>(c->d.f[c->cur]), p, c->d.massEnd);
-    k_mass_init<<<1, 1024, 0, c->stream>>>(c->d.massEnd, p.N, c->d.sc);
+    k_mass_init<<<kRedBlocks, kRedThreads, 0, c->stream>>>(c->d.massEnd, p.N, c->d.redPartial,
+                                                            c->d.sc);
     return cudaGetLastError();
 }
 
