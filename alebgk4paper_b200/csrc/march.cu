@@ -13,7 +13,10 @@
 // velocity stay in registers for the whole march, and every staged value
 // feeds the FMAs of up to four columns and five output planes, held in a
 // 4 x 5 register queue.  An output plane is complete two input planes after
-// its own and is stored straight from the queue.  Thread 0 refills a ring
+// its own and is stored straight from the queue; planes outside the lattice
+// are zero and are skipped.  Long segments run every queue slot without
+// tests; short ones (the single-plane wall layers) only the slots of their
+// own output planes.  Thread 0 refills a ring
 // slot two planes after the warps released it, so the warps of a CTA may
 // drift apart by two planes without stalling the loads, which run four
 // planes ahead.  Every wait is bounded; a timeout sets the step's error
@@ -80,8 +83,8 @@ __device__ __forceinline__ void tmaLoadPlane(void *dst, const CUtensorMap *map, 
 
 __global__ void __launch_bounds__(kMarchWarps * 32, 2)
 k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ units,
-        const float *__restrict__ coefT, float *__restrict__ out, int Nx, int Ny, int V,
-        int Vpad, int ldf, StepScalars *sc)
+        const float *__restrict__ coefT, float *__restrict__ out, int Nx, int Ny, int Nz,
+        int V, int Vpad, int ldf, StepScalars *sc)
 {
     extern __shared__ __align__(128) unsigned char marchSmem[];
     typedef float Plane[kPH][kPW][kMarchChunk];
@@ -95,6 +98,11 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
     const int k0 = blockIdx.y * kMarchChunk;
     const int k = k0 + lane;
     const int nin = zb - za + 4;                 // input planes za-2 .. zb+1
+    // Planes outside the lattice hold zeros: they are not staged; the queue
+    // only moves past them.  Staged plane m is lattice plane zlo + m.
+    const int zlo = max(za - 2, 0), zhi = min(zb + 1, Nz - 1);
+    const int nv = zhi - zlo + 1;
+    const int moff = zlo - (za - 2);            // staged index m = n - moff
     const bool active = warp < u.nsub;
     const int sub = active ? __ldg(&u.sub[warp]) : 0;
     const int bx = sub & 15, by = (sub >> 4) & 15, mask = (sub >> 8) & 15, cls = sub >> 12;
@@ -113,11 +121,10 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
     __syncthreads();
     if (giveUp) return;
     if (threadIdx.x == 0)
-        for (int n = 0; n < kRing && n < nin; ++n)
+        for (int m = 0; m < kRing && m < nv; ++m)
         {
-            mbarExpectTx(&full[n], kPlaneBytes);
-            tmaLoadPlane(&ring[n][0][0][0], &tmap, &full[n], k0, ux0 - 2, uy0 - 2,
-                         za - 2 + n);
+            mbarExpectTx(&full[m], kPlaneBytes);
+            tmaLoadPlane(&ring[m][0][0][0], &tmap, &full[m], k0, ux0 - 2, uy0 - 2, zlo + m);
         }
 
     float coef[kTmplOffsets];
@@ -133,85 +140,114 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
 #pragma unroll
         for (int r = 0; r < 5; ++r) acc[c][r] = 0.0f;
     const float scale = (float)sc->scale;
+    // Output column c of the warp's block at plane z:
+    // outBase + z planeStride + (c & 1) colStride + (c >> 1) rowStride.
+    const int colStride = ldf, rowStride = ldf * Nx, planeStride = rowStride * Ny;
+    float *outBase = out + ((size_t)(ux0 + bx) + (size_t)Nx * (uy0 + by)) * ldf + k;
+    const int smask = (k < V) ? mask : 0;
     bool dead = false;
 
-    for (int n = 0; n < nin; ++n)
-    {
-        const int s = n % kRing;
-        const uint32_t par = (uint32_t)(n / kRing) & 1u;
-        mbarWait(&full[s], par, dead);
-        const int zi = za - 2 + n;
-        if (active)
-        {
-            // output plane of queue slot r: zo = zi - 2 + r
-            bool rv[5];
-#pragma unroll
-            for (int r = 0; r < 5; ++r)
-            {
-                const int zo = zi - 2 + r;
-                rv[r] = zo >= za && zo < zb;
-            }
-            const float *P = &ring[s][0][0][0];
-            unroll<6>([&](auto DY) {
-                constexpr int dy = decltype(DY)::value - 2;
-                float v[6];
-                unroll<6>([&](auto DX) {
-                    constexpr int dx = decltype(DX)::value - 2;
-                    constexpr bool need = tidx(dx, dy, 0) >= 0 || tidx(dx - 1, dy, 0) >= 0 ||
-                                          tidx(dx, dy - 1, 0) >= 0 ||
-                                          tidx(dx - 1, dy - 1, 0) >= 0;
-                    if constexpr (need)
-                        v[dx + 2] = P[((by + dy + 2) * kPW + (bx + dx + 2)) * kMarchChunk + lane];
-                });
-                unroll<5>([&](auto R) {
-                    constexpr int r = decltype(R)::value;
-                    constexpr int dz = 2 - r;
-                    if (rv[r])
-                    {
-                        unroll<6>([&](auto DX) {
-                            constexpr int dx = decltype(DX)::value - 2;
-                            unroll<4>([&](auto C) {
-                                constexpr int c = decltype(C)::value;
-                                constexpr int o = tidx(dx - (c & 1), dy - (c >> 1), dz);
-                                if constexpr (o >= 0)
-                                    acc[c][r] = fmaf(coef[o], v[dx + 2], acc[c][r]);
-                            });
-                        });
-                    }
-                });
+    // The FMAs of one staged plane into the queue; with `gated`, only the
+    // slots holding the unit's own output planes (inSeg(r)).
+    auto fmaPlane = [&](const float *P, auto GATED, auto inSeg) {
+        constexpr bool gated = decltype(GATED)::value;
+        unroll<6>([&](auto DY) {
+            constexpr int dy = decltype(DY)::value - 2;
+            float v[6];
+            unroll<6>([&](auto DX) {
+                constexpr int dx = decltype(DX)::value - 2;
+                constexpr bool need = tidx(dx, dy, 0) >= 0 || tidx(dx - 1, dy, 0) >= 0 ||
+                                      tidx(dx, dy - 1, 0) >= 0 || tidx(dx - 1, dy - 1, 0) >= 0;
+                if constexpr (need)
+                    v[dx + 2] = P[((by + dy + 2) * kPW + (bx + dx + 2)) * kMarchChunk + lane];
             });
-            // queue slot 0 (zo = zi - 2) is complete
-            if (rv[0] && k < V)
-            {
-                const int zo = zi - 2;
-#pragma unroll
-                for (int c = 0; c < 4; ++c)
+            unroll<5>([&](auto R) {
+                constexpr int r = decltype(R)::value;
+                constexpr int dz = 2 - r;
+                if (!gated || inSeg(r))
                 {
-                    if (!(mask >> c & 1)) continue;
-                    const int x = ux0 + bx + (c & 1), y = uy0 + by + (c >> 1);
-                    const size_t i = (size_t)x + (size_t)Nx * (y + (size_t)Ny * zo);
-                    out[i * ldf + k] = acc[c][0] * scale;
+                    unroll<6>([&](auto DX) {
+                        constexpr int dx = decltype(DX)::value - 2;
+                        unroll<4>([&](auto C) {
+                            constexpr int c = decltype(C)::value;
+                            constexpr int o = tidx(dx - (c & 1), dy - (c >> 1), dz);
+                            if constexpr (o >= 0)
+                                acc[c][r] = fmaf(coef[o], v[dx + 2], acc[c][r]);
+                        });
+                    });
                 }
-            }
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-            {
-#pragma unroll
-                for (int r = 0; r < 4; ++r) acc[c][r] = acc[c][r + 1];
-                acc[c][4] = 0.0f;
-            }
-        }
-        __syncwarp();
-        if (lane == 0) mbarArrive(&empty[s]);
-        // Refill the slot of plane m = n - kLag with plane m + kRing.
-        const int m = n - kLag;
-        if (threadIdx.x == 0 && m >= 0 && m + kRing < nin)
+            });
+        });
+    };
+    // Queue slot 0 (output plane zi - 2) is complete: store it, shift.
+    auto storeShift = [&](int zi, bool store) {
+        if (store)
         {
-            const int sm = m % kRing;
-            mbarWait(&empty[sm], (uint32_t)(m / kRing) & 1u, dead);
-            mbarExpectTx(&full[sm], kPlaneBytes);
-            tmaLoadPlane(&ring[sm][0][0][0], &tmap, &full[sm], k0, ux0 - 2, uy0 - 2,
-                         za - 2 + m + kRing);
+            float *o = outBase + (long long)(zi - 2) * planeStride;
+            if (smask & 1) o[0] = acc[0][0] * scale;
+            if (smask & 2) o[colStride] = acc[1][0] * scale;
+            if (smask & 4) o[rowStride] = acc[2][0] * scale;
+            if (smask & 8) o[rowStride + colStride] = acc[3][0] * scale;
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+        {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[c][r] = acc[c][r + 1];
+            acc[c][4] = 0.0f;
+        }
+    };
+    // Consumer release of staged plane m, then the producer's lagged refill.
+    auto release = [&](int m) {
+        __syncwarp();
+        if (lane == 0) mbarArrive(&empty[m % kRing]);
+        const int mr = m - kLag;
+        if (threadIdx.x == 0 && mr >= 0 && mr + kRing < nv)
+        {
+            const int sr = mr % kRing;
+            mbarWait(&empty[sr], (uint32_t)(mr / kRing) & 1u, dead);
+            mbarExpectTx(&full[sr], kPlaneBytes);
+            tmaLoadPlane(&ring[sr][0][0][0], &tmap, &full[sr], k0, ux0 - 2, uy0 - 2,
+                         zlo + mr + kRing);
+        }
+    };
+
+    if (zb - za > 4)
+    {
+        // Long segment: every input plane is staged (the TMA zero-fills any
+        // outside the lattice) and every queue slot takes FMAs; a slot
+        // outside the segment is never stored and leaves as zero shifts in.
+        for (int n = 0; n < nin; ++n)
+        {
+            const int zi = za - 2 + n;
+            const int s = n % kRing;
+            mbarWait(&full[s], (uint32_t)(n / kRing) & 1u, dead);
+            if (active)
+            {
+                fmaPlane(&ring[s][0][0][0], std::false_type{}, [](int) { return true; });
+                storeShift(zi, zi - 2 >= za);
+            }
+            release(n);
+        }
+    }
+    else
+    {
+        // Short segment: planes outside the lattice are not staged, and
+        // only the slots of the unit's own planes take FMAs.
+        const unsigned L = (unsigned)(zb - za);
+        for (int n = 0; n < nin; ++n)
+        {
+            const int zi = za - 2 + n;
+            const int m = n - moff;
+            auto inSeg = [&](int r) { return (unsigned)(n - 4 + r) < L; };
+            if (m >= 0 && m < nv)
+            {
+                const int s = m % kRing;
+                mbarWait(&full[s], (uint32_t)(m / kRing) & 1u, dead);
+                if (active) fmaPlane(&ring[s][0][0][0], std::true_type{}, inSeg);
+                release(m);
+            }
+            if (active) storeShift(zi, inSeg(0));
         }
     }
     if (dead) atomicOr(&sc->err, 2);
@@ -273,8 +309,8 @@ cudaError_t launchMarch(alebgk_ctx *c, const void *tmap, float *outBuf, cudaStre
     dim3 grid(c->march.nunits, c->march.Vpad / kMarchChunk);
     k_march<<<grid, kMarchWarps * 32, kRing * kPlaneBytes, st>>>(*m, c->march.units,
                                                                  c->march.coefT, outBuf,
-                                               c->march.Nx, c->march.Ny, p.V, c->march.Vpad,
-                                               p.ldf, c->d.sc);
+                                               c->march.Nx, c->march.Ny, c->march.Nz, p.V,
+                                               c->march.Vpad, p.ldf, c->d.sc);
     return cudaGetLastError();
 }
 
