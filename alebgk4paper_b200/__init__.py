@@ -17,7 +17,7 @@ import numpy as np
 
 from . import _abi
 
-__all__ = ["Case", "Solver", "AlebgkError", "load_library", "CASE_NAMES"]
+__all__ = ["Case", "Solver", "AlebgkError", "load_library", "read_checkpoint", "CASE_NAMES"]
 
 CASE_NAMES = ("cavity2d", "cavity3d", "cavity2d-square", "cavity2d-circle",
               "cavity3d-sphere", "cavity3d-cube")
@@ -49,6 +49,34 @@ def _check(rc: int, ctx=None):
         buf = ctypes.create_string_buffer(512)
         lib.alebgk_last_error(ctx, buf, 512)
         raise AlebgkError(rc, buf.value.decode(errors="replace"))
+
+
+def read_checkpoint(path: str, N: int | None = None, gstride: int | None = None,
+                    dim: int | None = None, nbodies: int | None = None) -> dict:
+    """Reads a restart file in the reference's layout (Core/Checkpoint.hpp)
+    on the host: header fields plus xyz, meshv, wall, boundary, body_id, g,
+    macro, voxel and the body states.  Expected shapes default to the
+    file's own."""
+    lib = _abi.load()
+    h = _abi.CkptHeader()
+    _check(lib.alebgk_checkpoint_header(str(path).encode(), ctypes.byref(h)))
+    exp = _abi.CkptHeader(N=h.N if N is None else N, gstride=h.gstride if gstride is None
+                          else gstride, step=h.step, t=h.t,
+                          dim=h.dim if dim is None else dim,
+                          nbodies=h.nbodies if nbodies is None else nbodies)
+    n, gs, nb = int(exp.N), int(exp.gstride), int(exp.nbodies)
+    out = dict(step=int(h.step), t=float(h.t), dim=int(h.dim), N=n, gstride=gs,
+               xyz=np.zeros((n, 3)), meshv=np.zeros((n, 3)), wall=np.zeros((n, 7)),
+               boundary=np.zeros(n, np.int32), body_id=np.zeros(n, np.int32),
+               g=np.zeros((n, gs)), macro=np.zeros((n, 7)), voxel=np.zeros(n, np.int32))
+    cl = _abi.Cloud(_dp(out["xyz"]), _dp(out["meshv"]), _dp(out["wall"]), _ip(out["boundary"]),
+                    _ip(out["body_id"]), None, None, _dp(out["g"]), _dp(out["macro"]))
+    bodies = (_abi.Body * max(1, nb))()
+    _check(lib.alebgk_checkpoint_read(str(path).encode(), ctypes.byref(exp), ctypes.byref(cl),
+                                      _ip(out["voxel"]), bodies))
+    out["bodies"] = np.array([[bodies[b].state[k] for k in range(32)] for b in range(nb)])
+    out["body_rotates"] = np.array([bodies[b].rotates for b in range(nb)], np.int32)
+    return out
 
 
 class Case:
@@ -265,6 +293,49 @@ class Solver:
         g, macro = self.cudaDownloadFull()
         c.xyz, c.meshv, c.wall, c.g, c.macro = xyz, mv, wall, g, macro
         self.cudaUploadCloud(c)
+
+    def checkpoint_save(self, path: str, step: int = 0, t: float = 0.0,
+                        bodies: np.ndarray | None = None, voxel: np.ndarray | None = None):
+        """Writes a restart file in the reference's layout (Core/Checkpoint.hpp)
+        from the device state; ``bodies`` (nbodies x 32) defaults to the
+        case's."""
+        c = self.case
+        st = np.ascontiguousarray(c.bodies if bodies is None else bodies, np.float64)
+        nb = st.shape[0]
+        arr = (_abi.Body * max(1, nb))()
+        for b in range(nb):
+            arr[b].kind = int(c.body_kind[b])
+            arr[b].rotates = int(c.body_rotates[b])
+            arr[b].size = float(c.body_size[b])
+            for k in range(32):
+                arr[b].state[k] = float(st[b, k])
+        vg = np.array([c.params["vmin"], c.params["vmax"], c.params["dv"]])
+        vox = None if voxel is None else np.ascontiguousarray(voxel, np.int32)
+        _check(self.lib.alebgk_checkpoint_save(self.ctx, str(path).encode(), int(step),
+                                               float(t), _dp(vg),
+                                               None if vox is None else _ip(vox), nb, arr),
+               self.ctx)
+
+    def checkpoint_restore(self, path: str) -> dict:
+        """Reads a restart file of this cloud's shape and continues from it:
+        distribution and macros go to the device; if the file's geometry
+        (positions, mesh velocity, wall state) differs from the current one,
+        the cloud is uploaded again with it (neighbour lists kept).  Returns
+        the file's contents (step, t, bodies, ...)."""
+        c = self.case
+        d = read_checkpoint(path, N=self.N, gstride=self.gstride, dim=self.dim,
+                            nbodies=c.nbodies)
+        xyz, mv, wall = self.download_geometry()
+        if (np.array_equal(xyz, d["xyz"]) and np.array_equal(mv, d["meshv"])
+                and np.array_equal(wall, d["wall"])):
+            g = np.ascontiguousarray(d["g"])
+            m = np.ascontiguousarray(d["macro"])
+            _check(self.lib.alebgk_upload_state(self.ctx, _dp(g), _dp(m)), self.ctx)
+        else:
+            c.xyz, c.meshv, c.wall = d["xyz"], d["meshv"], d["wall"]
+            c.g, c.macro = d["g"], d["macro"]
+            self.cudaUploadCloud(c)
+        return d
 
     def download_geometry(self):
         """(xyz N x 3, meshv N x 3, wall N x 7) as stored on the device."""

@@ -44,6 +44,11 @@ class Body(ctypes.Structure):
                 ("state", ctypes.c_double * 32)]
 
 
+class CkptHeader(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_uint64), ("gstride", ctypes.c_uint64), ("step", ctypes.c_uint64),
+                ("t", ctypes.c_double), ("dim", ctypes.c_uint32), ("nbodies", ctypes.c_uint32)]
+
+
 class Counters(ctypes.Structure):
     _fields_ = [
         ("steps", ctypes.c_int64), ("transport_flags", ctypes.c_int),
@@ -91,6 +96,13 @@ SIGNATURES = {
     "alebgk_download_geometry": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p,
                                                 c_double_p]),
     "alebgk_case_body_shapes": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p, c_double_p]),
+    "alebgk_checkpoint_header": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(CkptHeader)]),
+    "alebgk_checkpoint_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(CkptHeader),
+                                              ctypes.POINTER(Cloud), c_int_p,
+                                              ctypes.POINTER(Body)]),
+    "alebgk_checkpoint_save": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int64,
+                                              ctypes.c_double, c_double_p, c_int_p, ctypes.c_int,
+                                              ctypes.POINTER(Body)]),
     "alebgk_body_set_surface_velocity": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
                                                         c_double_p, c_double_p]),
     "alebgk_case_build": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int,

@@ -300,6 +300,7 @@ int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
         return fail(c, ALEBGK_EINVAL,
                     "the lattice march needs FP32 and a complete 3-D lattice cloud");
     c->bodyIdHost.assign(cl->body_id, cl->body_id + N);
+    c->boundaryHost.assign(cl->boundary, cl->boundary + N);
     c->cur = 0;
     c->uploaded = true;
     return alebgk_upload_state(c, cl->g, cl->macro);
@@ -638,6 +639,37 @@ int alebgk_download_geometry(alebgk_ctx *c, double *xyz, double *meshv, double *
     if (meshv) CK(cudaMemcpy(meshv, c->d.meshv, 24 * N, cudaMemcpyDeviceToHost));
     if (wall) CK(cudaMemcpy(wall, c->d.wall, 56 * N, cudaMemcpyDeviceToHost));
     return ALEBGK_OK;
+}
+
+int alebgk_checkpoint_header(const char *path, alebgk_ckpt_header *out)
+{
+    if (!path || !out) return fail(nullptr, ALEBGK_EINVAL, "null argument");
+    std::string err;
+    const int rc = checkpointHeader(path, out, &err);
+    return rc ? fail(nullptr, rc, err) : ALEBGK_OK;
+}
+
+int alebgk_checkpoint_read(const char *path, const alebgk_ckpt_header *expect,
+                           alebgk_cloud *cloud, int *voxel, alebgk_body *bodies)
+{
+    if (!path || !expect || !cloud) return fail(nullptr, ALEBGK_EINVAL, "null argument");
+    std::string err;
+    const int rc = checkpointRead(path, expect, cloud, voxel, bodies, &err);
+    return rc ? fail(nullptr, rc, err) : ALEBGK_OK;
+}
+
+int alebgk_checkpoint_save(alebgk_ctx *c, const char *path, int64_t step, double t,
+                           const double *vgrid, const int *voxel, int nbodies,
+                           const alebgk_body *bodies)
+{
+    if (!c || !path) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (nbodies < 0 || (nbodies > 0 && !bodies))
+        return fail(c, ALEBGK_EINVAL, "bodies missing");
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    CK(cudaSetDevice(c->cfg.device));
+    std::string err;
+    const int rc = checkpointSave(c, path, step, t, vgrid, voxel, nbodies, bodies, &err);
+    return rc ? fail(c, rc, "checkpoint: " + err) : ALEBGK_OK;
 }
 
 // ---------------------------------------------------------------------------

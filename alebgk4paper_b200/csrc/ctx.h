@@ -109,6 +109,7 @@ struct alebgk_ctx
     size_t pStreamSmem = 0;
     std::string err;
     std::vector<int> bodyIdHost;
+    std::vector<int> boundaryHost;
     std::vector<int> surfHost;   // body-surface particle indices, ascending
     bool geometryDirty = false;  // a body step moved the surface since the upload
 };
@@ -129,6 +130,12 @@ constexpr int kMaxBodyIO = 64;                 // bodies per body call
 constexpr int kBodyIOHead = 13 * kMaxBodyIO;   // doubles before the surface rows
 cudaError_t bodyStep(alebgk_ctx *c, int nbodies, alebgk_body *bodies, const double *box,
                      double dx, double dt, std::string *err);
+// Restart files in the reference's checkpoint layout (checkpoint.cpp).
+int checkpointHeader(const char *path, alebgk_ckpt_header *out, std::string *err);
+int checkpointRead(const char *path, const alebgk_ckpt_header *expect, alebgk_cloud *cl,
+                   int *voxel, alebgk_body *bodies, std::string *err);
+int checkpointSave(alebgk_ctx *c, const char *path, int64_t step, double t, const double *vgrid,
+                   const int *voxel, int nbodies, const alebgk_body *bodies, std::string *err);
 // Body loads on the fixed device scratch of body_noalloc.cu (no allocation).
 constexpr int kNoAllocMaxBodies = ALEBGK_NOALLOC_MAX_BODIES;
 cudaError_t bodyLoadsNoAlloc(alebgk_ctx *c, int nbodies, const double *centre,

@@ -261,6 +261,44 @@ int alebgk_body_set_surface_velocity(alebgk_ctx *ctx, int nbodies,
                                      const double *body_centre,
                                      const double *state);
 
+/* ---- restart files ------------------------------------------------------
+ * The reference's checkpoint layout (Core/Checkpoint.hpp:37-236, magic
+ * "ALEBGK01", version 1): header, one record per particle, N*gStride FP64
+ * values of g, one record per body.  Files written here restore with the
+ * reference's ckpt::restore, and the reference's files read here. */
+typedef struct alebgk_ckpt_header
+{
+    uint64_t N;
+    uint64_t gstride;
+    uint64_t step;
+    double t;
+    uint32_t dim;
+    uint32_t nbodies;
+} alebgk_ckpt_header;
+
+/* Header of a restart file (host only). */
+int alebgk_checkpoint_header(const char *path, alebgk_ckpt_header *out);
+
+/* Reads a restart file into host arrays (host only): the non-NULL members
+ * xyz, meshv, wall, boundary, body_id, g, macro of cloud (nnb, nbr
+ * untouched: the reference rebuilds neighbour lists after a restore),
+ * voxel (N, may be NULL) and the state and rotates flag of nbodies bodies
+ * (may be NULL).  Fails, reading nothing past the header, if the file's N,
+ * gstride, dim or body count differs from *expect. */
+int alebgk_checkpoint_read(const char *path, const alebgk_ckpt_header *expect,
+                           alebgk_cloud *cloud, int *voxel, alebgk_body *bodies);
+
+/* Writes the context's state as a restart file: g (FP64, staged through
+ * pinned buffers, device copy overlapping the file write), macros,
+ * positions, mesh velocity and wall state from the device, boundary flags
+ * and body ids from the upload.  vgrid = {vlo, vhi, dv} per particle (NULL:
+ * from the configuration), voxel may be NULL (0), bodies may be NULL if
+ * nbodies is 0.  The file is written to path.tmp and renamed.  Replaces
+ * ckpt::save (Core/Checkpoint.hpp:84-155) after a cudaDownloadFull. */
+int alebgk_checkpoint_save(alebgk_ctx *ctx, const char *path, int64_t step, double t,
+                           const double *vgrid, const int *voxel, int nbodies,
+                           const alebgk_body *bodies);
+
 /* ---- host-side MLS coefficient tables (no device work) -------------------
  * The stencil classes and FP64 transport coefficients that alebgk_upload
  * builds: gt[i][k] = sum_s coef[cls[i]][s][k] * g[slots[i][s]][k], slot 0 =

@@ -245,6 +245,23 @@ class RefCase:
     def set_threads(self, n):
         self.L.ref_set_threads(int(n))
 
+    def checkpoint_save(self, path: str) -> bool:
+        """The reference's ckpt::save (Core/Checkpoint.hpp:84-155)."""
+        return bool(self.L.ref_checkpoint_save(self.h, path.encode()))
+
+    def checkpoint_load(self, path: str):
+        """The reference's ckpt::restore (Core/Checkpoint.hpp:157-236)."""
+        step = ctypes.c_long()
+        t = ctypes.c_double()
+        ok = self.L.ref_checkpoint_load(self.h, path.encode(), ctypes.byref(step),
+                                        ctypes.byref(t))
+        return bool(ok), step.value, t.value
+
+    def checkpoint_sizes(self):
+        out = (ctypes.c_int * 3)()
+        self.L.ref_checkpoint_sizes(out)
+        return tuple(out)
+
     def max_threads(self):
         return self.L.ref_max_threads()
 

@@ -23,6 +23,7 @@
 #include "MLSTransport.hpp"
 #include "RigidBody.hpp"
 #include "TestCases.hpp"
+#include "Checkpoint.hpp"
 
 #include <cmath>
 #include <cstring>
@@ -342,6 +343,29 @@ void ref_get_bodies(void *h, double *out)
             o[22 + k] = Rm ? Rm[k] : ((k % 4) == 0 ? 1.0 : 0.0);
         o[31] = r.getSurfaceArea();
     }
+}
+
+// The reference's own restart files (Core/Checkpoint.hpp): save the case's
+// state, restore into it, and the record sizes of the format.
+int ref_checkpoint_save(void *h, const char *path)
+{
+    auto *c = static_cast<RefCase *>(h);
+    return ckpt::save(path, c->step, c->t, c->P, c->bodies) ? 1 : 0;
+}
+
+int ref_checkpoint_load(void *h, const char *path, long *step, double *t)
+{
+    auto *c = static_cast<RefCase *>(h);
+    const bool ok = ckpt::restore(path, step, t, c->P, c->bodies);
+    if (ok) { c->step = *step; c->t = *t; }
+    return ok ? 1 : 0;
+}
+
+void ref_checkpoint_sizes(int *out)
+{
+    out[0] = (int)sizeof(ckpt::Header);
+    out[1] = (int)sizeof(ckpt::PRec);
+    out[2] = (int)sizeof(ckpt::BRec);
 }
 
 }  // extern "C"
