@@ -88,12 +88,14 @@ class Case:
     """
 
     def __init__(self, name: str, Nx: int = -1, Nv: int = -1, dt: float = -1.0,
-                 mls_order: int = 2, fixed_body: bool = False, body_scale: float = 1.0):
+                 mls_order: int = 2, fixed_body: bool = False, body_scale: float = 1.0,
+                 lid_speed: float = -1.0, rho0: float = -1.0, tau: float = -1.0):
         lib = _abi.load()
         h = ctypes.c_void_p()
-        _check(lib.alebgk_case_build(name.encode(), int(Nx), int(Nv), float(dt),
-                                     int(mls_order), int(bool(fixed_body)),
-                                     float(body_scale), ctypes.byref(h)))
+        _check(lib.alebgk_case_build_ex(name.encode(), int(Nx), int(Nv), float(dt),
+                                        int(mls_order), int(bool(fixed_body)),
+                                        float(body_scale), float(lid_speed), float(rho0),
+                                        float(tau), ctypes.byref(h)))
         try:
             info = np.zeros(8, np.int32)
             prm = np.zeros(24)
@@ -336,6 +338,36 @@ class Solver:
             c.g, c.macro = d["g"], d["macro"]
             self.cudaUploadCloud(c)
         return d
+
+    def set_launch(self, transport_threads: int, particle_warps: int):
+        _check(self.lib.alebgk_set_launch(self.ctx, int(transport_threads), int(particle_warps)),
+               self.ctx)
+
+    def get_launch(self):
+        t = ctypes.c_int()
+        w = ctypes.c_int()
+        _check(self.lib.alebgk_get_launch(self.ctx, ctypes.byref(t), ctypes.byref(w)), self.ctx)
+        return t.value, w.value
+
+    def autotune(self, steps: int = 3) -> float:
+        """Keeps the fastest launch shape; returns its ms per step."""
+        ms = ctypes.c_float()
+        _check(self.lib.alebgk_autotune(self.ctx, int(steps), ctypes.byref(ms)), self.ctx)
+        return ms.value
+
+    def residual(self) -> float:
+        """Steady residual of the last step (relative change of the conserved
+        moments over the interior particles)."""
+        r = ctypes.c_double()
+        _check(self.lib.alebgk_residual(self.ctx, ctypes.byref(r)), self.ctx)
+        return r.value
+
+    def residual_interval(self) -> float:
+        """Mean steady residual per step since the previous call (-1 on the
+        first call, which only takes the snapshot)."""
+        r = ctypes.c_double()
+        _check(self.lib.alebgk_residual_interval(self.ctx, ctypes.byref(r)), self.ctx)
+        return r.value
 
     def download_geometry(self):
         """(xyz N x 3, meshv N x 3, wall N x 7) as stored on the device."""

@@ -96,6 +96,22 @@ SIGNATURES = {
     "alebgk_download_geometry": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_double_p,
                                                 c_double_p]),
     "alebgk_case_body_shapes": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p, c_double_p]),
+    "alebgk_set_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "alebgk_get_launch": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p]),
+    "alebgk_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_float)]),
+    "alebgk_residual": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "alebgk_residual_interval": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "alebgk_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                           ctypes.POINTER(ctypes.c_void_p)]),
+    "alebgk_batch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "alebgk_batch_residuals": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "alebgk_batch_sync": (ctypes.c_int, [ctypes.c_void_p]),
+    "alebgk_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "alebgk_case_build_ex": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                            ctypes.c_double, ctypes.POINTER(ctypes.c_void_p)]),
     "alebgk_checkpoint_header": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(CkptHeader)]),
     "alebgk_checkpoint_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(CkptHeader),
                                               ctypes.POINTER(Cloud), c_int_p,

@@ -49,6 +49,9 @@ void freeBuffers(alebgk_ctx *c)
     for (void *p : ptrs)
         if (p) cudaFree(p);
     d = DeviceBuffers();
+    if (c->macSnap) { cudaFree(c->macSnap); c->macSnap = nullptr; }
+    c->snapSteps = -1;
+    c->hostSteps = 0;
     if (c->march.units) cudaFree(c->march.units);
     if (c->march.coefT) cudaFree(c->march.coefT);
     c->march = MarchState();
@@ -365,6 +368,7 @@ int alebgk_step(alebgk_ctx *c, int nsteps)
         }
         CK(cudaGraphLaunch(c->graph[from], c->stream));
         c->cur = 1 - from;
+        ++c->hostSteps;
     }
     return ALEBGK_OK;
 }
@@ -750,6 +754,32 @@ int alebgk_case_build(const char *name, int Nx, int Nv, double dt, int mls_order
     CaseParams prm;
     if (!configureCase(id, Nx, Nv, dt, mls_order, fixed_body != 0, prm))
         return fail(nullptr, ALEBGK_EINVAL, "configureCase failed");
+    auto *c = new (std::nothrow) alebgk_case();
+    if (!c) return fail(nullptr, ALEBGK_ENOMEM, "host allocation failed");
+    std::string err;
+    if (!buildCloud(prm, body_scale, c->cloud, &err))
+    {
+        delete c;
+        return fail(nullptr, ALEBGK_EINVAL, err);
+    }
+    *out = c;
+    return ALEBGK_OK;
+}
+
+int alebgk_case_build_ex(const char *name, int Nx, int Nv, double dt, int mls_order,
+                         int fixed_body, double body_scale, double lid_speed, double rho0,
+                         double tau, alebgk_case **out)
+{
+    if (!name || !out) return fail(nullptr, ALEBGK_EINVAL, "null argument");
+    *out = nullptr;
+    int id = 0;
+    if (!caseByName(name, &id)) return fail(nullptr, ALEBGK_EINVAL, std::string("unknown case ") + name);
+    CaseParams prm;
+    if (!configureCase(id, Nx, Nv, dt, mls_order, fixed_body != 0, prm))
+        return fail(nullptr, ALEBGK_EINVAL, "configureCase failed");
+    if (lid_speed > 0) prm.lidSpeed = lid_speed;
+    if (rho0 > 0) prm.rho0 = rho0;
+    if (tau > 0) prm.tau = tau;
     auto *c = new (std::nothrow) alebgk_case();
     if (!c) return fail(nullptr, ALEBGK_ENOMEM, "host allocation failed");
     std::string err;

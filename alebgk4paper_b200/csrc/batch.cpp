@@ -1,0 +1,313 @@
+// batch.cpp -- launch-shape autotuning, the steady residual, and batches of
+// independent cavities advanced by one CUDA graph per step.
+//
+// A batch holds contexts on one device that advance in lockstep.  One graph
+// per ping-pong parity holds every context's whole step (and its residual)
+// as a parallel branch: a master stream forks to each context's stream and
+// joins them again, so one graph launch advances all cavities and the small
+// kernels of different cavities share the SMs.
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "ctx.h"
+
+using namespace alebgk;
+
+struct alebgk_batch
+{
+    std::vector<alebgk_ctx *> ctx;
+    int device = 0;
+    cudaStream_t master = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    double *resid = nullptr;              // device, one per context
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    std::string err;
+};
+
+namespace {
+
+int failc(alebgk_ctx *c, int code, const std::string &msg)
+{
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CKC(call)                                                                      \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess)                                                         \
+            return failc(c, ALEBGK_ECUDA, std::string(#call) + ": " +                 \
+                                              cudaGetErrorString(e_));                 \
+    } while (0)
+
+void dropGraphs(alebgk_ctx *c)
+{
+    for (auto &g : c->graph)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+}  // namespace
+
+extern "C" {
+
+int alebgk_set_launch(alebgk_ctx *c, int transport_threads, int particle_warps)
+{
+    if (!c) return ALEBGK_EINVAL;
+    if (transport_threads < 32 || transport_threads > 256 || transport_threads % 32)
+        return failc(c, ALEBGK_EINVAL, "transport threads: a multiple of 32 in 32..256");
+    if (particle_warps < 0 || particle_warps > 8)
+        return failc(c, ALEBGK_EINVAL, "particle warps: 0 (as many as fit) or 1..8");
+    if (c->tune.transportThreads != transport_threads || c->tune.particleWarps != particle_warps)
+    {
+        c->tune.transportThreads = transport_threads;
+        c->tune.particleWarps = particle_warps;
+        dropGraphs(c);
+    }
+    return ALEBGK_OK;
+}
+
+int alebgk_get_launch(alebgk_ctx *c, int *transport_threads, int *particle_warps)
+{
+    if (!c || !transport_threads || !particle_warps) return ALEBGK_EINVAL;
+    *transport_threads = c->tune.transportThreads;
+    *particle_warps = c->tune.particleWarps;
+    return ALEBGK_OK;
+}
+
+int alebgk_autotune(alebgk_ctx *c, int steps, float *best_ms)
+{
+    if (!c) return ALEBGK_EINVAL;
+    if (!c->uploaded) return failc(c, ALEBGK_ESTATE, "upload the cloud first");
+    if (steps < 1) return failc(c, ALEBGK_EINVAL, "steps must be >= 1");
+    CKC(cudaSetDevice(c->cfg.device));
+    CKC(cudaStreamSynchronize(c->stream));
+    // Snapshot of everything a step reads: the current distribution and
+    // macros, the moodCheck flags and the step scalars.
+    const StepParams &p = c->sp;
+    const size_t es = (c->cfg.precision == 64) ? 8 : 4;
+    const size_t fBytes = (size_t)p.N * p.ldf * es, mBytes = 48 * (size_t)p.N;
+    const int cur0 = c->cur;
+    void *snapF = nullptr, *snapM = nullptr, *snapMood = nullptr, *snapSc = nullptr;
+    CKC(cudaMalloc(&snapF, fBytes));
+    CKC(cudaMalloc(&snapM, mBytes));
+    CKC(cudaMalloc(&snapMood, 4 * (size_t)p.N));
+    CKC(cudaMalloc(&snapSc, sizeof(StepScalars)));
+    cudaError_t e = cudaMemcpy(snapF, c->d.f[cur0], fBytes, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(snapM, c->d.macro[cur0], mBytes, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(snapMood, c->d.mood, 4 * (size_t)p.N, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(snapSc, c->d.sc, sizeof(StepScalars), cudaMemcpyDeviceToDevice);
+    auto restore = [&]() {
+        c->cur = cur0;
+        cudaError_t r = cudaMemcpy(c->d.f[cur0], snapF, fBytes, cudaMemcpyDeviceToDevice);
+        if (r == cudaSuccess)
+            r = cudaMemcpy(c->d.macro[cur0], snapM, mBytes, cudaMemcpyDeviceToDevice);
+        if (r == cudaSuccess) r = cudaMemcpy(c->d.mood, snapMood, 4 * (size_t)p.N, cudaMemcpyDeviceToDevice);
+        if (r == cudaSuccess) r = cudaMemcpy(c->d.sc, snapSc, sizeof(StepScalars), cudaMemcpyDeviceToDevice);
+        return r;
+    };
+    const int tts[] = {64, 128, 256};
+    const int pws[] = {1, 2, 4, 0};
+    float best = -1.0f;
+    int bestT = c->tune.transportThreads, bestW = c->tune.particleWarps;
+    int rc = ALEBGK_OK;
+    for (int tt : tts)
+    {
+        for (int pw : pws)
+        {
+            if (e != cudaSuccess || rc != ALEBGK_OK) break;
+            rc = alebgk_set_launch(c, tt, pw);
+            float ms = 0.0f;
+            if (rc == ALEBGK_OK) rc = alebgk_step(c, 2);      // captures both graphs
+            if (rc == ALEBGK_OK) rc = alebgk_step_timed(c, steps, &ms);
+            e = restore();
+            if (rc == ALEBGK_OK && e == cudaSuccess && (best < 0 || ms < best))
+            {
+                best = ms;
+                bestT = tt;
+                bestW = pw;
+            }
+        }
+    }
+    cudaFree(snapF);
+    cudaFree(snapM);
+    cudaFree(snapMood);
+    cudaFree(snapSc);
+    if (e != cudaSuccess)
+        return failc(c, ALEBGK_ECUDA, std::string("autotune: ") + cudaGetErrorString(e));
+    if (rc != ALEBGK_OK) return rc;
+    rc = alebgk_set_launch(c, bestT, bestW);
+    if (best_ms) *best_ms = best / steps;
+    return rc;
+}
+
+int alebgk_residual(alebgk_ctx *c, double *res)
+{
+    if (!c || !res) return ALEBGK_EINVAL;
+    if (!c->uploaded) return failc(c, ALEBGK_ESTATE, "upload the cloud first");
+    CKC(cudaSetDevice(c->cfg.device));
+    CKC(launchResidual(c, c->d.redPartial, c->stream));
+    CKC(cudaMemcpyAsync(res, c->d.redPartial, 8, cudaMemcpyDeviceToHost, c->stream));
+    CKC(cudaStreamSynchronize(c->stream));
+    return ALEBGK_OK;
+}
+
+int alebgk_residual_interval(alebgk_ctx *c, double *res)
+{
+    if (!c || !res) return ALEBGK_EINVAL;
+    if (!c->uploaded) return failc(c, ALEBGK_ESTATE, "upload the cloud first");
+    CKC(cudaSetDevice(c->cfg.device));
+    const size_t mBytes = 48 * (size_t)c->sp.N;
+    if (!c->macSnap) CKC(cudaMalloc(&c->macSnap, mBytes));
+    *res = -1.0;
+    const long long k = c->hostSteps - c->snapSteps;
+    if (c->snapSteps >= 0 && k > 0)
+    {
+        // residual of "one step" from the snapshot to now, per step
+        const int keep = c->cur;
+        double *old = c->d.macro[1 - keep];
+        c->d.macro[1 - keep] = c->macSnap;
+        const cudaError_t e = launchResidual(c, c->d.redPartial, c->stream);
+        c->d.macro[1 - keep] = old;
+        CKC(e);
+        CKC(cudaMemcpyAsync(res, c->d.redPartial, 8, cudaMemcpyDeviceToHost, c->stream));
+        CKC(cudaStreamSynchronize(c->stream));
+        *res /= (double)k;
+    }
+    CKC(cudaMemcpyAsync(c->macSnap, c->d.macro[c->cur], mBytes, cudaMemcpyDeviceToDevice,
+                        c->stream));
+    CKC(cudaStreamSynchronize(c->stream));
+    c->snapSteps = c->hostSteps;
+    return ALEBGK_OK;
+}
+
+int alebgk_batch_create(int n, alebgk_ctx **ctxs, alebgk_batch **out)
+{
+    if (!ctxs || !out || n < 1) return ALEBGK_EINVAL;
+    *out = nullptr;
+    for (int i = 0; i < n; ++i)
+    {
+        alebgk_ctx *c = ctxs[i];
+        if (!c || !c->uploaded) return ALEBGK_ESTATE;
+        if (c->geometryDirty) return failc(c, ALEBGK_ESTATE, "upload the cloud again first");
+        if (c->cfg.device != ctxs[0]->cfg.device)
+            return failc(c, ALEBGK_EINVAL, "a batch lives on one device");
+        if (c->cur != ctxs[0]->cur)
+            return failc(c, ALEBGK_EINVAL, "the contexts of a batch must be in step");
+        for (int j = 0; j < i; ++j)
+            if (ctxs[j] == c) return failc(c, ALEBGK_EINVAL, "a context appears twice");
+    }
+    auto *b = new (std::nothrow) alebgk_batch();
+    if (!b) return ALEBGK_ENOMEM;
+    b->ctx.assign(ctxs, ctxs + n);
+    b->device = ctxs[0]->cfg.device;
+    b->join.assign(n, nullptr);
+    cudaError_t e = cudaSetDevice(b->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->master, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    for (int i = 0; i < n && e == cudaSuccess; ++i)
+        e = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMalloc(&b->resid, 8 * (size_t)n);
+    if (e == cudaSuccess) e = cudaMemset(b->resid, 0, 8 * (size_t)n);
+    if (e != cudaSuccess)
+    {
+        alebgk_batch_destroy(b);
+        return ALEBGK_ECUDA;
+    }
+    *out = b;
+    return ALEBGK_OK;
+}
+
+int alebgk_batch_step(alebgk_batch *b, int nsteps)
+{
+    if (!b || nsteps < 0) return ALEBGK_EINVAL;
+    alebgk_ctx *c = b->ctx[0];
+    CKC(cudaSetDevice(b->device));
+    for (alebgk_ctx *x : b->ctx)
+        if (x->geometryDirty || x->cur != c->cur)
+            return failc(x, ALEBGK_ESTATE, "a context of the batch left the lockstep");
+    for (int n = 0; n < nsteps; ++n)
+    {
+        const int from = c->cur;
+        if (!b->graph[from])
+        {
+            cudaGraph_t g = nullptr;
+            CKC(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
+            cudaError_t le = cudaEventRecord(b->fork, b->master);
+            for (size_t i = 0; i < b->ctx.size() && le == cudaSuccess; ++i)
+            {
+                alebgk_ctx *x = b->ctx[i];
+                le = cudaStreamWaitEvent(x->stream, b->fork, 0);
+                if (le == cudaSuccess) le = launchStep(x, from);
+                // the residual compares the new macros with the old ones
+                const int keep = x->cur;
+                x->cur = 1 - from;
+                if (le == cudaSuccess) le = launchResidual(x, b->resid + i, x->stream);
+                x->cur = keep;
+                if (le == cudaSuccess) le = cudaEventRecord(b->join[i], x->stream);
+                if (le == cudaSuccess) le = cudaStreamWaitEvent(b->master, b->join[i], 0);
+            }
+            cudaError_t ee = cudaStreamEndCapture(b->master, &g);
+            if (le != cudaSuccess || ee != cudaSuccess)
+            {
+                if (g) cudaGraphDestroy(g);
+                return failc(c, ALEBGK_ECUDA,
+                             std::string("batch capture: ") +
+                                 cudaGetErrorString(le != cudaSuccess ? le : ee));
+            }
+            cudaError_t ie = cudaGraphInstantiate(&b->graph[from], g, 0);
+            cudaGraphDestroy(g);
+            if (ie != cudaSuccess)
+                return failc(c, ALEBGK_ECUDA, std::string("batch graph: ") + cudaGetErrorString(ie));
+        }
+        CKC(cudaGraphLaunch(b->graph[from], b->master));
+        for (alebgk_ctx *x : b->ctx)
+        {
+            x->cur = 1 - from;
+            ++x->hostSteps;
+        }
+    }
+    // the contexts' own streams see the batch's work before their next call
+    CKC(cudaEventRecord(b->fork, b->master));
+    for (alebgk_ctx *x : b->ctx) CKC(cudaStreamWaitEvent(x->stream, b->fork, 0));
+    return ALEBGK_OK;
+}
+
+int alebgk_batch_residuals(alebgk_batch *b, double *out)
+{
+    if (!b || !out) return ALEBGK_EINVAL;
+    alebgk_ctx *c = b->ctx[0];
+    CKC(cudaSetDevice(b->device));
+    CKC(cudaMemcpyAsync(out, b->resid, 8 * b->ctx.size(), cudaMemcpyDeviceToHost, b->master));
+    CKC(cudaStreamSynchronize(b->master));
+    return ALEBGK_OK;
+}
+
+int alebgk_batch_sync(alebgk_batch *b)
+{
+    if (!b) return ALEBGK_EINVAL;
+    alebgk_ctx *c = b->ctx[0];
+    CKC(cudaSetDevice(b->device));
+    CKC(cudaStreamSynchronize(b->master));
+    return ALEBGK_OK;
+}
+
+int alebgk_batch_destroy(alebgk_batch *b)
+{
+    if (!b) return ALEBGK_OK;
+    cudaSetDevice(b->device);
+    if (b->master) cudaStreamSynchronize(b->master);
+    for (auto &g : b->graph)
+        if (g) cudaGraphExecDestroy(g);
+    for (auto &e : b->join)
+        if (e) cudaEventDestroy(e);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->resid) cudaFree(b->resid);
+    if (b->master) cudaStreamDestroy(b->master);
+    delete b;
+    return ALEBGK_OK;
+}
+
+}  // extern "C"

@@ -103,6 +103,12 @@ struct alebgk_ctx
     int ncls = 0;
     int degenerateParticles = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    // Launch shapes of the general kernels (alebgk_set_launch / autotune).
+    struct
+    {
+        int transportThreads = 256;   // coefficient-gather transport, per block
+        int particleWarps = 0;        // warp-per-particle kernel; 0 = as many as fit
+    } tune;
     // Streamed particle kernel: on, warps per block, blocks, dynamic smem.
     bool pStream = false;
     int pStreamWpb = 0, pStreamBlocks = 0;
@@ -112,6 +118,9 @@ struct alebgk_ctx
     std::vector<int> boundaryHost;
     std::vector<int> surfHost;   // body-surface particle indices, ascending
     bool geometryDirty = false;  // a body step moved the surface since the upload
+    long long hostSteps = 0;     // steps enqueued since the upload
+    double *macSnap = nullptr;   // macros at the last interval residual (N x 6)
+    long long snapSteps = -1;    // hostSteps of that snapshot (-1: none)
 };
 
 namespace alebgk {
@@ -140,6 +149,7 @@ int checkpointSave(alebgk_ctx *c, const char *path, int64_t step, double t, cons
 constexpr int kNoAllocMaxBodies = ALEBGK_NOALLOC_MAX_BODIES;
 cudaError_t bodyLoadsNoAlloc(alebgk_ctx *c, int nbodies, const double *centre,
                              const double *area, double *out, std::string *err);
+cudaError_t launchResidual(alebgk_ctx *c, double *out, cudaStream_t st);
 cudaError_t launchConvertIn(alebgk_ctx *c, const double *src, int buf);
 cudaError_t launchConvertOut(alebgk_ctx *c, double *dst, int buf);
 cudaError_t launchMarch(alebgk_ctx *c, const void *tmap, float *outBuf, cudaStream_t st);

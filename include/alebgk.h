@@ -261,6 +261,46 @@ int alebgk_body_set_surface_velocity(alebgk_ctx *ctx, int nbodies,
                                      const double *body_centre,
                                      const double *state);
 
+/* ---- launch shapes, steady residual, batches ------------------------------
+ * No reference counterpart: the reference runs one cavity per process. */
+
+/* Launch shapes of the general kernels: threads per block of the
+ * coefficient-gather transport (a multiple of 32 in 32..256) and particles
+ * (warps) per block of the warp-per-particle kernel (1..8; 0 = as many as
+ * their shared-memory rows allow).  The lattice march and the streamed
+ * particle kernel have fixed shapes.  Drops the captured step graphs. */
+int alebgk_set_launch(alebgk_ctx *ctx, int transport_threads, int particle_warps);
+int alebgk_get_launch(alebgk_ctx *ctx, int *transport_threads, int *particle_warps);
+
+/* Times every candidate launch shape over `steps` steps, each on a device
+ * snapshot of the state that is restored afterwards, and keeps the fastest;
+ * *best_ms (may be NULL) is its time per step. */
+int alebgk_autotune(alebgk_ctx *ctx, int steps, float *best_ms);
+
+/* Steady residual of the last step over the interior particles: the largest
+ * of ||d rho|| / ||rho||, ||d(rho ux)|| / ||rho c||, ||d(rho uy)|| / ||rho c||
+ * and ||d(rho E)|| / ||rho E|| (2-norms over particles, E = |u|^2/2 + 3RT/2,
+ * c = sqrt(RT) the thermal speed, so that momentum changes are measured
+ * against the thermal momentum).  The reference defines no residual. */
+int alebgk_residual(alebgk_ctx *ctx, double *res);
+
+/* The same measure between the macros of the previous call and now,
+ * divided by the steps in between: the mean change per step over the
+ * interval, in which the FP32 rounding noise of single steps averages out.
+ * The first call only takes the snapshot and returns -1. */
+int alebgk_residual_interval(alebgk_ctx *ctx, double *res);
+
+/* Independent cavities on one device advanced in lockstep by one CUDA graph
+ * launch per step: each context's whole step and residual is a parallel
+ * branch of the graph.  The contexts stay usable on their own between
+ * batch calls, as long as they stay in step. */
+typedef struct alebgk_batch alebgk_batch;
+int alebgk_batch_create(int n, alebgk_ctx **ctxs, alebgk_batch **out);
+int alebgk_batch_step(alebgk_batch *b, int nsteps);
+int alebgk_batch_residuals(alebgk_batch *b, double *out);   /* n residuals */
+int alebgk_batch_sync(alebgk_batch *b);
+int alebgk_batch_destroy(alebgk_batch *b);
+
 /* ---- restart files ------------------------------------------------------
  * The reference's checkpoint layout (Core/Checkpoint.hpp:37-236, magic
  * "ALEBGK01", version 1): header, one record per particle, N*gStride FP64
@@ -326,6 +366,13 @@ int alebgk_case_build(const char *name, int Nx, int Nv, double dt,
                       int mls_order, int fixed_body, double body_scale,
                       alebgk_case **out);
 void alebgk_case_free(alebgk_case *c);
+
+/* The same with the lid speed (m/s), initial density and relaxation time
+ * of the case overridden where > 0 (the batched-cavity workloads vary
+ * them; the reference varies them by editing TestCases.cpp). */
+int alebgk_case_build_ex(const char *name, int Nx, int Nv, double dt, int mls_order,
+                         int fixed_body, double body_scale, double lid_speed, double rho0,
+                         double tau, alebgk_case **out);
 
 /* info[0..7]  = N, dim, Nv, gstride, nbodies, mls_order, Nx, moving_bodies
  * prm[0..23]  = dt, tau, R, dx, dy, dz, radius, minDist, dv, vmin, vmax,
