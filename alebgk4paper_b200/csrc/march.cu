@@ -105,7 +105,8 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
     const int moff = zlo - (za - 2);            // staged index m = n - moff
     const bool active = warp < u.nsub;
     const int sub = active ? __ldg(&u.sub[warp]) : 0;
-    const int bx = sub & 15, by = (sub >> 4) & 15, mask = (sub >> 8) & 15, cls = sub >> 12;
+    const int bx = sub & 15, by = (sub >> 4) & 15, mask = (sub >> 8) & 15;
+    const int shape = (sub >> 12) & 3, cls = sub >> 14;
     if (threadIdx.x == 0)
     {
         // An earlier CTA that timed out set the error word: skip the work.
@@ -147,32 +148,48 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
     const int smask = (k < V) ? mask : 0;
     bool dead = false;
 
-    // The FMAs of one staged plane into the queue; with `gated`, only the
-    // slots holding the unit's own output planes (inSeg(r)).
-    auto fmaPlane = [&](const float *P, auto GATED, auto inSeg) {
+    // The FMAs of one staged plane into the queue for a warp block of shape
+    // SHAPE (column c at (CX(c), CY(c)) from the block origin); with
+    // `gated`, only the slots holding the unit's own output planes.
+    auto fmaPlane = [&](auto SHAPE, const float *P, auto GATED, auto inSeg) {
+        constexpr int shp = decltype(SHAPE)::value;
         constexpr bool gated = decltype(GATED)::value;
-        unroll<6>([&](auto DY) {
-            constexpr int dy = decltype(DY)::value - 2;
-            float v[6];
-            unroll<6>([&](auto DX) {
-                constexpr int dx = decltype(DX)::value - 2;
-                constexpr bool need = tidx(dx, dy, 0) >= 0 || tidx(dx - 1, dy, 0) >= 0 ||
-                                      tidx(dx, dy - 1, 0) >= 0 || tidx(dx - 1, dy - 1, 0) >= 0;
+        constexpr auto CX = [](int c) { return shp == kShapeBlock ? (c & 1)
+                                               : shp == kShapeColumn ? 0 : c; };
+        constexpr auto CY = [](int c) { return shp == kShapeBlock ? (c >> 1)
+                                               : shp == kShapeColumn ? c : 0; };
+        constexpr int EX = (shp == kShapeRow) ? 8 : (shp == kShapeBlock ? 6 : 5);
+        constexpr int EY = (shp == kShapeColumn) ? 8 : (shp == kShapeBlock ? 6 : 5);
+        // Outer loop along the block's long side, so that one short line of
+        // the neighbourhood (at most six values) is live at a time.
+        constexpr bool xMajor = (shp == kShapeRow);
+        constexpr int EA = xMajor ? EX : EY, EB = xMajor ? EY : EX;
+        unroll<EA>([&](auto A) {
+            float v[EB];
+            unroll<EB>([&](auto B) {
+                constexpr int dx = (xMajor ? decltype(A)::value : decltype(B)::value) - 2;
+                constexpr int dy = (xMajor ? decltype(B)::value : decltype(A)::value) - 2;
+                constexpr bool need = tidx(dx - CX(0), dy - CY(0), 0) >= 0 ||
+                                      tidx(dx - CX(1), dy - CY(1), 0) >= 0 ||
+                                      tidx(dx - CX(2), dy - CY(2), 0) >= 0 ||
+                                      tidx(dx - CX(3), dy - CY(3), 0) >= 0;
                 if constexpr (need)
-                    v[dx + 2] = P[((by + dy + 2) * kPW + (bx + dx + 2)) * kMarchChunk + lane];
+                    v[decltype(B)::value] =
+                        P[((by + dy + 2) * kPW + (bx + dx + 2)) * kMarchChunk + lane];
             });
             unroll<5>([&](auto R) {
                 constexpr int r = decltype(R)::value;
                 constexpr int dz = 2 - r;
                 if (!gated || inSeg(r))
                 {
-                    unroll<6>([&](auto DX) {
-                        constexpr int dx = decltype(DX)::value - 2;
+                    unroll<EB>([&](auto B) {
+                        constexpr int dx = (xMajor ? decltype(A)::value : decltype(B)::value) - 2;
+                        constexpr int dy = (xMajor ? decltype(B)::value : decltype(A)::value) - 2;
                         unroll<4>([&](auto C) {
                             constexpr int c = decltype(C)::value;
-                            constexpr int o = tidx(dx - (c & 1), dy - (c >> 1), dz);
+                            constexpr int o = tidx(dx - CX(c), dy - CY(c), dz);
                             if constexpr (o >= 0)
-                                acc[c][r] = fmaf(coef[o], v[dx + 2], acc[c][r]);
+                                acc[c][r] = fmaf(coef[o], v[decltype(B)::value], acc[c][r]);
                         });
                     });
                 }
@@ -180,14 +197,18 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
         });
     };
     // Queue slot 0 (output plane zi - 2) is complete: store it, shift.
-    auto storeShift = [&](int zi, bool store) {
+    auto storeShift = [&](auto SHAPE, int zi, bool store) {
+        constexpr int shp = decltype(SHAPE)::value;
         if (store)
         {
             float *o = outBase + (long long)(zi - 2) * planeStride;
+            const int s1 = (shp == kShapeColumn) ? rowStride : colStride;
+            const int s2 = (shp == kShapeBlock) ? rowStride : 2 * s1;
+            const int s3 = (shp == kShapeBlock) ? rowStride + colStride : 3 * s1;
             if (smask & 1) o[0] = acc[0][0] * scale;
-            if (smask & 2) o[colStride] = acc[1][0] * scale;
-            if (smask & 4) o[rowStride] = acc[2][0] * scale;
-            if (smask & 8) o[rowStride + colStride] = acc[3][0] * scale;
+            if (smask & 2) o[s1] = acc[1][0] * scale;
+            if (smask & 4) o[s2] = acc[2][0] * scale;
+            if (smask & 8) o[s3] = acc[3][0] * scale;
         }
 #pragma unroll
         for (int c = 0; c < 4; ++c)
@@ -212,11 +233,10 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
         }
     };
 
-    if (zb - za > 4)
-    {
-        // Long segment: every input plane is staged (the TMA zero-fills any
-        // outside the lattice) and every queue slot takes FMAs; a slot
-        // outside the segment is never stored and leaves as zero shifts in.
+    // Long segment: every input plane is staged (the TMA zero-fills any
+    // outside the lattice) and every queue slot takes FMAs; a slot outside
+    // the segment is never stored and leaves as zero shifts in.
+    auto marchLong = [&](auto SHAPE) {
         for (int n = 0; n < nin; ++n)
         {
             const int zi = za - 2 + n;
@@ -224,16 +244,15 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
             mbarWait(&full[s], (uint32_t)(n / kRing) & 1u, dead);
             if (active)
             {
-                fmaPlane(&ring[s][0][0][0], std::false_type{}, [](int) { return true; });
-                storeShift(zi, zi - 2 >= za);
+                fmaPlane(SHAPE, &ring[s][0][0][0], std::false_type{}, [](int) { return true; });
+                storeShift(SHAPE, zi, zi - 2 >= za);
             }
             release(n);
         }
-    }
-    else
-    {
-        // Short segment: planes outside the lattice are not staged, and
-        // only the slots of the unit's own planes take FMAs.
+    };
+    // Short segment: planes outside the lattice are not staged, and only the
+    // slots of the unit's own planes take FMAs.
+    auto marchShort = [&](auto SHAPE) {
         const unsigned L = (unsigned)(zb - za);
         for (int n = 0; n < nin; ++n)
         {
@@ -244,11 +263,26 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
             {
                 const int s = m % kRing;
                 mbarWait(&full[s], (uint32_t)(m / kRing) & 1u, dead);
-                if (active) fmaPlane(&ring[s][0][0][0], std::true_type{}, inSeg);
+                if (active) fmaPlane(SHAPE, &ring[s][0][0][0], std::true_type{}, inSeg);
                 release(m);
             }
-            if (active) storeShift(zi, inSeg(0));
+            if (active) storeShift(SHAPE, zi, inSeg(0));
         }
+    };
+    using ShapeBlock = std::integral_constant<int, kShapeBlock>;
+    using ShapeColumn = std::integral_constant<int, kShapeColumn>;
+    using ShapeRow = std::integral_constant<int, kShapeRow>;
+    if (zb - za > 4)
+    {
+        if (shape == kShapeColumn) marchLong(ShapeColumn{});
+        else if (shape == kShapeRow) marchLong(ShapeRow{});
+        else marchLong(ShapeBlock{});
+    }
+    else
+    {
+        if (shape == kShapeColumn) marchShort(ShapeColumn{});
+        else if (shape == kShapeRow) marchShort(ShapeRow{});
+        else marchShort(ShapeBlock{});
     }
     if (dead) atomicOr(&sc->err, 2);
 }

@@ -5,8 +5,8 @@
 // and every neighbour lies within two lattice steps, the transport is a
 // stencil over lattice positions: gt(x,y,z;k) = sum_o C[class][o][k] f(x+o;k)
 // over the 81 offsets |o|^2 <= 6 (self included).  The plan groups lattice
-// columns into work units of class-uniform 2x2 column blocks that march
-// through z.
+// columns into work units of class-uniform four-column blocks (2x2, 1x4 or
+// 4x1) that march through z.
 #pragma once
 #include <cstdint>
 #include <vector>
@@ -24,11 +24,18 @@ constexpr int kMarchChunk = 32;     // velocities per CTA (one per lane)
 // Canonical template offset index of (dx, dy, dz), or -1 if outside.
 int templateIndex(int dx, int dy, int dz);
 
+// Warp block shapes: the four columns c = 0..3 of a block at (bx, by) are
+// (bx + (c & 1), by + (c >> 1)) for kShapeBlock, (bx, by + c) for
+// kShapeColumn and (bx + c, by) for kShapeRow.
+constexpr int kShapeBlock = 0;    // 2 x 2
+constexpr int kShapeColumn = 1;   // 1 x 4 (one lattice x, four y)
+constexpr int kShapeRow = 2;      // 4 x 1 (four x, one lattice y)
+
 struct MarchUnit
 {
     int x0, y0, za, zb;   // tile origin (columns) and output planes [za, zb)
     int nsub;             // active warps
-    int sub[kMarchWarps]; // bx | by << 4 | mask << 8 | class << 12
+    int sub[kMarchWarps]; // bx | by << 4 | mask << 8 | shape << 12 | class << 14
 };
 
 struct MarchPlan

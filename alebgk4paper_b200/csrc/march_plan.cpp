@@ -126,27 +126,56 @@ void buildMarchPlan(const double *xyz, int N, int dim, const int *nnb, const int
     }
     cuts.push_back(nz);
 
-    // Work units: per segment and 8x4 column tile, class-uniform (partial)
-    // 2x2 blocks, at most kMarchWarps per unit.
+    // Work units: per segment and 8x4 column tile, the tile's columns are
+    // covered by class-uniform warp blocks: whole 2x2 blocks first, then
+    // 1x4 strips along y (one column x), then 4x1 strips along x, and what
+    // is left by 2x2 blocks split per class (masked).  The strips cover the
+    // columns next to the tile's x and y walls, whose classes change from
+    // column to column.  At most kMarchWarps blocks per unit.
     for (size_t sgi = 0; sgi + 1 < cuts.size(); ++sgi)
     {
         const int za = cuts[sgi], zb = cuts[sgi + 1];
         for (int y0 = 0; y0 < ny; y0 += kMarchTileY)
             for (int x0 = 0; x0 < nx; x0 += kMarchTileX)
             {
+                // class of tile column (bx, by), or -1 outside the lattice
+                int tc[kMarchTileY][kMarchTileX];
+                for (int by = 0; by < kMarchTileY; ++by)
+                    for (int bx = 0; bx < kMarchTileX; ++bx)
+                    {
+                        const int x = x0 + bx, y = y0 + by;
+                        tc[by][bx] = (x < nx && y < ny) ? cls(x, y, za) : -1;
+                    }
                 std::vector<int> subs;
+                auto take = [&](int bx, int by, int shape, const int (&cx)[4],
+                                const int (&cy)[4]) {
+                    const int k = tc[by + cy[0]][bx + cx[0]];
+                    if (k < 0) return;
+                    for (int q = 1; q < 4; ++q)
+                        if (tc[by + cy[q]][bx + cx[q]] != k) return;
+                    for (int q = 0; q < 4; ++q) tc[by + cy[q]][bx + cx[q]] = -1;
+                    subs.push_back(bx | by << 4 | 15 << 8 | shape << 12 | k << 14);
+                };
+                const int bX[4] = {0, 1, 0, 1}, bY[4] = {0, 0, 1, 1};     // 2x2
+                const int vX[4] = {0, 0, 0, 0}, vY[4] = {0, 1, 2, 3};     // 1x4
+                const int hX[4] = {0, 1, 2, 3}, hY[4] = {0, 0, 0, 0};     // 4x1
+                for (int by = 0; by < kMarchTileY; by += 2)
+                    for (int bx = 0; bx < kMarchTileX; bx += 2) take(bx, by, kShapeBlock, bX, bY);
+                for (int bx = 0; bx < kMarchTileX; ++bx) take(bx, 0, kShapeColumn, vX, vY);
+                for (int by = 0; by < kMarchTileY; ++by)
+                    for (int bx = 0; bx < kMarchTileX; bx += 4) take(bx, by, kShapeRow, hX, hY);
                 for (int by = 0; by < kMarchTileY; by += 2)
                     for (int bx = 0; bx < kMarchTileX; bx += 2)
                     {
                         std::map<int, int> masks;   // class -> column mask
                         for (int q = 0; q < 4; ++q)
                         {
-                            const int x = x0 + bx + (q & 1), y = y0 + by + (q >> 1);
-                            if (x >= nx || y >= ny) continue;
-                            masks[cls(x, y, za)] |= 1 << q;
+                            const int k = tc[by + (q >> 1)][bx + (q & 1)];
+                            if (k >= 0) masks[k] |= 1 << q;
                         }
                         for (auto &m : masks)
-                            subs.push_back(bx | by << 4 | m.second << 8 | m.first << 12);
+                            subs.push_back(bx | by << 4 | m.second << 8 | kShapeBlock << 12 |
+                                           m.first << 14);
                     }
                 for (size_t a = 0; a < subs.size(); a += kMarchWarps)
                 {
@@ -158,7 +187,7 @@ void buildMarchPlan(const double *xyz, int N, int dim, const int *nnb, const int
                 }
             }
     }
-    plan.ok = ncls < (1 << 19);
+    plan.ok = ncls < (1 << 17);
 }
 
 }  // namespace alebgk
