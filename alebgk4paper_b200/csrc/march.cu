@@ -4,7 +4,8 @@
 // offsets |o|^2 <= 6, for a cloud that is a complete lattice (march.h).
 //
 // CTA = one work unit (an 8x4 tile of lattice columns, output planes
-// [za, zb)) x one chunk of 32 velocities, lane = velocity.  The CTA marches
+// [za, zb)) x one chunk of 32 velocities, lane = velocity; the chunks of a
+// unit are consecutive CTAs.  The CTA marches
 // through z: every input plane of the tile plus a two-column halo (12x8
 // particles x 32 velocities, 12 KB) is brought into a six-slot shared-
 // memory ring by one TMA tensor load (cp.async.bulk.tensor.4d, completion on
@@ -93,9 +94,11 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
     __shared__ int giveUp;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const MarchUnit &u = units[blockIdx.x];
+    // blockIdx.x = velocity chunk, blockIdx.y = unit: the chunks of one unit
+    // run back to back and read the same rows of f while they are in L2.
+    const MarchUnit &u = units[blockIdx.y];
     const int ux0 = u.x0, uy0 = u.y0, za = u.za, zb = u.zb;
-    const int k0 = blockIdx.y * kMarchChunk;
+    const int k0 = blockIdx.x * kMarchChunk;
     const int k = k0 + lane;
     const int nin = zb - za + 4;                 // input planes za-2 .. zb+1
     // Planes outside the lattice hold zeros: they are not staged; the queue
@@ -340,7 +343,7 @@ cudaError_t launchMarch(alebgk_ctx *c, const void *tmap, float *outBuf, cudaStre
 {
     const StepParams &p = c->sp;
     const CUtensorMap *m = static_cast<const CUtensorMap *>(tmap);
-    dim3 grid(c->march.nunits, c->march.Vpad / kMarchChunk);
+    dim3 grid(c->march.Vpad / kMarchChunk, c->march.nunits);
     k_march<<<grid, kMarchWarps * 32, kRing * kPlaneBytes, st>>>(*m, c->march.units,
                                                                  c->march.coefT, outBuf,
                                                c->march.Nx, c->march.Ny, c->march.Nz, p.V,
