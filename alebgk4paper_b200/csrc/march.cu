@@ -200,11 +200,10 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
         });
     };
     // Queue slot 0 (output plane zi - 2) is complete: store it, shift.
-    auto storeShift = [&](auto SHAPE, int zi, bool store) {
+    auto storeShift = [&](auto SHAPE, float *o, bool store) {
         constexpr int shp = decltype(SHAPE)::value;
         if (store)
         {
-            float *o = outBase + (long long)(zi - 2) * planeStride;
             const int s1 = (shp == kShapeColumn) ? rowStride : colStride;
             const int s2 = (shp == kShapeBlock) ? rowStride : 2 * s1;
             const int s3 = (shp == kShapeBlock) ? rowStride + colStride : 3 * s1;
@@ -222,14 +221,16 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
         }
     };
     // Consumer release of staged plane m, then the producer's lagged refill.
-    auto release = [&](int m) {
+    // Staged plane m sits in ring slot s with phase parity par.
+    auto release = [&](int m, int s, uint32_t par) {
         __syncwarp();
-        if (lane == 0) mbarArrive(&empty[m % kRing]);
+        if (lane == 0) mbarArrive(&empty[s]);
         const int mr = m - kLag;
         if (threadIdx.x == 0 && mr >= 0 && mr + kRing < nv)
         {
-            const int sr = mr % kRing;
-            mbarWait(&empty[sr], (uint32_t)(mr / kRing) & 1u, dead);
+            const int sr = (s >= kLag) ? s - kLag : s - kLag + kRing;
+            const uint32_t pr = (s >= kLag) ? par : par ^ 1u;
+            mbarWait(&empty[sr], pr, dead);
             mbarExpectTx(&full[sr], kPlaneBytes);
             tmaLoadPlane(&ring[sr][0][0][0], &tmap, &full[sr], k0, ux0 - 2, uy0 - 2,
                          zlo + mr + kRing);
@@ -240,36 +241,42 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
     // outside the lattice) and every queue slot takes FMAs; a slot outside
     // the segment is never stored and leaves as zero shifts in.
     auto marchLong = [&](auto SHAPE) {
+        int s = 0;
+        uint32_t par = 0;
+        float *o = outBase + (long long)(za - 4) * planeStride;   // plane zi - 2 at n = 0
         for (int n = 0; n < nin; ++n)
         {
-            const int zi = za - 2 + n;
-            const int s = n % kRing;
-            mbarWait(&full[s], (uint32_t)(n / kRing) & 1u, dead);
+            mbarWait(&full[s], par, dead);
             if (active)
             {
                 fmaPlane(SHAPE, &ring[s][0][0][0], std::false_type{}, [](int) { return true; });
-                storeShift(SHAPE, zi, zi - 2 >= za);
+                storeShift(SHAPE, o, n >= 4);
             }
-            release(n);
+            release(n, s, par);
+            o += planeStride;
+            if (++s == kRing) { s = 0; par ^= 1u; }
         }
     };
     // Short segment: planes outside the lattice are not staged, and only the
     // slots of the unit's own planes take FMAs.
     auto marchShort = [&](auto SHAPE) {
         const unsigned L = (unsigned)(zb - za);
+        int s = 0;
+        uint32_t par = 0;
+        float *o = outBase + (long long)(za - 4) * planeStride;
         for (int n = 0; n < nin; ++n)
         {
-            const int zi = za - 2 + n;
             const int m = n - moff;
             auto inSeg = [&](int r) { return (unsigned)(n - 4 + r) < L; };
             if (m >= 0 && m < nv)
             {
-                const int s = m % kRing;
-                mbarWait(&full[s], (uint32_t)(m / kRing) & 1u, dead);
+                mbarWait(&full[s], par, dead);
                 if (active) fmaPlane(SHAPE, &ring[s][0][0][0], std::true_type{}, inSeg);
-                release(m);
+                release(m, s, par);
+                if (++s == kRing) { s = 0; par ^= 1u; }
             }
-            if (active) storeShift(SHAPE, zi, inSeg(0));
+            if (active) storeShift(SHAPE, o, inSeg(0));
+            o += planeStride;
         }
     };
     using ShapeBlock = std::integral_constant<int, kShapeBlock>;

@@ -9,7 +9,7 @@
 
 namespace alebgk {
 
-constexpr long long kSpinLimit = 1ll << 20;
+constexpr int kSpinLimit = 1 << 20;
 
 __device__ __forceinline__ uint32_t smemAddr(const void *p)
 {
@@ -56,7 +56,7 @@ __device__ __forceinline__ bool mbarTryWait(uint64_t *bar, uint32_t parity)
 __device__ __forceinline__ bool mbarWait(uint64_t *bar, uint32_t parity, bool &dead)
 {
     if (dead) return false;
-    for (long long it = 0; it < kSpinLimit; ++it)
+    for (int it = 0; it < kSpinLimit; ++it)
         if (mbarTryWait(bar, parity)) return true;
     dead = true;
     return false;
