@@ -54,6 +54,7 @@ void freeBuffers(alebgk_ctx *c)
     c->hostSteps = 0;
     if (c->march.units) cudaFree(c->march.units);
     if (c->march.coefT) cudaFree(c->march.coefT);
+    if (c->march.coefTy) cudaFree(c->march.coefTy);
     c->march = MarchState();
     for (auto &g : c->graph)
         if (g) { cudaGraphExecDestroy(g); g = nullptr; }
@@ -284,17 +285,32 @@ int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
         if (plan.ok)
         {
             MarchState &m = c->march;
-            m.nunits = (int)plan.units.size();
+            // one list, the long y-march units first
+            std::vector<MarchUnit> all(plan.unitsY);
+            all.insert(all.end(), plan.units.begin(), plan.units.end());
+            m.nunits = (int)all.size();
+            m.nunitsY = (int)plan.unitsY.size();
             m.Vpad = plan.Vpad; m.Nx = plan.Nx; m.Ny = plan.Ny; m.Nz = plan.Nz;
             CK(cudaMalloc(&m.units, sizeof(MarchUnit) * m.nunits));
-            CK(cudaMemcpy(m.units, plan.units.data(), sizeof(MarchUnit) * m.nunits,
+            CK(cudaMemcpy(m.units, all.data(), sizeof(MarchUnit) * m.nunits,
                           cudaMemcpyHostToDevice));
             CK(cudaMalloc(&m.coefT, plan.coefT.size() * 4));
             CK(cudaMemcpy(m.coefT, plan.coefT.data(), plan.coefT.size() * 4,
                           cudaMemcpyHostToDevice));
+            if (m.nunitsY > 0)
+            {
+                CK(cudaMalloc(&m.coefTy, plan.coefTy.size() * 4));
+                CK(cudaMemcpy(m.coefTy, plan.coefTy.data(), plan.coefTy.size() * 4,
+                              cudaMemcpyHostToDevice));
+            }
             for (int b = 0; b < 2; ++b)
-                if (!encodeMarchMap(m.tmap[b], d.f[b], p.V, m.Nx, m.Ny, m.Nz, p.ldf, &err))
+            {
+                if (!encodeMarchMap(m.tmap[b], d.f[b], p.V, m.Nx, m.Ny, m.Nz, p.ldf, false, &err))
                     return fail(c, ALEBGK_ECUDA, err);
+                if (m.nunitsY > 0 &&
+                    !encodeMarchMap(m.tmapY[b], d.f[b], p.V, m.Nx, m.Ny, m.Nz, p.ldf, true, &err))
+                    return fail(c, ALEBGK_ECUDA, err);
+            }
             CK(prepareMarch());
             m.enabled = true;
         }

@@ -16,10 +16,11 @@ struct MarchUnit;
 struct MarchState
 {
     bool enabled = false;
-    int nunits = 0, Vpad = 0, Nx = 0, Ny = 0, Nz = 0;
-    MarchUnit *units = nullptr;
-    float *coefT = nullptr;
+    int nunits = 0, nunitsY = 0, Vpad = 0, Nx = 0, Ny = 0, Nz = 0;
+    MarchUnit *units = nullptr;               // y-march units first, then z-march
+    float *coefT = nullptr, *coefTy = nullptr;
     alignas(64) unsigned char tmap[2][128];   // CUtensorMap per source buffer
+    alignas(64) unsigned char tmapY[2][128];  // the same with the y-march box
 };
 
 // Per-step scalars kept on the device so that a step needs no host
@@ -152,9 +153,9 @@ cudaError_t bodyLoadsNoAlloc(alebgk_ctx *c, int nbodies, const double *centre,
 cudaError_t launchResidual(alebgk_ctx *c, double *out, cudaStream_t st);
 cudaError_t launchConvertIn(alebgk_ctx *c, const double *src, int buf);
 cudaError_t launchConvertOut(alebgk_ctx *c, double *dst, int buf);
-cudaError_t launchMarch(alebgk_ctx *c, const void *tmap, float *outBuf, cudaStream_t st);
+cudaError_t launchMarch(alebgk_ctx *c, int from, float *outBuf, cudaStream_t st);
 cudaError_t prepareMarch();
 bool encodeMarchMap(void *tmapOut, void *f, int V, int Nx, int Ny, int Nz, int ldf,
-                    std::string *err);
+                    bool yMarch, std::string *err);
 
 }  // namespace alebgk

@@ -83,9 +83,10 @@ __device__ __forceinline__ void tmaLoadPlane(void *dst, const CUtensorMap *map, 
 }  // namespace
 
 __global__ void __launch_bounds__(kMarchWarps * 32, 2)
-k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ units,
-        const float *__restrict__ coefT, float *__restrict__ out, int Nx, int Ny, int Nz,
-        int V, int Vpad, int ldf, StepScalars *sc)
+k_march(const __grid_constant__ CUtensorMap tmapZ, const __grid_constant__ CUtensorMap tmapY,
+        const MarchUnit *__restrict__ units, const float *__restrict__ coefTz,
+        const float *__restrict__ coefTy, float *__restrict__ out, int ldf, int Nx, int Ny,
+        int Nz, int V, int Vpad, StepScalars *sc)
 {
     extern __shared__ __align__(128) unsigned char marchSmem[];
     typedef float Plane[kPH][kPW][kMarchChunk];
@@ -98,12 +99,21 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
     // run back to back and read the same rows of f while they are in L2.
     const MarchUnit &u = units[blockIdx.y];
     const int ux0 = u.x0, uy0 = u.y0, za = u.za, zb = u.zb;
+    // Orientation: z-march tiles are (x, y) at one z; y-march tiles (x, z)
+    // at one y, with the coefficients in that frame.
+    const bool yMarch = u.yMarch != 0;
+    const CUtensorMap *tmap = yMarch ? &tmapY : &tmapZ;
+    const float *coefT = yMarch ? coefTy : coefTz;
+    const int colStride = ldf;
+    const int rowStride = yMarch ? ldf * Nx * Ny : ldf * Nx;
+    const int planeStride = yMarch ? ldf * Nx : ldf * Nx * Ny;
+    const int marchLen = yMarch ? Ny : Nz;
     const int k0 = blockIdx.x * kMarchChunk;
     const int k = k0 + lane;
     const int nin = zb - za + 4;                 // input planes za-2 .. zb+1
     // Planes outside the lattice hold zeros: they are not staged; the queue
     // only moves past them.  Staged plane m is lattice plane zlo + m.
-    const int zlo = max(za - 2, 0), zhi = min(zb + 1, Nz - 1);
+    const int zlo = max(za - 2, 0), zhi = min(zb + 1, marchLen - 1);
     const int nv = zhi - zlo + 1;
     const int moff = zlo - (za - 2);            // staged index m = n - moff
     const bool active = warp < u.nsub;
@@ -124,11 +134,19 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
     }
     __syncthreads();
     if (giveUp) return;
+    // Plane z of the march: (x, y) tile rows at lattice z, or in the y-march
+    // frame (x, lattice z) rows at lattice y (a box one y deep, eight z).
+    auto loadPlane = [&](void *dst, uint64_t *bar, int z) {
+        if (yMarch)
+            tmaLoadPlane(dst, tmap, bar, k0, ux0 - 2, z, uy0 - 2);
+        else
+            tmaLoadPlane(dst, tmap, bar, k0, ux0 - 2, uy0 - 2, z);
+    };
     if (threadIdx.x == 0)
         for (int m = 0; m < kRing && m < nv; ++m)
         {
             mbarExpectTx(&full[m], kPlaneBytes);
-            tmaLoadPlane(&ring[m][0][0][0], &tmap, &full[m], k0, ux0 - 2, uy0 - 2, zlo + m);
+            loadPlane(&ring[m][0][0][0], &full[m], zlo + m);
         }
 
     float coef[kTmplOffsets];
@@ -146,8 +164,7 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
     const float scale = (float)sc->scale;
     // Output column c of the warp's block at plane z:
     // outBase + z planeStride + (c & 1) colStride + (c >> 1) rowStride.
-    const int colStride = ldf, rowStride = ldf * Nx, planeStride = rowStride * Ny;
-    float *outBase = out + ((size_t)(ux0 + bx) + (size_t)Nx * (uy0 + by)) * ldf + k;
+    float *outBase = out + (long long)(ux0 + bx) * colStride + (long long)(uy0 + by) * rowStride + k;
     const int smask = (k < V) ? mask : 0;
     bool dead = false;
 
@@ -232,8 +249,7 @@ k_march(const __grid_constant__ CUtensorMap tmap, const MarchUnit *__restrict__ 
             const uint32_t pr = (s >= kLag) ? par : par ^ 1u;
             mbarWait(&empty[sr], pr, dead);
             mbarExpectTx(&full[sr], kPlaneBytes);
-            tmaLoadPlane(&ring[sr][0][0][0], &tmap, &full[sr], k0, ux0 - 2, uy0 - 2,
-                         zlo + mr + kRing);
+            loadPlane(&ring[sr][0][0][0], &full[sr], zlo + mr + kRing);
         }
     };
 
@@ -307,7 +323,7 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t
                                   CUtensorMapFloatOOBfill);
 
 bool encodeMarchMap(void *tmapOut, void *f, int V, int Nx, int Ny, int Nz, int ldf,
-                    std::string *err)
+                    bool yMarch, std::string *err)
 {
     static EncodeTiledFn fn = nullptr;
     if (!fn)
@@ -326,7 +342,11 @@ bool encodeMarchMap(void *tmapOut, void *f, int V, int Nx, int Ny, int Nz, int l
     const cuuint64_t dims[4] = {(cuuint64_t)V, (cuuint64_t)Nx, (cuuint64_t)Ny, (cuuint64_t)Nz};
     const cuuint64_t strides[3] = {(cuuint64_t)ldf * 4, (cuuint64_t)ldf * 4 * Nx,
                                    (cuuint64_t)ldf * 4 * Nx * Ny};
-    const cuuint32_t box[4] = {kMarchChunk, kPW, kPH, 1};
+    // z-march: a 12 x 8 (x, y) tile at one z; y-march: a 12 x 8 (x, z) tile
+    // at one y.  Both land in shared memory as [8][12][32 velocities].
+    const cuuint32_t boxZ[4] = {kMarchChunk, kPW, kPH, 1};
+    const cuuint32_t boxY[4] = {kMarchChunk, kPW, 1, kPH};
+    const cuuint32_t *box = yMarch ? boxY : boxZ;
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     CUresult r = fn(reinterpret_cast<CUtensorMap *>(tmapOut), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
                     f, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -346,15 +366,16 @@ cudaError_t prepareMarch()
                                 (int)(kRing * kPlaneBytes));
 }
 
-cudaError_t launchMarch(alebgk_ctx *c, const void *tmap, float *outBuf, cudaStream_t st)
+cudaError_t launchMarch(alebgk_ctx *c, int from, float *outBuf, cudaStream_t st)
 {
     const StepParams &p = c->sp;
-    const CUtensorMap *m = static_cast<const CUtensorMap *>(tmap);
-    dim3 grid(c->march.Vpad / kMarchChunk, c->march.nunits);
-    k_march<<<grid, kMarchWarps * 32, kRing * kPlaneBytes, st>>>(*m, c->march.units,
-                                                                 c->march.coefT, outBuf,
-                                               c->march.Nx, c->march.Ny, c->march.Nz, p.V,
-                                               c->march.Vpad, p.ldf, c->d.sc);
+    const MarchState &ms = c->march;
+    const CUtensorMap *tz = reinterpret_cast<const CUtensorMap *>(ms.tmap[from]);
+    const CUtensorMap *ty = reinterpret_cast<const CUtensorMap *>(ms.nunitsY ? ms.tmapY[from]
+                                                                              : ms.tmap[from]);
+    k_march<<<dim3(ms.Vpad / kMarchChunk, ms.nunits), kMarchWarps * 32, kRing * kPlaneBytes,
+              st>>>(*tz, *ty, ms.units, ms.coefT, ms.coefTy ? ms.coefTy : ms.coefT, outBuf,
+                    p.ldf, ms.Nx, ms.Ny, ms.Nz, p.V, ms.Vpad, c->d.sc);
     return cudaGetLastError();
 }
 

@@ -20,6 +20,7 @@ constexpr int kMarchTileX = 8;      // CTA column tile
 constexpr int kMarchTileY = 4;
 constexpr int kMarchWarps = 8;      // one 2x2 column block per warp
 constexpr int kMarchChunk = 32;     // velocities per CTA (one per lane)
+constexpr int kThinSegment = 4;     // segments shorter than this are marched across
 
 // Canonical template offset index of (dx, dy, dz), or -1 if outside.
 int templateIndex(int dx, int dy, int dz);
@@ -34,6 +35,7 @@ constexpr int kShapeRow = 2;      // 4 x 1 (four x, one lattice y)
 struct MarchUnit
 {
     int x0, y0, za, zb;   // tile origin (columns) and output planes [za, zb)
+    int yMarch;           // 0: lattice (x, y) columns through z; 1: (x, z) through y
     int nsub;             // active warps
     int sub[kMarchWarps]; // bx | by << 4 | mask << 8 | shape << 12 | class << 14
 };
@@ -43,8 +45,10 @@ struct MarchPlan
     bool ok = false;
     int Nx = 0, Ny = 0, Nz = 0;
     int ncls = 0, Vpad = 0;
-    std::vector<MarchUnit> units;
+    std::vector<MarchUnit> units;    // marching through z
+    std::vector<MarchUnit> unitsY;   // thin z-planes, marching through y
     std::vector<float> coefT;        // [class][81][Vpad]
+    std::vector<float> coefTy;       // the same in the y-march frame
     std::vector<float> coefTLin;     // same, linear MLS
 };
 

@@ -1554,7 +1554,7 @@ static cudaError_t stepT(alebgk_ctx *c, int from, cudaEvent_t *ev)
     mark();
     if (sizeof(T) == 4 && c->march.enabled)
     {
-        cudaError_t e = launchMarch(c, c->march.tmap[from], reinterpret_cast<float *>(fb), st);
+        cudaError_t e = launchMarch(c, from, reinterpret_cast<float *>(fb), st);
         if (e != cudaSuccess) return e;
     }
     else
