@@ -9,6 +9,7 @@ LIB_PATH = os.path.join(HERE, "libalebgk_b200.so")
 
 c_int_p = ctypes.POINTER(ctypes.c_int)
 c_double_p = ctypes.POINTER(ctypes.c_double)
+c_float_p = ctypes.POINTER(ctypes.c_float)
 
 MAX_NEIGH = 128
 NOALLOC_MAX_BODIES = 16        # ALEBGK_NOALLOC_MAX_BODIES
@@ -130,6 +131,25 @@ SIGNATURES = {
     "alebgk_case_bodies": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
     "alebgk_case_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                           ctypes.POINTER(Config)]),
+    "alebgk_moments13": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "alebgk_seed_grad13": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                          c_double_p, c_double_p]),
+    "alebgk_net_nparams": (ctypes.c_int, []),
+    "alebgk_net_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "alebgk_net_destroy": (None, [ctypes.c_void_p]),
+    "alebgk_net_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "alebgk_net_set_params": (ctypes.c_int, [ctypes.c_void_p, c_float_p]),
+    "alebgk_net_get_params": (ctypes.c_int, [ctypes.c_void_p, c_float_p]),
+    "alebgk_net_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_int, ctypes.c_void_p]),
+    "alebgk_net_grad": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_int, c_float_p, c_float_p,
+                                       c_float_p]),
+    "alebgk_net_train_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_int, c_float_p,
+                                             ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                             ctypes.c_float, c_float_p]),
+    "alebgk_net_sync": (ctypes.c_int, [ctypes.c_void_p]),
 }
 
 _lib = None

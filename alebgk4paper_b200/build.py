@@ -19,8 +19,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libalebgk_b200.so")
 
-SOURCES = ["step.cu", "march.cu", "body_noalloc.cu", "body_step.cu", "checkpoint.cpp", "batch.cpp", "api.cpp", "coeffs.cpp", "cases.cpp", "march_plan.cpp"]
-HEADERS = ["ctx.h", "coeffs.h", "cases.h", "march.h", "mbar.cuh"]
+SOURCES = ["step.cu", "march.cu", "body_noalloc.cu", "body_step.cu", "warm.cu", "checkpoint.cpp", "batch.cpp", "api.cpp", "coeffs.cpp", "cases.cpp", "march_plan.cpp"]
+HEADERS = ["ctx.h", "coeffs.h", "cases.h", "march.h", "mbar.cuh", "umma.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -351,6 +351,34 @@ int alebgk_upload_state(alebgk_ctx *c, const double *g, const double *macro)
     return ALEBGK_OK;
 }
 
+int alebgk_moments13(alebgk_ctx *c, double *out)
+{
+    if (!c || !out) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    if (c->sp.dim != 2) return fail(c, ALEBGK_EINVAL, "13 moments are defined for 2-D clouds");
+    CK(cudaSetDevice(c->cfg.device));
+    CK(launchMoments13(c, out));
+    CK(cudaStreamSynchronize(c->stream));
+    return ALEBGK_OK;
+}
+
+int alebgk_seed_grad13(alebgk_ctx *c, const float *net, int ldnet, const double *scale,
+                       const double *shift)
+{
+    if (!c || !net || !scale || !shift) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    if (c->sp.dim != 2) return fail(c, ALEBGK_EINVAL, "the Grad-13 seed is for 2-D clouds");
+    if (ldnet < 9) return fail(c, ALEBGK_EINVAL, "ldnet must be >= 9");
+    CK(cudaSetDevice(c->cfg.device));
+    cudaError_t e = launchSeedGrad13(c, net, ldnet, scale, shift);
+    if (e == cudaSuccess) e = launchMassInit(c);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess)
+        return fail(c, ALEBGK_ECUDA, std::string("grad13 seed: ") + cudaGetErrorString(e));
+    c->snapSteps = -1;
+    return ALEBGK_OK;
+}
+
 int alebgk_step(alebgk_ctx *c, int nsteps)
 {
     if (!c) return ALEBGK_EINVAL;

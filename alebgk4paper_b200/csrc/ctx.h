@@ -130,6 +130,9 @@ namespace alebgk {
 cudaError_t prepareKernels(alebgk_ctx *c);
 cudaError_t launchStep(alebgk_ctx *c, int from, cudaEvent_t *ev = nullptr);
 cudaError_t launchMassInit(alebgk_ctx *c);
+cudaError_t launchSeedGrad13(alebgk_ctx *c, const float *net, int ldnet, const double *scale,
+                             const double *shift);
+cudaError_t launchMoments13(alebgk_ctx *c, double *out);
 cudaError_t launchBodyLoads(alebgk_ctx *c, int nbodies, const double *centreDev,
                             const double *areaDev);
 cudaError_t launchSetSurfaceVelocity(alebgk_ctx *c, int nbodies,

@@ -301,6 +301,53 @@ int alebgk_batch_residuals(alebgk_batch *b, double *out);   /* n residuals */
 int alebgk_batch_sync(alebgk_batch *b);
 int alebgk_batch_destroy(alebgk_batch *b);
 
+/* ---- learned warm start (2-D cavities) -----------------------------------
+ * The reference has no counterpart: it always starts from the Maxwellian at
+ * rest (Initialization/InitialConditions.cpp:18-80).
+ *
+ * 13 moments of the current 2-D state, per particle 9 FP64 values
+ * rho, ux, uy, T, sigma_xx, sigma_xy, sigma_yy, q_x, q_y (sigma the traceless
+ * stress, q the heat flux) taken with the discrete sums of
+ * MomentCalculations/Moments.cpp:66-97.  out_dev is DEVICE memory, N x 9. */
+int alebgk_moments13(alebgk_ctx *ctx, double *out_dev);
+
+/* Seeds the 2-D state from 13-moment fields by Grad's 13-moment expansion in
+ * the Chu representation (g1, g2).  The moments of particle i are
+ * shift[c] + scale[c] * net_dev[i * ldnet + c], c = 0..8, in the order of
+ * alebgk_moments13 (net_dev DEVICE FP32, e.g. the network output rows).
+ * The macros and mass bookkeeping are reset from the seeded rows, as after
+ * alebgk_upload_state. */
+int alebgk_seed_grad13(alebgk_ctx *ctx, const float *net_dev, int ldnet,
+                       const double *scale, const double *shift);
+
+/* Coordinate network: 64 features (x, y, scaled log density, scaled lid
+ * Mach number, and sin/cos(k pi x), sin/cos(k pi y), k = 1..12) -> 4 tanh
+ * layers of width 128 -> 16 outputs (9 used).  BF16 weights, FP32
+ * accumulation in tensor memory, FP32 master weights and Adam state.
+ * Points are DEVICE float4 rows (x/L, y/L, a, b); idx_dev (optional) picks
+ * the batch's rows; targets and outputs are DEVICE FP32 rows of 16. */
+typedef struct alebgk_net alebgk_net;
+int alebgk_net_nparams(void);
+int alebgk_net_create(int device, alebgk_net **out);
+void alebgk_net_destroy(alebgk_net *net);
+const char *alebgk_net_last_error(const alebgk_net *net);
+/* FP32 parameters, flat: W0[128][64], W1..W3[128][128], W4[16][128],
+ * b0..b3[128], b4[16]; rows 9..15 of W4 and b4 are kept zero. */
+int alebgk_net_set_params(alebgk_net *net, const float *host);
+int alebgk_net_get_params(alebgk_net *net, float *host);
+int alebgk_net_forward(alebgk_net *net, const float *pts_dev, const int *idx_dev, int n,
+                       float *out_dev);
+/* Gradient of sum_i sum_c w_c (O_ic - T_ic)^2 / n over the batch (no update);
+ * grad_host receives alebgk_net_nparams() floats. */
+int alebgk_net_grad(alebgk_net *net, const float *pts_dev, const float *tgt_dev,
+                    const int *idx_dev, int n, const float *chan_w, float *grad_host,
+                    float *loss_host);
+/* One Adam step on that loss; loss_host may be NULL (no synchronisation). */
+int alebgk_net_train_step(alebgk_net *net, const float *pts_dev, const float *tgt_dev,
+                          const int *idx_dev, int n, const float *chan_w, float lr,
+                          float beta1, float beta2, float eps, float *loss_host);
+int alebgk_net_sync(alebgk_net *net);
+
 /* ---- restart files ------------------------------------------------------
  * The reference's checkpoint layout (Core/Checkpoint.hpp:37-236, magic
  * "ALEBGK01", version 1): header, one record per particle, N*gStride FP64

@@ -17,8 +17,7 @@ def test_instances_are_seeded_and_in_range():
         assert 0.5 <= s["lid_speed"] <= 10.0 and 0.5 <= s["rho0"] <= 11.0
         assert s["tau"] == 3.7142e-10 / s["rho0"]
         dx = 1e-6 / (s["Nx"] - 1)
-        assert s["dt"] * CAVITY2D_VMAX / dx == 0.75 or math.isclose(
-            s["dt"] * CAVITY2D_VMAX / dx, 0.75, rel_tol=1e-15)
+        assert math.isclose(s["dt"] * CAVITY2D_VMAX / dx, 1.25, rel_tol=1e-15)
     # every choice appears in a batch of 96
     assert {s["Nx"] for s in a} == {24, 32, 40, 48}
     assert {s["Nv"] for s in a} == {16, 20, 24}
