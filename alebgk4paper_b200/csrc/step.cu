@@ -1605,10 +1605,21 @@ static cudaError_t prepareT(alebgk_ctx *c)
     const StepParams &p = c->sp;
     const size_t rowBytes = (size_t)p.L * p.V * sizeof(T);
     const int wpb = particleWarpsPerBlock(p, sizeof(T));
-    cudaError_t e = cudaSuccess;
+    // The dynamic shared-memory cap is an attribute of the kernel, shared by
+    // every context in the process, so it is raised to the device's opt-in
+    // maximum rather than set to this context's need: contexts of different
+    // row sizes (a batch of uneven cavities) then all stay launchable.
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     auto set = [&](const void *fn, size_t bytes) {
+        cudaFuncAttributes fa{};
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
+        const size_t cap = (size_t)optin - fa.sharedSizeBytes;   // minus static shared memory
+        if (e == cudaSuccess && bytes > cap) e = cudaErrorInvalidValue;
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
     };
     set((const void *)k_particle<T, 1>, wpb * rowBytes);
     set((const void *)k_particle<T, 2>, wpb * rowBytes);
@@ -1626,8 +1637,7 @@ static cudaError_t prepareT(alebgk_ctx *c)
         {
             const size_t smem = streamSmemBytes<T>(p.V, p.ldf, w);
             set((const void *)k_particle_stream<T>, smem);
-            int occ = 0, sms = 0, dev = 0;
-            if (e == cudaSuccess) e = cudaGetDevice(&dev);
+            int occ = 0, sms = 0;
             if (e == cudaSuccess)
                 e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
             if (e == cudaSuccess)

@@ -262,10 +262,12 @@ def seed(solver: Solver, net: WarmStartNet, case: Case | None = None):
 
 
 def steady_dataset(specs, tol: float = 1e-6, check_every: int = 25, max_steps: int = 20000,
-                   chunk: int = 96, precision: int = 32, device: int = 0, verbose=False):
-    """Runs batches of cavities to the steady residual and returns per case a
-    dict: inputs (N, 4), mom (N, 9) 13-moment rows, targets (N, 9) scaled,
-    steps to steady (-1 if never)."""
+                   chunk: int = 96, precision: int = 32, device: int = 0, settle: int = 0,
+                   verbose=False):
+    """Runs batches of cavities to the steady residual, then `settle` more
+    steps (the residual tolerance leaves the slow modes a few percent from
+    their limit), and returns per case a dict: inputs (N, 4), mom (N, 9)
+    13-moment rows, targets (N, 9) scaled, steps to steady (-1 if never)."""
     from .batch import BatchSolver
     out = []
     for a in range(0, len(specs), chunk):
@@ -273,6 +275,9 @@ def steady_dataset(specs, tol: float = 1e-6, check_every: int = 25, max_steps: i
         t0 = time.perf_counter()
         b = BatchSolver(part, precision=precision, device=device)
         done = b.run_to_steady(tol=tol, check_every=check_every, max_steps=max_steps)
+        if settle:
+            b.step(settle)
+            b.sync()
         for s, c, d in zip(b.solvers, b.cases, done):
             m = moments13(s)
             out.append(dict(inputs=case_inputs(c), mom=m, targets=case_targets(c, m),

@@ -76,3 +76,22 @@ def test_small_batch_runs_to_steady(gpu):
     assert (done > 0).all()
     assert (b.residuals() < 1e-6).all()
     b.close()
+
+
+def test_uneven_batch_with_smallest_rows_last(gpu):
+    """Cavities with different velocity grids in one batch, the smallest rows
+    uploaded last: every context's kernels must stay launchable (the shared
+    memory cap of a kernel is shared by all contexts of the process)."""
+    specs = [dict(name="cavity2d", Nx=24, Nv=nv, lid_speed=2.0, rho0=1.0, tau=3.7142e-10,
+                  dt=1.25 * (1e-6 / 23) / 1303.0, mls_order=2) for nv in (24, 20, 16)]
+    b = BatchSolver(specs, precision=32)
+    b.step(4)
+    b.sync()
+    alone = [BatchSolver([sp], precision=32) for sp in specs]
+    for a in alone:
+        a.step(4)
+        a.sync()
+    for s, a in zip(b.solvers, alone):
+        np.testing.assert_array_equal(s.cudaDownloadFull()[0], a.solvers[0].cudaDownloadFull()[0])
+        a.close()
+    b.close()
