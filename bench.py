@@ -162,7 +162,29 @@ def recorded_traffic(kernel: str):
 
 
 # ---------------------------------------------------------------------------
+class _StdoutToStderr:
+    """Sends file descriptor 1 to stderr while the reference's CPU code runs:
+    it prints progress lines, and stdout carries only the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        return False
+
+
 def cpu_baseline_reference(seconds_budget: float = 40.0):
+    with _StdoutToStderr():
+        return _cpu_baseline_reference(seconds_budget)
+
+
+def _cpu_baseline_reference(seconds_budget: float):
     """One full reference CPU step of the same workload on all host cores."""
     from oracle.oracle import RefCase, ref_library
     if ref_library() is None:
@@ -185,11 +207,16 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
+    with _StdoutToStderr():
+        line = _run_reference(args)
+    print(json.dumps(line))
+
+
+def _run_reference(args):
     from oracle.oracle import RefCase, ref_library
     if ref_library() is None:
-        print(json.dumps({"impl": "reference",
-                          "unavailable": "oracle/_ref (the compiled reference) is not built"}))
-        return
+        return {"impl": "reference",
+                "unavailable": "oracle/_ref (the compiled reference) is not built"}
     cores = os.cpu_count() or 1
     r = RefCase(WORKLOAD["case"], WORKLOAD["Nx"], WORKLOAD["Nv"], -1.0, WORKLOAD["mls_order"])
     r.set_threads(cores)
@@ -208,7 +235,7 @@ def run_reference(args):
     r.step(k)
     t = time.perf_counter() - t0
     v = updates * k / t
-    print(json.dumps({
+    return {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "updates/s",
         "n_gpus": 0, "steps": k, "warmup": warm + 1, "ms_per_step": 1e3 * t / k,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -220,7 +247,7 @@ def run_reference(args):
                                    f"CPU build {os.path.basename(r.path)}, {cores} OpenMP threads"},
         "e2e": {"value": v, "unit": "updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
-    }))
+    }
 
 
 # ---------------------------------------------------------------------------
