@@ -521,9 +521,28 @@ def run_ncu(args):
     s.close()
 
 
+def run_ncu_warm(args):
+    """Profiler mode of the warm-start workload: the network kernels alone,
+    three inference passes and three training steps on seeded points."""
+    import torch
+    from alebgk4paper_b200 import warm_train as wt
+    from alebgk4paper_b200 import warmstart as ws
+    net = ws.WarmStartNet.load(wt.DEFAULT_MODEL)
+    rng = np.random.default_rng(0)
+    pts = rng.uniform(0, 1, (73728, 4)).astype(np.float32)
+    tgt = rng.normal(size=(73728, 9)).astype(np.float32)
+    for _ in range(3):
+        net.forward(pts)
+    net.fit(pts, tgt, steps=3, batch=16384, log_every=0)
+    torch.cuda.synchronize()
+    net.close()
+
+
 def main():
     args = parse()
-    if args.ncu:
+    if args.ncu and args.workload == "warm-start":
+        run_ncu_warm(args)
+    elif args.ncu:
         run_ncu(args)
     elif args.workload == "batched-cavity2d" and args.impl == "ours":
         run_batched(args)
