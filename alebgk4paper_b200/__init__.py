@@ -17,7 +17,8 @@ import numpy as np
 
 from . import _abi
 
-__all__ = ["Case", "Solver", "AlebgkError", "load_library", "read_checkpoint", "CASE_NAMES"]
+__all__ = ["Case", "LatticeCase", "Solver", "AlebgkError", "load_library", "read_checkpoint",
+           "CASE_NAMES"]
 
 CASE_NAMES = ("cavity2d", "cavity3d", "cavity2d-square", "cavity2d-circle",
               "cavity3d-sphere", "cavity3d-cube")
@@ -161,6 +162,61 @@ class Case:
                           _ip(nbr), _dp(g), _dp(mac))
 
 
+class LatticeCase:
+    """A box cavity without bodies whose set-up runs on the device.
+
+    It carries the case parameters only (``alebgk_lattice_info``); the lattice,
+    wall state, neighbour lists and rest state are built on the GPU when a
+    :class:`Solver` takes it (``alebgk_upload_lattice``), bitwise equal to
+    what :class:`Case` builds on the host.  Same arguments as :class:`Case`.
+    """
+
+    def __init__(self, name: str, Nx: int = -1, Nv: int = -1, dt: float = -1.0,
+                 mls_order: int = 2, lid_speed: float = -1.0, rho0: float = -1.0,
+                 tau: float = -1.0):
+        lib = _abi.load()
+        self._args = (name.encode(), int(Nx), int(Nv), float(dt), int(mls_order),
+                      float(lid_speed), float(rho0), float(tau))
+        info = np.zeros(8, np.int32)
+        prm = np.zeros(24)
+        _check(lib.alebgk_lattice_info(*self._args, _ip(info), _dp(prm)))
+        self.name = name
+        self.N, self.dim, self.Nv, self.gstride = int(info[0]), int(info[1]), int(info[2]), \
+            int(info[3])
+        self.nbodies, self.mls_order, self.Nx = 0, int(info[5]), int(info[6])
+        self.moving_bodies = False
+        keys = ("dt", "tau", "R", "dx", "dy", "dz", "radius", "minDist", "dv",
+                "vmin", "vmax", "rho0", "Tw", "xleft", "xright", "ybottom", "ytop",
+                "zfront", "zback", "dt_requested", "tfinal", "dHS", "lid_speed",
+                "save_every")
+        self.params = {k: float(v) for k, v in zip(keys, prm)}
+        self.dt = self.params["dt"]
+        self.bodies = np.zeros((0, 32))
+        self._xyz = None
+
+    config = Case.config
+
+    @property
+    def xyz(self) -> np.ndarray:
+        """Particle positions (N, 3), from the device set-up."""
+        if self._xyz is None:
+            self._xyz = self.build_on_device()["xyz"]
+        return self._xyz
+
+    def build_on_device(self, device: int = 0) -> dict:
+        """The device-built arrays: xyz, wall, boundary, nnb, nbr."""
+        lib = _abi.load()
+        N = self.N
+        out = dict(xyz=np.zeros((N, 3)), wall=np.zeros((N, 7)),
+                   boundary=np.zeros(N, np.int32), nnb=np.zeros(N, np.int32),
+                   nbr=np.zeros((N, _abi.MAX_NEIGH), np.int32))
+        _check(lib.alebgk_lattice_build_device(*self._args, int(device), _dp(out["xyz"]),
+                                               _dp(out["wall"]), _ip(out["boundary"]),
+                                               _ip(out["nnb"]), _ip(out["nbr"])))
+        self._xyz = out["xyz"]
+        return out
+
+
 class Solver:
     """One device-resident cloud advanced by the B200 step.
 
@@ -189,6 +245,9 @@ class Solver:
 
     # -- reference-named API ------------------------------------------------
     def cudaUploadCloud(self, case: Case):
+        if isinstance(case, LatticeCase):
+            _check(self.lib.alebgk_upload_lattice(self.ctx, *case._args), self.ctx)
+            return
         cl = case.cloud()
         _check(self.lib.alebgk_upload(self.ctx, ctypes.byref(cl), self.dt), self.ctx)
 

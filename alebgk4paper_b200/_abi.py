@@ -131,6 +131,19 @@ SIGNATURES = {
     "alebgk_case_bodies": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
     "alebgk_case_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                           ctypes.POINTER(Config)]),
+    "alebgk_lattice_info": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                           ctypes.c_double, ctypes.c_double, c_int_p,
+                                           c_double_p]),
+    "alebgk_lattice_build_device": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                                   ctypes.c_double, ctypes.c_int,
+                                                   ctypes.c_double, ctypes.c_double,
+                                                   ctypes.c_double, ctypes.c_int, c_double_p,
+                                                   c_double_p, c_int_p, c_int_p, c_int_p]),
+    "alebgk_upload_lattice": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                             ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_double]),
     "alebgk_moments13": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "alebgk_seed_grad13": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                           c_double_p, c_double_p]),

@@ -15,7 +15,7 @@ import math
 import numpy as np
 
 from . import _abi
-from . import Case, Solver, _check, _dp
+from . import Case, LatticeCase, Solver, _check, _dp
 
 __all__ = ["BatchSolver", "batched_cavity2d", "partition_lpt", "CAVITY2D_VMAX"]
 
@@ -73,11 +73,15 @@ class BatchSolver:
 
     ``specs`` are keyword dictionaries for :class:`Case` (as
     :func:`batched_cavity2d` returns).  With ``autotune`` every cavity's
-    launch shapes are tuned before the batch graph is captured.
+    launch shapes are tuned before the batch graph is captured.  With
+    ``setup="device"`` each cavity's lattice, neighbour lists and rest state
+    are built on the GPU (:class:`LatticeCase`) instead of on the host.
     """
 
     def __init__(self, specs, precision: int = 32, device: int = 0, autotune: bool = False,
-                 tune_steps: int = 3):
+                 tune_steps: int = 3, setup: str = "host"):
+        if setup not in ("host", "device"):
+            raise ValueError("setup must be 'host' or 'device'")
         self.lib = _abi.load()
         self.specs = list(specs)
         self.cases = []
@@ -85,7 +89,7 @@ class BatchSolver:
         for sp in self.specs:
             kw = dict(sp)
             name = kw.pop("name")
-            c = Case(name, **kw)
+            c = LatticeCase(name, **kw) if setup == "device" else Case(name, **kw)
             self.cases.append(c)
             self.solvers.append(Solver(c, precision=precision, device=device))
         self.tuned_ms = None

@@ -154,11 +154,13 @@ int alebgk_last_error(const alebgk_ctx *c, char *buf, size_t len)
     return ALEBGK_OK;
 }
 
-int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
+// The geometry part of alebgk_upload (tables, march plan, buffers); with
+// withState also the state (g and macros) from the cloud.
+static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool withState)
 {
     if (!c || !cl) return fail(c, ALEBGK_EINVAL, "null argument");
     if (!cl->xyz || !cl->meshv || !cl->wall || !cl->boundary || !cl->body_id ||
-        !cl->nnb || !cl->nbr || !cl->g || !cl->macro)
+        !cl->nnb || !cl->nbr || (withState && (!cl->g || !cl->macro)))
         return fail(c, ALEBGK_EINVAL, "alebgk_upload needs every cloud member");
     if (!(dt > 0)) return fail(c, ALEBGK_EINVAL, "dt must be > 0");
     CK(cudaSetDevice(c->cfg.device));
@@ -322,7 +324,12 @@ int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
     c->boundaryHost.assign(cl->boundary, cl->boundary + N);
     c->cur = 0;
     c->uploaded = true;
-    return alebgk_upload_state(c, cl->g, cl->macro);
+    return withState ? alebgk_upload_state(c, cl->g, cl->macro) : ALEBGK_OK;
+}
+
+int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
+{
+    return uploadCloud(c, cl, dt, true);
 }
 
 int alebgk_upload_state(alebgk_ctx *c, const double *g, const double *macro)
@@ -838,15 +845,13 @@ int alebgk_case_build_ex(const char *name, int Nx, int Nv, double dt, int mls_or
 
 void alebgk_case_free(alebgk_case *c) { delete c; }
 
-int alebgk_case_info(const alebgk_case *cs, int *info, double *prm)
+static void caseInfo(const CaseParams &p, int N, int gStride, int nbodies, int *info,
+                     double *prm)
 {
-    if (!cs) return ALEBGK_EINVAL;
-    const Cloud &c = cs->cloud;
-    const CaseParams &p = c.prm;
     if (info)
     {
-        info[0] = c.N; info[1] = p.dim; info[2] = p.Nv; info[3] = c.gStride;
-        info[4] = (int)c.bodies.size(); info[5] = p.mlsOrder; info[6] = p.Nx;
+        info[0] = N; info[1] = p.dim; info[2] = p.Nv; info[3] = gStride;
+        info[4] = nbodies; info[5] = p.mlsOrder; info[6] = p.Nx;
         info[7] = p.movingBodies ? 1 : 0;
     }
     if (prm)
@@ -857,6 +862,178 @@ int alebgk_case_info(const alebgk_case *cs, int *info, double *prm)
                         p.tfinal, p.dHS, p.lidSpeed, (double)p.saveEvery};
         std::memcpy(prm, v, sizeof v);
     }
+}
+
+int alebgk_case_info(const alebgk_case *cs, int *info, double *prm)
+{
+    if (!cs) return ALEBGK_EINVAL;
+    const Cloud &c = cs->cloud;
+    caseInfo(c.prm, c.N, c.gStride, (int)c.bodies.size(), info, prm);
+    return ALEBGK_OK;
+}
+
+// ---- lattice set-up on the device -------------------------------------------
+// The case parameters of a box cavity without bodies, as buildCloud sets
+// them, without building the cloud.
+static int latticeCase(const char *name, int Nx, int Nv, double dt, int mls_order,
+                       double lid_speed, double rho0, double tau, CaseParams &prm)
+{
+    if (!name) return fail(nullptr, ALEBGK_EINVAL, "null argument");
+    int id = 0;
+    if (!caseByName(name, &id))
+        return fail(nullptr, ALEBGK_EINVAL, std::string("unknown case ") + name);
+    if (!configureCase(id, Nx, Nv, dt, mls_order, false, prm))
+        return fail(nullptr, ALEBGK_EINVAL, "configureCase failed");
+    if (prm.hasBody)
+        return fail(nullptr, ALEBGK_EINVAL,
+                    std::string("case ") + name +
+                        " has rigid bodies; its set-up is host-only (alebgk_case_build_ex)");
+    if (prm.Nx < 3 || prm.Nv < 2)
+        return fail(nullptr, ALEBGK_EINVAL, "Nx must be >= 3 and Nv >= 2");
+    if (lid_speed > 0) prm.lidSpeed = lid_speed;
+    if (rho0 > 0) prm.rho0 = rho0;
+    if (tau > 0) prm.tau = tau;
+    latticeParams(prm);
+    clampDt(prm);
+    return ALEBGK_OK;
+}
+
+static size_t latticeN(const CaseParams &p)
+{
+    return (size_t)p.Nx * p.Ny * (p.dim == 3 ? p.Nz : 1);
+}
+
+namespace {
+
+struct LatticeBuffers
+{
+    LatticeDev d;
+    ~LatticeBuffers()
+    {
+        for (void *q : {(void *)d.xyz, (void *)d.wall, (void *)d.meshv, (void *)d.boundary,
+                        (void *)d.bodyId, (void *)d.voxel, (void *)d.voxCount, (void *)d.voxStart,
+                        (void *)d.voxCursor, (void *)d.voxList, (void *)d.nnb, (void *)d.nbr})
+            if (q) cudaFree(q);
+    }
+    cudaError_t alloc(const CaseParams &p)
+    {
+        const size_t N = latticeN(p);
+        const size_t nvox = (size_t)p.nbhBox * p.nbvBox * p.nbwBox;
+        cudaError_t e = dalloc(&d.xyz, 3 * N);
+        if (e == cudaSuccess) e = dalloc(&d.wall, 7 * N);
+        if (e == cudaSuccess) e = dalloc(&d.meshv, 3 * N);
+        if (e == cudaSuccess) e = dalloc(&d.boundary, N);
+        if (e == cudaSuccess) e = dalloc(&d.bodyId, N);
+        if (e == cudaSuccess) e = dalloc(&d.voxel, N);
+        if (e == cudaSuccess) e = dalloc(&d.voxCount, nvox);
+        if (e == cudaSuccess) e = dalloc(&d.voxStart, nvox + 1);
+        if (e == cudaSuccess) e = dalloc(&d.voxCursor, nvox);
+        if (e == cudaSuccess) e = dalloc(&d.voxList, N);
+        if (e == cudaSuccess) e = dalloc(&d.nnb, N);
+        if (e == cudaSuccess) e = dalloc(&d.nbr, N * ALEBGK_MAX_NEIGH);
+        return e;
+    }
+};
+
+// Host copies of the device-built geometry, laid out as an alebgk_cloud.
+struct LatticeHost
+{
+    std::vector<double> xyz, wall, meshv;
+    std::vector<int> boundary, bodyId, nnb, nbr;
+    cudaError_t fetch(const LatticeDev &d, size_t N)
+    {
+        xyz.resize(3 * N); wall.resize(7 * N); meshv.resize(3 * N);
+        boundary.resize(N); bodyId.resize(N); nnb.resize(N);
+        nbr.resize(N * ALEBGK_MAX_NEIGH);
+        cudaError_t e = cudaMemcpy(xyz.data(), d.xyz, 24 * N, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(wall.data(), d.wall, 56 * N, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(meshv.data(), d.meshv, 24 * N, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(boundary.data(), d.boundary, 4 * N, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(bodyId.data(), d.bodyId, 4 * N, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(nnb.data(), d.nnb, 4 * N, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(nbr.data(), d.nbr, 4 * N * ALEBGK_MAX_NEIGH, cudaMemcpyDeviceToHost);
+        return e;
+    }
+};
+
+}  // namespace
+
+int alebgk_lattice_info(const char *name, int Nx, int Nv, double dt, int mls_order,
+                        double lid_speed, double rho0, double tau, int *info, double *prm)
+{
+    CaseParams p;
+    int rc = latticeCase(name, Nx, Nv, dt, mls_order, lid_speed, rho0, tau, p);
+    if (rc) return rc;
+    const int gs = (p.dim == 3) ? p.Nv * p.Nv * p.Nv : 2 * p.Nv * p.Nv;
+    caseInfo(p, (int)latticeN(p), gs, 0, info, prm);
+    return ALEBGK_OK;
+}
+
+int alebgk_lattice_build_device(const char *name, int Nx, int Nv, double dt, int mls_order,
+                                double lid_speed, double rho0, double tau, int device,
+                                double *xyz, double *wall, int *boundary, int *nnb, int *nbr)
+{
+    alebgk_ctx *c = nullptr;
+    CaseParams p;
+    int rc = latticeCase(name, Nx, Nv, dt, mls_order, lid_speed, rho0, tau, p);
+    if (rc) return rc;
+    CK(cudaSetDevice(device));
+    LatticeBuffers b;
+    CK(b.alloc(p));
+    CK(buildLatticeDevice(p, b.d, nullptr));
+    CK(cudaDeviceSynchronize());
+    const size_t N = latticeN(p);
+    LatticeHost h;
+    CK(h.fetch(b.d, N));
+    if (xyz) std::memcpy(xyz, h.xyz.data(), 24 * N);
+    if (wall) std::memcpy(wall, h.wall.data(), 56 * N);
+    if (boundary) std::memcpy(boundary, h.boundary.data(), 4 * N);
+    if (nnb) std::memcpy(nnb, h.nnb.data(), 4 * N);
+    if (nbr) std::memcpy(nbr, h.nbr.data(), 4 * N * ALEBGK_MAX_NEIGH);
+    return ALEBGK_OK;
+}
+
+int alebgk_upload_lattice(alebgk_ctx *c, const char *name, int Nx, int Nv, double dt,
+                          int mls_order, double lid_speed, double rho0, double tau)
+{
+    if (!c) return ALEBGK_EINVAL;
+    CaseParams p;
+    int rc = latticeCase(name, Nx, Nv, dt, mls_order, lid_speed, rho0, tau, p);
+    if (rc) return fail(c, rc, gCreateError);
+    const StepParams &sp = c->sp;
+    const size_t N = latticeN(p);
+    if ((size_t)sp.N != N || sp.dim != p.dim || sp.Nv != p.Nv || sp.mlsOrder != p.mlsOrder ||
+        sp.vmin != p.VMin || sp.dv != p.dv || sp.h != p.radius || sp.tau != p.tau ||
+        sp.R != p.R)
+        return fail(c, ALEBGK_EINVAL,
+                    "the context's configuration does not match this lattice case "
+                    "(N, dim, Nv, MLS order, velocity grid, radius, tau or R)");
+    CK(cudaSetDevice(c->cfg.device));
+    LatticeBuffers b;
+    CK(b.alloc(p));
+    CK(buildLatticeDevice(p, b.d, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    LatticeHost h;
+    CK(h.fetch(b.d, N));
+    alebgk_cloud view{};
+    view.xyz = h.xyz.data(); view.meshv = h.meshv.data(); view.wall = h.wall.data();
+    view.boundary = h.boundary.data(); view.body_id = h.bodyId.data();
+    view.nnb = h.nnb.data(); view.nbr = h.nbr.data();
+    rc = uploadCloud(c, &view, p.dt, false);
+    if (rc) return rc;
+    std::vector<double> row;
+    restRow(p, row);
+    double *rowDev = nullptr;
+    CK(cudaMalloc(&rowDev, row.size() * 8));
+    cudaError_t e = cudaMemcpy(rowDev, row.data(), row.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launchRestState(c, rowDev, p.rho0, 270.0);
+    if (e == cudaSuccess) e = launchMassInit(c);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(rowDev);
+    if (e != cudaSuccess)
+        return fail(c, ALEBGK_ECUDA, std::string("lattice state: ") + cudaGetErrorString(e));
     return ALEBGK_OK;
 }
 

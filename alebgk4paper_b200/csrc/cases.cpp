@@ -350,10 +350,10 @@ bool configureCase(int caseId, int Nx, int Nv, double dt, int mlsOrder,
     return true;
 }
 
-// Initialization/ParticleGeneration.cpp:30-200 (non-periodic, Fixed grid)
-static void generateLattice(Cloud &c)
+// Initialization/ParticleGeneration.cpp:30-200 (non-periodic, Fixed grid):
+// lattice spacings, support radius and voxel boxes.
+void latticeParams(CaseParams &p)
 {
-    CaseParams &p = c.prm;
     int ndim = p.dim;
     int Nx = p.Nx, Ny = p.Ny, Nz = (ndim == 3) ? p.Nz : 1;
     double Lx = p.xright - p.xleft;
@@ -377,7 +377,15 @@ static void generateLattice(Cloud &c)
         p.nbwBox = static_cast<int>(std::ceil(Lz / p.wBox)) + 1;
     }
     else { p.wBox = 1.0; p.nbwBox = 1; }
+}
 
+// Initialization/ParticleGeneration.cpp:30-200 (non-periodic, Fixed grid)
+static void generateLattice(Cloud &c)
+{
+    CaseParams &p = c.prm;
+    latticeParams(p);
+    int ndim = p.dim;
+    int Nx = p.Nx, Ny = p.Ny, Nz = (ndim == 3) ? p.Nz : 1;
     for (int k = 0; k < Nz; k++)
     {
         double z = (ndim == 3) ? std::fma((double)k, p.dz, p.zfront) : 0.0;
@@ -609,17 +617,13 @@ static void wallState(Cloud &c)
     }
 }
 
-// Initialization/InitialConditions.cpp:18-80 -- uniform Maxwellian at rest.
-static void initialState(Cloud &c)
+// Initialization/InitialConditions.cpp:18-80 -- the row of the uniform
+// Maxwellian at rest that every particle starts from.
+void restRow(const CaseParams &p, std::vector<double> &row)
 {
-    const CaseParams &p = c.prm;
     int Nv = p.Nv, Nv2 = Nv * Nv;
-    c.gStride = (p.dim == 3) ? Nv * Nv * Nv : 2 * Nv2;
-    c.g.assign((size_t)c.N * c.gStride, 0.0);
-    c.macro.assign((size_t)c.N * 7, 0.0);
-    c.meshv.assign((size_t)c.N * 3, 0.0);
+    row.assign((p.dim == 3) ? Nv * Nv * Nv : 2 * Nv2, 0.0);
     const double rho = p.rho0, T = 270.0, R = p.R;
-    std::vector<double> row(c.gStride);
     if (p.dim == 3)
     {
         for (int kv = 0; kv < Nv; ++kv)
@@ -641,6 +645,19 @@ static void initialState(Cloud &c)
                 row[iv + Nv * jv + Nv2] = 0.5 * R * T * m;
             }
     }
+}
+
+static void initialState(Cloud &c)
+{
+    const CaseParams &p = c.prm;
+    int Nv = p.Nv, Nv2 = Nv * Nv;
+    c.gStride = (p.dim == 3) ? Nv * Nv * Nv : 2 * Nv2;
+    c.g.assign((size_t)c.N * c.gStride, 0.0);
+    c.macro.assign((size_t)c.N * 7, 0.0);
+    c.meshv.assign((size_t)c.N * 3, 0.0);
+    const double rho = p.rho0, T = 270.0, R = p.R;
+    std::vector<double> row;
+    restRow(p, row);
     for (int i = 0; i < c.N; ++i)
     {
         std::copy(row.begin(), row.end(), c.g.begin() + (size_t)i * c.gStride);
@@ -666,14 +683,18 @@ bool buildCloud(const CaseParams &prmIn, double bodyScale, Cloud &c,
     rebuildNeighbours(c);
     wallState(c);
     initialState(c);
-    // Foot-point clamp, Solver/Solver.cpp:167-205.
-    CaseParams &p = c.prm;
+    clampDt(c.prm);
+    return true;
+}
+
+// Foot-point clamp, Solver/Solver.cpp:167-205.
+void clampDt(CaseParams &p)
+{
     double vmax = std::max(std::fabs(p.VMax), std::fabs(p.VMin));
     double dxmin = std::fabs(p.dx);
     if (std::fabs(p.dy) < dxmin) dxmin = std::fabs(p.dy);
     if (p.dim == 3 && std::fabs(p.dz) < dxmin) dxmin = std::fabs(p.dz);
     if (vmax * p.dt / dxmin > 1.5) p.dt = 0.75 * dxmin / vmax;
-    return true;
 }
 
 }  // namespace alebgk

@@ -93,6 +93,17 @@ bool configureCase(int caseId, int Nx, int Nv, double dt, int mlsOrder,
 bool buildCloud(const CaseParams &prmIn, double bodyScale, Cloud &c,
                 std::string *err);
 
+// Lattice spacings, support radius and voxel boxes of a configured case
+// (the scalar part of Initialization/ParticleGeneration.cpp:30-200).
+void latticeParams(CaseParams &p);
+
+// The rest-state Maxwellian row every particle starts from
+// (Initialization/InitialConditions.cpp:18-80).
+void restRow(const CaseParams &p, std::vector<double> &row);
+
+// Foot-point clamp of dt (Solver/Solver.cpp:167-205).
+void clampDt(CaseParams &p);
+
 // Rebuilds voxel bins and neighbour lists from the positions
 // (Initialization/NeighbourSearch.cpp:17-99).
 void rebuildNeighbours(Cloud &c);

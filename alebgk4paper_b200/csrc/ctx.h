@@ -130,6 +130,17 @@ namespace alebgk {
 cudaError_t prepareKernels(alebgk_ctx *c);
 cudaError_t launchStep(alebgk_ctx *c, int from, cudaEvent_t *ev = nullptr);
 cudaError_t launchMassInit(alebgk_ctx *c);
+struct CaseParams;
+// Device arrays of the lattice set-up (setup.cu).
+struct LatticeDev
+{
+    double *xyz = nullptr, *wall = nullptr, *meshv = nullptr;
+    int *boundary = nullptr, *bodyId = nullptr, *voxel = nullptr, *voxCount = nullptr;
+    int *voxStart = nullptr, *voxCursor = nullptr, *voxList = nullptr;
+    int *nnb = nullptr, *nbr = nullptr;
+};
+cudaError_t buildLatticeDevice(const CaseParams &p, const LatticeDev &o, cudaStream_t st);
+cudaError_t launchRestState(alebgk_ctx *c, const double *rowDev, double rho, double T0);
 cudaError_t launchSeedGrad13(alebgk_ctx *c, const float *net, int ldnet, const double *scale,
                              const double *shift);
 cudaError_t launchMoments13(alebgk_ctx *c, double *out);

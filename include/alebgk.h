@@ -438,6 +438,31 @@ int alebgk_case_bodies(const alebgk_case *c, double *out);
 /* Shape of every body of the case: kind (alebgk_body), rotates, size. */
 int alebgk_case_body_shapes(const alebgk_case *c, int *kind, int *rotates, double *size);
 
+/* ---- lattice set-up on the device -------------------------------------------
+ * Box cavities without bodies (cavity2d, cavity3d and their overrides) can be
+ * set up on the GPU instead of by alebgk_case_build_ex on the host: the
+ * lattice (Initialization/ParticleGeneration.cpp:30-200), the wall state
+ * (Core/MLSBasis.hpp:228-287, TestCases/TestCases.cpp:230-249), the voxel
+ * bins and neighbour lists (Initialization/NeighbourSearch.cpp:17-99) and the
+ * rest-state Maxwellian (Initialization/InitialConditions.cpp:18-80), each
+ * bitwise equal to the host set-up.  The stencil classes and transport
+ * coefficients are still built on the host from the device's neighbour lists.
+ *
+ * alebgk_lattice_info: info/prm as alebgk_case_info, without building a cloud
+ * (cases with bodies are rejected). */
+int alebgk_lattice_info(const char *name, int Nx, int Nv, double dt, int mls_order,
+                        double lid_speed, double rho0, double tau, int *info, double *prm);
+/* The device-built arrays, copied to host buffers (any may be NULL): xyz N*3,
+ * wall N*7, boundary N, nnb N, nbr N*ALEBGK_MAX_NEIGH (-1 padded). */
+int alebgk_lattice_build_device(const char *name, int Nx, int Nv, double dt, int mls_order,
+                                double lid_speed, double rho0, double tau, int device,
+                                double *xyz, double *wall, int *boundary, int *nnb, int *nbr);
+/* alebgk_upload for a lattice case set up on the device: the context (made
+ * from the alebgk_lattice_info configuration) gets the same state that
+ * alebgk_upload of the host-built case gives it. */
+int alebgk_upload_lattice(alebgk_ctx *ctx, const char *name, int Nx, int Nv, double dt,
+                          int mls_order, double lid_speed, double rho0, double tau);
+
 /* Fills a solver configuration from a case (precision 32 or 64). */
 int alebgk_case_config(const alebgk_case *c, int precision, int device,
                        alebgk_config *cfg);

@@ -79,3 +79,15 @@ def test_setup_matches_compiled_reference(case, Nx, Nv):
     np.testing.assert_array_equal(c.nnb, cl["nnb"])
     np.testing.assert_array_equal(c.nbr, cl["nbr"])
     np.testing.assert_allclose(c.g, r.g(), rtol=1e-14, atol=0)
+
+
+def test_lattice_case_matches_host_parameters_and_rejects_bodies():
+    """The device set-up's case parameters are the host set-up's; cases with
+    rigid bodies keep the host set-up."""
+    from alebgk4paper_b200 import AlebgkError, Case, LatticeCase
+    for name, kw in (("cavity2d", dict(Nx=24, Nv=16, lid_speed=3.0, rho0=2.0, tau=1.8e-10)),
+                     ("cavity3d", dict(Nx=13, Nv=8))):
+        lc, c = LatticeCase(name, **kw), Case(name, **kw)
+        assert lc.params == c.params and lc.N == c.N and lc.gstride == c.gstride
+    with pytest.raises(AlebgkError, match="rigid bodies"):
+        LatticeCase("cavity2d-square", Nx=12, Nv=8)

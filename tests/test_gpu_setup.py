@@ -1,0 +1,70 @@
+"""Lattice set-up on the device (``alebgk_upload_lattice``): every array the
+GPU builds equals the host set-up bitwise, and a solver set up on the device
+steps to exactly the state of one set up on the host."""
+import numpy as np
+import pytest
+
+from alebgk4paper_b200 import Case, LatticeCase, Solver
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    ("cavity2d", dict(Nx=12, Nv=8)),
+    ("cavity2d", dict(Nx=24, Nv=16, lid_speed=3.0, rho0=2.0, tau=1.8e-10, dt=3.0e-11)),
+    ("cavity2d", dict(Nx=48, Nv=20, lid_speed=7.5, rho0=0.6, tau=6e-10, dt=2.0e-11)),
+    ("cavity3d", dict(Nx=9, Nv=6)),
+    ("cavity3d", dict(Nx=13, Nv=8, lid_speed=2.0)),
+    ("cavity3d", dict(Nx=40, Nv=10)),
+]
+
+
+def _need_gpu():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+@pytest.mark.parametrize("name,kw", CASES)
+def test_device_lattice_equals_host_setup(name, kw):
+    _need_gpu()
+    host = Case(name, **kw)
+    dev = LatticeCase(name, **kw).build_on_device()
+    assert np.array_equal(dev["xyz"], host.xyz)
+    assert np.array_equal(dev["wall"], host.wall)
+    assert np.array_equal(dev["boundary"], host.boundary)
+    assert np.array_equal(dev["nnb"], host.nnb)
+    assert np.array_equal(dev["nbr"], host.nbr)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+@pytest.mark.parametrize("name,kw", [CASES[1], CASES[4]])
+def test_device_setup_steps_like_host_setup(name, kw, precision):
+    _need_gpu()
+    a = Solver(Case(name, **kw), precision=precision)
+    b = Solver(LatticeCase(name, **kw), precision=precision)
+    ga, ma = a.cudaDownloadFull()
+    gb, mb = b.cudaDownloadFull()
+    assert np.array_equal(ga, gb) and np.array_equal(ma, mb)
+    a.cudaStep(5)
+    b.cudaStep(5)
+    ga, ma = a.cudaDownloadFull()
+    gb, mb = b.cudaDownloadFull()
+    assert np.array_equal(ga, gb) and np.array_equal(ma, mb)
+    assert a.counters() == b.counters()
+    a.cudaFreeCloud()
+    b.cudaFreeCloud()
+
+
+def test_batch_with_device_setup_matches_host_setup():
+    _need_gpu()
+    from alebgk4paper_b200.batch import BatchSolver, batched_cavity2d
+    specs = batched_cavity2d(6, seed=5)
+    a = BatchSolver(specs, setup="host")
+    b = BatchSolver(specs, setup="device")
+    a.step(10)
+    b.step(10)
+    for sa, sb in zip(a.solvers, b.solvers):
+        assert np.array_equal(sa.cudaDownloadFull()[0], sb.cudaDownloadFull()[0])
+    assert np.array_equal(a.residuals(), b.residuals())
+    a.close()
+    b.close()
