@@ -144,6 +144,12 @@ SIGNATURES = {
                                              ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                              ctypes.c_double, ctypes.c_double,
                                              ctypes.c_double]),
+    "alebgk_slab_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                          c_int_p, c_int_p, ctypes.c_int, c_int_p,
+                                          ctypes.POINTER(ctypes.c_void_p)]),
+    "alebgk_slab_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "alebgk_slab_sync": (ctypes.c_int, [ctypes.c_void_p]),
+    "alebgk_slab_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "alebgk_moments13": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "alebgk_seed_grad13": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                           c_double_p, c_double_p]),

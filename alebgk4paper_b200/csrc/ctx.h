@@ -46,6 +46,7 @@ struct StepScalars
     int err;               // device error bits
     unsigned redCount;     // ticket of the grid sums (zero between kernels)
     long long steps;
+    double slabPart[3];    // slab group: this slab's owned-range partial sums
 };
 
 struct DeviceBuffers
@@ -76,6 +77,9 @@ struct DeviceBuffers
 struct StepParams
 {
     int N = 0, dim = 3, Nv = 0, V = 0, L = 1, gs = 0, ldf = 0, S = 0;
+    // Slab group: particles [ownLo, ownHi) are this slab's own, the rest are
+    // ghost copies of the neighbouring slabs' rows (ownHi <= ownLo: no slab).
+    int ownLo = 0, ownHi = 0;
     int limiter = 2, tauVar = 0, mlsOrder = 2;
     int periodic[3] = {0, 0, 0};
     double Lp[3] = {0, 0, 0};
@@ -130,6 +134,12 @@ namespace alebgk {
 cudaError_t prepareKernels(alebgk_ctx *c);
 cudaError_t launchStep(alebgk_ctx *c, int from, cudaEvent_t *ev = nullptr);
 cudaError_t launchMassInit(alebgk_ctx *c);
+// Slab groups (slab.cpp): one segment of the split step (0..3) on stream st,
+// the cross-slab combine of a segment's partial sums (phase 0..3, 4 = set-up
+// mass), and the owned-range mass of a freshly uploaded slab into slabPart[1].
+cudaError_t launchSlabSegment(alebgk_ctx *c, int from, int seg, cudaStream_t st);
+cudaError_t launchSlabCombine(StepScalars *const *scs, int n, int phase, cudaStream_t st);
+cudaError_t launchSlabInitSum(alebgk_ctx *c, cudaStream_t st);
 struct CaseParams;
 // Device arrays of the lattice set-up (setup.cu).
 struct LatticeDev

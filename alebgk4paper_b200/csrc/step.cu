@@ -1199,6 +1199,8 @@ __global__ void k_scale_mood(StepParams p, const int *__restrict__ boundary,
     mac[5] *= sigma;
     if (p.limiter != 2) return;
     if (boundary[i]) { mood[i] = 0; return; }
+    // a slab's ghost rows are copies: their moodCheck belongs to their owner
+    if (p.ownHi > p.ownLo && (i < p.ownLo || i >= p.ownHi)) { mood[i] = 0; return; }
     const int fail = (mac[0] < 1.0e-10) || (mac[4] < 1.0e-6) || (sigma * minG[i] < -1.0e-14);
     mood[i] = fail;
     if (fail) atomicOr(&sc->moodfail, 1);
@@ -1283,6 +1285,75 @@ k_mass_end(const double *__restrict__ massEnd, int N, double *partial, StepScala
     {
         sc->massEnd = sc->sigma * m;
         sc->massOld = sc->massEnd;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Slab groups.  The global sums of the step (Conservation.cpp:48-109, the
+// moodCheck flag of Conservation.cpp:16-38) become, per slab, a sum over the
+// owned range into slabPart[q], then one combine over all slabs in slab
+// order -- the rank-ordered Allgather of the reference's decomposed mode
+// (Conservation.cpp:76-84) -- that writes the global values back to every
+// slab's scalars.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kRedThreads)
+k_sum_range(const double *__restrict__ a, int n, double *partial, StepScalars *sc, int q,
+            int gate)
+{
+    if (gate && sc->moodfail == 0) return;
+    double m;
+    if (gridSumLast(a, n, partial, sc, &m)) sc->slabPart[q] = m;
+}
+
+__global__ void k_slab_combine(StepScalars *const *scs, int n, int phase)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    StepScalars *s0 = scs[0];
+    auto total = [&](int q) {
+        double m = 0.0;
+        for (int i = 0; i < n; ++i) m += scs[i]->slabPart[q];
+        return m;
+    };
+    if (phase == 0)            // k_sigma
+    {
+        const double m = total(0);
+        const double sigma = (m > 1.0e-30) ? s0->massOld / m : 1.0;
+        for (int i = 0; i < n; ++i) { scs[i]->massNew = m; scs[i]->sigma = sigma; }
+    }
+    else if (phase == 1)       // k_mass_sum
+    {
+        const double sigma = s0->sigma;
+        const double me = sigma * total(1);
+        for (int i = 0; i < n; ++i)
+        {
+            scs[i]->massEnd = me;
+            scs[i]->massOld = me;
+            scs[i]->scale = sigma;
+            scs[i]->steps += 1;
+        }
+    }
+    else if (phase == 2)       // moodCheck: any slab failed
+    {
+        int f = 0;
+        for (int i = 0; i < n; ++i) f |= scs[i]->moodfail;
+        for (int i = 0; i < n; ++i) scs[i]->moodfail = f;
+    }
+    else if (phase == 3)       // k_mass_end
+    {
+        if (s0->moodfail == 0) return;
+        const double me = s0->sigma * total(2);
+        for (int i = 0; i < n; ++i) { scs[i]->massEnd = me; scs[i]->massOld = me; }
+    }
+    else                       // set-up: k_mass_init over the whole domain
+    {
+        const double m = total(1);
+        for (int i = 0; i < n; ++i)
+        {
+            scs[i]->massOld = m;
+            scs[i]->massEnd = m;
+            scs[i]->scale = 1.0;
+            scs[i]->sigma = 1.0;
+        }
     }
 }
 
@@ -1677,6 +1748,107 @@ static cudaError_t massInitT(alebgk_ctx *c)
     k_mass_init<<<kRedBlocks, kRedThreads, 0, c->stream>>>(c->d.massEnd, p.N, c->d.redPartial,
                                                             c->d.sc);
     return cudaGetLastError();
+}
+
+// One segment of the step of a slab, on stream st: the launches of stepT up
+// to each global sum, with the sum restricted to the owned range.
+template <typename T>
+static cudaError_t slabSegT(alebgk_ctx *c, int from, int seg, cudaStream_t st)
+{
+    const StepParams &p = c->sp;
+    DeviceBuffers &d = c->d;
+    T *fa = static_cast<T *>(d.f[from]);
+    T *fb = static_cast<T *>(d.f[1 - from]);
+    double *macA = d.macro[from], *macB = d.macro[1 - from];
+    ParticleArgs<T> pa;
+    pa.g = fb; pa.fold = fa; pa.coefLin = static_cast<const T *>(d.coefLin);
+    pa.boundary = d.boundary; pa.cls = d.cls; pa.nslot = d.nslot; pa.slots = d.slots;
+    pa.wall = d.wall; pa.macPrev = macA; pa.macNew = macB;
+    pa.massPos = d.massPos; pa.massEnd = d.massEnd; pa.minG = d.minG; pa.dpx = d.dpx;
+    pa.flag = d.flag; pa.flagList = d.flagList; pa.degList = d.degList; pa.sc = d.sc;
+    pa.nad = d.nad;
+    const int pBlocks = (p.N + kNT / 32 - 1) / (kNT / 32);
+    const int listBlocks = min(p.N, 296);
+    const int lo = p.ownLo, n = p.ownHi - p.ownLo;
+    const size_t rowBytes = (size_t)p.L * p.V * sizeof(T);
+    if (seg == 0)
+    {
+        const bool nadOn = c->pStream && p.limiter == 2;
+        const int nadBlocks = min((p.N + kNT / 32 - 1) / (kNT / 32), 1184);
+        k_step_begin<<<nadOn ? nadBlocks : 1, kNT, 0, st>>>(
+            d.sc, 1, macA, d.boundary, d.nslot, d.slots, p.S, p.N, nadOn ? d.nad : nullptr);
+        if (sizeof(T) == 4 && c->march.enabled)
+        {
+            cudaError_t e = launchMarch(c, from, reinterpret_cast<float *>(fb), st);
+            if (e != cudaSuccess) return e;
+        }
+        else
+        {
+            const int tt = c->tune.transportThreads;
+            dim3 gt(p.N, (p.V + tt - 1) / tt);
+            k_transport<T><<<gt, tt, 0, st>>>(fa, fb, static_cast<const T *>(d.coef), d.cls,
+                                               d.nslot, d.slots, p.S, p.V, p.L, p.ldf, d.sc);
+        }
+        const int wmax = particleWarpsPerBlock(p, sizeof(T));
+        const int wpb = (c->tune.particleWarps > 0 && c->tune.particleWarps < wmax)
+                            ? c->tune.particleWarps : wmax;
+        const int ppBlocks = (p.N + wpb - 1) / wpb;
+        if (c->pStream)
+            k_particle_stream<T><<<c->pStreamBlocks, kNT, c->pStreamSmem, st>>>(
+                pa, p, c->pStreamWpb);
+        else if (p.L == 2) k_particle<T, 2><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
+        else k_particle<T, 1><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
+        if (p.L == 2) k_redo<T, 2><<<listBlocks, kNT, rowBytes, st>>>(pa, p);
+        else k_redo<T, 1><<<listBlocks, kNT, rowBytes, st>>>(pa, p);
+        k_sum_range<<<kRedBlocks, kRedThreads, 0, st>>>(d.massPos + lo, n, d.redPartial, d.sc,
+                                                        0, 0);
+    }
+    else if (seg == 1)
+    {
+        k_fixup<T><<<min(pBlocks, 296), kNT, 0, st>>>(pa, p);
+        k_sum_range<<<kRedBlocks, kRedThreads, 0, st>>>(d.massEnd + lo, n, d.redPartial, d.sc,
+                                                        1, 0);
+    }
+    else if (seg == 2)
+        k_scale_mood<<<(p.N + 255) / 256, 256, 0, st>>>(p, d.boundary, macB, d.minG, d.mood,
+                                                         d.sc);
+    else if (seg == 3 && p.limiter == 2)
+    {
+        k_recollide<T><<<min(pBlocks, 592), kNT, 0, st>>>(fb, p, d.boundary, macB, d.massEnd,
+                                                         d.sc);
+        k_sum_range<<<kRedBlocks, kRedThreads, 0, st>>>(d.massEnd + lo, n, d.redPartial, d.sc,
+                                                        2, 1);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launchSlabSegment(alebgk_ctx *c, int from, int seg, cudaStream_t st)
+{
+    return (c->cfg.precision == 64) ? slabSegT<double>(c, from, seg, st)
+                                    : slabSegT<float>(c, from, seg, st);
+}
+
+cudaError_t launchSlabCombine(StepScalars *const *scs, int n, int phase, cudaStream_t st)
+{
+    k_slab_combine<<<1, 32, 0, st>>>(scs, n, phase);
+    return cudaGetLastError();
+}
+
+template <typename T>
+static cudaError_t slabInitT(alebgk_ctx *c, cudaStream_t st)
+{
+    const StepParams &p = c->sp;
+    const int pBlocks = (p.N + kNT / 32 - 1) / (kNT / 32);
+    k_particle_mass<T><<<pBlocks, kNT, 0, st>>>(static_cast<const T *>(c->d.f[c->cur]), p,
+                                                c->d.massEnd);
+    k_sum_range<<<kRedBlocks, kRedThreads, 0, st>>>(c->d.massEnd + p.ownLo, p.ownHi - p.ownLo,
+                                                    c->d.redPartial, c->d.sc, 1, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launchSlabInitSum(alebgk_ctx *c, cudaStream_t st)
+{
+    return (c->cfg.precision == 64) ? slabInitT<double>(c, st) : slabInitT<float>(c, st);
 }
 
 cudaError_t launchMassInit(alebgk_ctx *c)

@@ -348,6 +348,24 @@ int alebgk_net_train_step(alebgk_net *net, const float *pts_dev, const float *tg
                           float beta1, float beta2, float eps, float *loss_host);
 int alebgk_net_sync(alebgk_net *net);
 
+/* ---- slab mode ---------------------------------------------------------------
+ * One cavity split into slabs along its outermost lattice axis, one context
+ * per slab (the reference's decomposed mode, Solver/MpiExchange.cpp:114-466,
+ * driven from one process).  Each context holds its slab's owned particles
+ * [own_lo[i], own_hi[i]) and ghost copies of the neighbouring slabs' rows.
+ * copies: ncopies rows of 5 ints (dst slab, dst first particle, src slab, src
+ * first particle, particle count): after every step, the ghost block is
+ * refreshed from its owner (f and macros).  The global mass sums and the
+ * moodCheck flag are combined over the slabs in slab order.  Contexts may
+ * sit on different devices (peer access is enabled); they must not be
+ * stepped on their own while in a group. */
+typedef struct alebgk_slab alebgk_slab;
+int alebgk_slab_create(int n, alebgk_ctx **ctxs, const int *own_lo, const int *own_hi,
+                       int ncopies, const int *copies, alebgk_slab **out);
+int alebgk_slab_step(alebgk_slab *g, int nsteps);
+int alebgk_slab_sync(alebgk_slab *g);
+int alebgk_slab_destroy(alebgk_slab *g);
+
 /* ---- restart files ------------------------------------------------------
  * The reference's checkpoint layout (Core/Checkpoint.hpp:37-236, magic
  * "ALEBGK01", version 1): header, one record per particle, N*gStride FP64
