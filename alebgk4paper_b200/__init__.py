@@ -340,18 +340,44 @@ class Solver:
                                          float(self.dt if dt is None else dt)), self.ctx)
         return np.array([[arr[b].state[k] for k in range(32)] for b in range(nb)])
 
+    def neighbour_grid(self):
+        """(grid, boxes) of the case's voxel binning (ParticleGeneration.cpp
+        box sizes 3 dx, 3 dy, 3 dz; NeighbourSearch.cpp:17-99)."""
+        import math
+        p = self.case.params
+        d3 = self.case.dim == 3
+        hx, hy = 3.0 * p["dx"], 3.0 * p["dy"]
+        hz = 3.0 * p["dz"] if d3 else 1.0
+        nx = int(math.ceil((p["xright"] - p["xleft"]) / hx)) + 1
+        ny = int(math.ceil((p["ytop"] - p["ybottom"]) / hy)) + 1
+        nz = int(math.ceil((p["zback"] - p["zfront"]) / hz)) + 1 if d3 else 1
+        grid = np.array([p["xleft"], p["ybottom"], p["zfront"], hx, hy, hz, p["radius"]])
+        return grid, np.array([nx, ny, nz], np.int32)
+
+    def rebuild_neighbours(self):
+        """Neighbour lists (nnb, nbr) of the device's current positions,
+        built on the device (updateVoxelsAndNeighbours,
+        NeighbourSearch.cpp:17-99)."""
+        grid, boxes = self.neighbour_grid()
+        nnb = np.zeros(self.N, np.int32)
+        nbr = np.zeros((self.N, _abi.MAX_NEIGH), np.int32)
+        _check(self.lib.alebgk_neighbours_device(self.ctx, _dp(grid), _ip(boxes), _ip(nnb),
+                                                 _ip(nbr)), self.ctx)
+        return nnb, nbr
+
     def refresh_geometry(self):
         """Uploads the cloud again after :meth:`body_step` moved the surface:
         positions, mesh velocities and wall state as the device holds them,
-        with the current distribution and macros, and the neighbour lists
-        kept.  The reference instead runs its cloud management here
-        (manageRemove, mergeCloseParticles, manageRefill and a neighbour
-        rebuild, Solver.cpp:373-401); this keeps the particle set, which is
-        what those routines leave while the body stays clear of the fluid
-        particles."""
+        with the current distribution and macros, and neighbour lists rebuilt
+        on the device from the moved positions (the rebuild of
+        Solver.cpp:385).  The reference also runs its cloud management here
+        (manageRemove, mergeCloseParticles, manageRefill, Solver.cpp:373-401);
+        this keeps the particle set, which is what those routines leave
+        while the body stays clear of the fluid particles."""
         c = self.case
         xyz, mv, wall = self.download_geometry()
         g, macro = self.cudaDownloadFull()
+        c.nnb, c.nbr = self.rebuild_neighbours()
         c.xyz, c.meshv, c.wall, c.g, c.macro = xyz, mv, wall, g, macro
         self.cudaUploadCloud(c)
 

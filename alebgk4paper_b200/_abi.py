@@ -150,6 +150,8 @@ SIGNATURES = {
     "alebgk_slab_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "alebgk_slab_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "alebgk_slab_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "alebgk_neighbours_device": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_int_p, c_int_p,
+                                                c_int_p]),
     "alebgk_moments13": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "alebgk_seed_grad13": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                           c_double_p, c_double_p]),

@@ -995,6 +995,39 @@ int alebgk_lattice_build_device(const char *name, int Nx, int Nv, double dt, int
     return ALEBGK_OK;
 }
 
+int alebgk_neighbours_device(alebgk_ctx *c, const double *grid, const int *boxes, int *nnb,
+                             int *nbr)
+{
+    if (!c || !grid || !boxes || !nnb || !nbr) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    NeighbourGrid g;
+    g.dim = c->sp.dim;
+    g.x0 = grid[0]; g.y0 = grid[1]; g.z0 = grid[2];
+    g.hx = grid[3]; g.hy = grid[4]; g.hz = grid[5]; g.radius = grid[6];
+    g.nx = boxes[0]; g.ny = boxes[1]; g.nz = boxes[2];
+    // box sizes carry the sign of the axis (the z lattice of the 3-D body
+    // cases runs from zfront = L down to zback = 0)
+    if (g.nx < 1 || g.ny < 1 || g.nz < 1 || (g.dim == 2 && g.nz != 1) || !(g.hx != 0) ||
+        !(g.hy != 0) || !(g.hz != 0) || !(g.radius > 0))
+        return fail(c, ALEBGK_EINVAL, "bad voxel grid");
+    CK(cudaSetDevice(c->cfg.device));
+    const size_t N = c->sp.N;
+    const size_t nvox = (size_t)g.nx * g.ny * g.nz;
+    LatticeBuffers b;
+    CK(dalloc(&b.d.voxel, N));
+    CK(dalloc(&b.d.voxCount, nvox));
+    CK(dalloc(&b.d.voxStart, nvox + 1));
+    CK(dalloc(&b.d.voxCursor, nvox));
+    CK(dalloc(&b.d.voxList, N));
+    CK(dalloc(&b.d.nnb, N));
+    CK(dalloc(&b.d.nbr, N * ALEBGK_MAX_NEIGH));
+    CK(buildNeighboursDevice(g, c->d.pos, (int)N, b.d, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaMemcpy(nnb, b.d.nnb, 4 * N, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(nbr, b.d.nbr, 4 * N * ALEBGK_MAX_NEIGH, cudaMemcpyDeviceToHost));
+    return ALEBGK_OK;
+}
+
 int alebgk_upload_lattice(alebgk_ctx *c, const char *name, int Nx, int Nv, double dt,
                           int mls_order, double lid_speed, double rho0, double tau)
 {

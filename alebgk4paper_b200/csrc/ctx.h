@@ -150,6 +150,15 @@ struct LatticeDev
     int *nnb = nullptr, *nbr = nullptr;
 };
 cudaError_t buildLatticeDevice(const CaseParams &p, const LatticeDev &o, cudaStream_t st);
+// Voxel grid of the neighbour search: origin, box sizes, box counts, radius.
+struct NeighbourGrid
+{
+    int dim = 3;
+    double x0 = 0, y0 = 0, z0 = 0, hx = 1, hy = 1, hz = 1, radius = 0;
+    int nx = 1, ny = 1, nz = 1;
+};
+cudaError_t buildNeighboursDevice(const NeighbourGrid &g, const double *xyz, int N,
+                                  const LatticeDev &o, cudaStream_t st);
 cudaError_t launchRestState(alebgk_ctx *c, const double *rowDev, double rho, double T0);
 cudaError_t launchSeedGrad13(alebgk_ctx *c, const float *net, int ldnet, const double *scale,
                              const double *shift);

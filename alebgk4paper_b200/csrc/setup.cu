@@ -120,6 +120,21 @@ __global__ void k_lattice(LatticeArgs a, double *__restrict__ xyz, int *__restri
     atomicAdd(voxCount + v, 1);
 }
 
+// Voxel bin of arbitrary positions (NeighbourSearch.cpp:24-37).
+__global__ void k_voxel_assign(LatticeArgs a, const double *__restrict__ xyz, int N,
+                               int *__restrict__ voxel, int *__restrict__ voxCount)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double x = xyz[3 * (size_t)i], y = xyz[3 * (size_t)i + 1], z = xyz[3 * (size_t)i + 2];
+    const int vi = max(0, min(a.nbh - 1, (int)floor((x - a.xleft) / a.hBox)));
+    const int vj = max(0, min(a.nbv - 1, (int)floor((y - a.ybottom) / a.vBox)));
+    const int vk = (a.dim == 3) ? max(0, min(a.nbw - 1, (int)floor((z - a.zfront) / a.wBox))) : 0;
+    const int v = vi + a.nbh * (vj + a.nbv * vk);
+    voxel[i] = v;
+    atomicAdd(voxCount + v, 1);
+}
+
 // Exclusive scan of the voxel counts (one thread: a few thousand voxels).
 __global__ void k_voxel_scan(const int *__restrict__ count, int nvox, int *start, int *cursor)
 {
@@ -254,6 +269,28 @@ cudaError_t buildLatticeDevice(const CaseParams &p, const LatticeDev &o, cudaStr
     k_voxel_sort<<<(nvox + 127) / 128, 128, 0, st>>>(o.voxStart, nvox, o.voxList);
     k_neighbours<<<(a.N + 127) / 128, 128, 0, st>>>(a, o.xyz, o.voxel, o.voxStart, o.voxList,
                                                     o.nnb, o.nbr);
+    return cudaGetLastError();
+}
+
+cudaError_t buildNeighboursDevice(const NeighbourGrid &gr, const double *xyz, int N,
+                                  const LatticeDev &o, cudaStream_t st)
+{
+    LatticeArgs a{};
+    a.dim = gr.dim; a.N = N;
+    a.xleft = gr.x0; a.ybottom = gr.y0; a.zfront = gr.z0;
+    a.hBox = gr.hx; a.vBox = gr.hy; a.wBox = gr.hz;
+    a.nbh = gr.nx; a.nbv = gr.ny; a.nbw = gr.nz;
+    a.r2max = gr.radius * gr.radius;
+    const int nvox = a.nbh * a.nbv * a.nbw;
+    const int nb = (N + 255) / 256;
+    cudaError_t e = cudaMemsetAsync(o.voxCount, 0, sizeof(int) * nvox, st);
+    if (e != cudaSuccess) return e;
+    k_voxel_assign<<<nb, 256, 0, st>>>(a, xyz, N, o.voxel, o.voxCount);
+    k_voxel_scan<<<1, 32, 0, st>>>(o.voxCount, nvox, o.voxStart, o.voxCursor);
+    k_voxel_fill<<<nb, 256, 0, st>>>(o.voxel, N, o.voxCursor, o.voxList);
+    k_voxel_sort<<<(nvox + 127) / 128, 128, 0, st>>>(o.voxStart, nvox, o.voxList);
+    k_neighbours<<<(N + 127) / 128, 128, 0, st>>>(a, xyz, o.voxel, o.voxStart, o.voxList,
+                                                  o.nnb, o.nbr);
     return cudaGetLastError();
 }
 

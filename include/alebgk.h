@@ -348,6 +348,14 @@ int alebgk_net_train_step(alebgk_net *net, const float *pts_dev, const float *tg
                           float beta1, float beta2, float eps, float *loss_host);
 int alebgk_net_sync(alebgk_net *net);
 
+/* Neighbour lists of the context's current device positions (body surface
+ * particles included), as Initialization/NeighbourSearch.cpp:17-99 builds
+ * them: grid = x0, y0, z0 (box origin), hBox, vBox, wBox (voxel sizes),
+ * radius; boxes = voxel counts per axis.  nnb (N) and nbr (N x
+ * ALEBGK_MAX_NEIGH, -1 padded) are host buffers. */
+int alebgk_neighbours_device(alebgk_ctx *ctx, const double *grid, const int *boxes, int *nnb,
+                             int *nbr);
+
 /* ---- slab mode ---------------------------------------------------------------
  * One cavity split into slabs along its outermost lattice axis, one context
  * per slab (the reference's decomposed mode, Solver/MpiExchange.cpp:114-466,

@@ -68,3 +68,20 @@ def test_batch_with_device_setup_matches_host_setup():
     assert np.array_equal(a.residuals(), b.residuals())
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("name,kw", [("cavity2d-square", dict(Nx=24, Nv=6)),
+                                     ("cavity2d-circle", dict(Nx=24, Nv=6)),
+                                     ("cavity3d-cube", dict(Nx=16, Nv=4)),
+                                     ("cavity3d-sphere", dict(Nx=16, Nv=4)),
+                                     ("cavity3d", dict(Nx=12, Nv=4))])
+def test_device_neighbour_rebuild_equals_host_search(name, kw):
+    """Neighbour lists of arbitrary clouds (body surface particles among the
+    lattice) built on the device equal the host search bitwise."""
+    _need_gpu()
+    case = Case(name, **kw)
+    s = Solver(case, precision=64)
+    nnb, nbr = s.rebuild_neighbours()
+    assert np.array_equal(nnb, case.nnb)
+    assert np.array_equal(nbr, case.nbr)
+    s.cudaFreeCloud()
