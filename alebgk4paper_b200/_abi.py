@@ -152,6 +152,12 @@ SIGNATURES = {
     "alebgk_slab_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "alebgk_neighbours_device": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_int_p, c_int_p,
                                                 c_int_p]),
+    "alebgk_manage_cloud": (ctypes.c_int, [ctypes.c_int, c_double_p, c_int_p, ctypes.c_int,
+                                           ctypes.POINTER(Body), ctypes.c_int, ctypes.c_int,
+                                           ctypes.POINTER(Cloud), ctypes.POINTER(ctypes.c_void_p)]),
+    "alebgk_managed_info": (ctypes.c_int, [ctypes.c_void_p, c_int_p]),
+    "alebgk_managed_cloud": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Cloud)]),
+    "alebgk_managed_free": (None, [ctypes.c_void_p]),
     "alebgk_moments13": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "alebgk_seed_grad13": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                           c_double_p, c_double_p]),

@@ -19,7 +19,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libalebgk_b200.so")
 
-SOURCES = ["step.cu", "march.cu", "body_noalloc.cu", "body_step.cu", "warm.cu", "setup.cu", "checkpoint.cpp", "batch.cpp", "slab.cpp", "api.cpp", "coeffs.cpp", "cases.cpp", "march_plan.cpp"]
+SOURCES = ["step.cu", "march.cu", "body_noalloc.cu", "body_step.cu", "warm.cu", "setup.cu", "cloud.cu", "checkpoint.cpp", "batch.cpp", "slab.cpp", "api.cpp", "coeffs.cpp", "cases.cpp", "march_plan.cpp"]
 HEADERS = ["ctx.h", "coeffs.h", "cases.h", "march.h", "mbar.cuh", "umma.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -47,6 +47,8 @@ const CaseRow kCases[6] = {
     {"cavity3d-cube", 3, true, 2, kParabolicPeak},
 };
 
+}  // namespace
+
 // Core/MLSBasis.hpp:112-122 (3-D Maxwellian, Theta = 2RT)
 double maxwellian3(double vx, double vy, double vz, double ux, double uy,
                    double uz, double T, double rho, double R)
@@ -68,7 +70,6 @@ double maxwellianG1(double vx, double vy, double ux, double uy, double T,
     return rho / (kPi * twoRT) * std::exp(e);
 }
 
-}  // namespace
 
 // ---------------------------------------------------------------------------
 // Bodies: RigidBody/Geometry.hpp:84-362

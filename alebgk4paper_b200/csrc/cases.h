@@ -101,6 +101,13 @@ void latticeParams(CaseParams &p);
 // (Initialization/InitialConditions.cpp:18-80).
 void restRow(const CaseParams &p, std::vector<double> &row);
 
+// The reference's Maxwellians (Core/MLSBasis.hpp:87-122), in the FMA form of
+// its compiled build.
+double maxwellian3(double vx, double vy, double vz, double ux, double uy, double uz,
+                   double T, double rho, double R);
+double maxwellianG1(double vx, double vy, double ux, double uy, double T, double rho,
+                    double R);
+
 // Foot-point clamp of dt (Solver/Solver.cpp:167-205).
 void clampDt(CaseParams &p);
 

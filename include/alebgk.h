@@ -356,6 +356,23 @@ int alebgk_net_sync(alebgk_net *net);
 int alebgk_neighbours_device(alebgk_ctx *ctx, const double *grid, const int *boxes, int *nnb,
                              int *nbr);
 
+/* Cloud management after a body motion (RigidBody/CloudManagement.cpp:17-275
+ * in the order of Solver.cpp:381-395): remove, neighbour rebuild, merge,
+ * refill, with the all-particle tests and the rebuilds on device `device`
+ * and the result bitwise equal to the reference's.  Input: the host cloud
+ * (N particles, gstride values per row; nnb/nbr unused), the bodies, and
+ * prm = dx, minDist, radius, xleft, xright, ybottom, ytop, zfront, zback,
+ * vmin, dv, R, hBox, vBox, wBox; iprm = dim, Nv, nbh, nbv, nbw.  The managed
+ * cloud (new N, neighbour lists rebuilt) lives in *out until
+ * alebgk_managed_free; alebgk_managed_info gives N, removed, merged, added. */
+typedef struct alebgk_managed alebgk_managed;
+int alebgk_manage_cloud(int device, const double *prm, const int *iprm, int nbodies,
+                        const alebgk_body *bodies, int N, int gstride,
+                        const alebgk_cloud *cloud, alebgk_managed **out);
+int alebgk_managed_info(const alebgk_managed *m, int *info);
+int alebgk_managed_cloud(alebgk_managed *m, alebgk_cloud *view);
+void alebgk_managed_free(alebgk_managed *m);
+
 /* ---- slab mode ---------------------------------------------------------------
  * One cavity split into slabs along its outermost lattice axis, one context
  * per slab (the reference's decomposed mode, Solver/MpiExchange.cpp:114-466,

@@ -345,6 +345,58 @@ void ref_get_bodies(void *h, double *out)
     }
 }
 
+// Test hook: shifts body b and its surface particles by (dx, dy, dz), as a
+// body motion larger than one step would, so that the cloud management below
+// has work to do.
+void ref_shift_body(void *h, int b, double dx, double dy, double dz)
+{
+    auto *c = static_cast<RefCase *>(h);
+    if (b < 0 || b >= (int)c->bodies.size()) return;
+    RigidBody &r = *c->bodies[b];
+    r.cx += dx; r.cy += dy; r.cz += dz;
+    for (Particle &p : c->P)
+        if (p.boundary && p.bodyId == b)
+        {
+            p.x += dx; p.y += dy;
+            if (c->cp.dim == 3) p.z += dz;
+        }
+}
+
+// Test hook: sets body b's velocity.
+void ref_set_body_velocity(void *h, int b, double vx, double vy, double vz)
+{
+    auto *c = static_cast<RefCase *>(h);
+    if (b < 0 || b >= (int)c->bodies.size()) return;
+    RigidBody &r = *c->bodies[b];
+    r.velx = vx; r.vely = vy; r.velz = vz;
+}
+
+// Test hook: moves particle i to (x, y, z).
+void ref_set_position(void *h, int i, double x, double y, double z)
+{
+    auto *c = static_cast<RefCase *>(h);
+    if (i < 0 || i >= (int)c->P.size()) return;
+    c->P[i].x = x; c->P[i].y = y; c->P[i].z = z;
+}
+
+// The cloud-management block of the moving-body step (Solver.cpp:381-395,
+// ref_step above): remove, rebuild, merge (+ rebuild), refill (+ rebuild).
+// counts = removed, merged, added.
+void ref_manage(void *h, int *counts)
+{
+    auto *c = static_cast<RefCase *>(h);
+    int removed = manageRemove(c->P, c->bodies, c->cp);
+    updateVoxelsAndNeighbours(c->P, c->cp, c->dom);
+    int mergedN = mergeCloseParticles(c->P, c->cp);
+    if (mergedN > 0) updateVoxelsAndNeighbours(c->P, c->cp, c->dom);
+    int added = manageRefill(c->P, c->bodies, c->sp, c->cp, c->dom, c->gc.R);
+    if (added > 0) updateVoxelsAndNeighbours(c->P, c->cp, c->dom);
+    c->cp.N = static_cast<int>(c->P.size());
+    counts[0] = removed;
+    counts[1] = mergedN;
+    counts[2] = added;
+}
+
 // The reference's own restart files (Core/Checkpoint.hpp): save the case's
 // state, restore into it, and the record sizes of the format.
 int ref_checkpoint_save(void *h, const char *path)
