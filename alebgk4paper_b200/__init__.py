@@ -367,39 +367,47 @@ class Solver:
 
     def refresh_geometry(self, bodies: np.ndarray | None = None, manage: bool = True):
         """Uploads the cloud again after :meth:`body_step` moved the surface:
-        positions, mesh velocities and wall state as the device holds them,
-        with the current distribution and macros.  With ``manage`` (and
-        bodies in the case) the reference's cloud management runs first --
-        remove, merge, refill and the neighbour rebuilds of Solver.cpp:381-395
-        (:func:`alebgk4paper_b200.cloud.manage_cloud`), for the bodies at
-        ``bodies`` (nbodies x 32, default the case's) -- and the context is
-        rebuilt when the particle count changes; otherwise only the
-        neighbour lists are rebuilt on the device.  Returns the cloud
+        positions, mesh velocities and wall state as the device holds them.
+        With ``manage`` (and bodies in the case) the reference's cloud
+        management runs first -- remove, merge, refill and the neighbour
+        rebuilds of Solver.cpp:381-395 (:func:`alebgk4paper_b200.cloud.
+        manage_cloud`), for the bodies at ``bodies`` (nbodies x 32, default
+        the case's); otherwise only the neighbour lists are rebuilt on the
+        device.  While the particle set stays the same (the usual step) the
+        distribution never leaves the device (``alebgk_upload_geometry``);
+        when it changes, the state is read back, managed and uploaded, and
+        the context is rebuilt for the new particle count.  Returns the cloud
         management counts (removed, merged, added)."""
+        from .cloud import manage_cloud
         c = self.case
         xyz, mv, wall = self.download_geometry()
-        g, macro = self.cudaDownloadFull()
+        c.xyz, c.meshv, c.wall = xyz, mv, wall
         counts = (0, 0, 0)
         if manage and getattr(c, "nbodies", 0):
-            from .cloud import manage_cloud
             st = c.bodies if bodies is None else bodies
-            out, counts = manage_cloud(c, dict(xyz=xyz, meshv=mv, wall=wall,
-                                               boundary=c.boundary, body_id=c.body_id, g=g,
-                                               macro=macro), st, self.cfg.device)
-            c.xyz, c.meshv, c.wall = out["xyz"], out["meshv"], out["wall"]
-            c.boundary, c.body_id = out["boundary"], out["body_id"]
-            c.nnb, c.nbr, c.g, c.macro = out["nnb"], out["nbr"], out["g"], out["macro"]
-            if len(c.xyz) != self.N:
-                c.N = self.N = len(c.xyz)
-                self.lib.alebgk_destroy(self.ctx)
-                self.cfg.N = self.N
-                h = ctypes.c_void_p()
-                _check(self.lib.alebgk_create(ctypes.byref(self.cfg), ctypes.byref(h)))
-                self.ctx = h
+            geo = dict(xyz=xyz, meshv=mv, wall=wall, boundary=c.boundary, body_id=c.body_id)
+            out, counts, need = manage_cloud(c, geo, st, self.cfg.device, decide_only=True)
+            if need:
+                g, macro = self.cudaDownloadFull()
+                geo.update(g=g, macro=macro)
+                out, counts, _ = manage_cloud(c, geo, st, self.cfg.device)
+                c.xyz, c.meshv, c.wall = out["xyz"], out["meshv"], out["wall"]
+                c.boundary, c.body_id = out["boundary"], out["body_id"]
+                c.nnb, c.nbr, c.g, c.macro = out["nnb"], out["nbr"], out["g"], out["macro"]
+                if len(c.xyz) != self.N:
+                    c.N = self.N = len(c.xyz)
+                    self.lib.alebgk_destroy(self.ctx)
+                    self.cfg.N = self.N
+                    h = ctypes.c_void_p()
+                    _check(self.lib.alebgk_create(ctypes.byref(self.cfg), ctypes.byref(h)))
+                    self.ctx = h
+                self.cudaUploadCloud(c)
+                return counts
+            c.nnb, c.nbr = out["nnb"], out["nbr"]
         else:
             c.nnb, c.nbr = self.rebuild_neighbours()
-            c.xyz, c.meshv, c.wall, c.g, c.macro = xyz, mv, wall, g, macro
-        self.cudaUploadCloud(c)
+        cl = c.cloud()
+        _check(self.lib.alebgk_upload_geometry(self.ctx, ctypes.byref(cl), self.dt), self.ctx)
         return counts
 
     def checkpoint_save(self, path: str, step: int = 0, t: float = 0.0,

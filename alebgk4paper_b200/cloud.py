@@ -29,11 +29,15 @@ def _params(case):
     return prm, iprm
 
 
-def manage_cloud(case, cloud: dict, bodies_state: np.ndarray, device: int = 0):
+def manage_cloud(case, cloud: dict, bodies_state: np.ndarray, device: int = 0,
+                 decide_only: bool = False):
     """Runs the cloud management on a host cloud (dict with xyz, meshv, wall,
     boundary, body_id, g, macro) whose bodies are at ``bodies_state``
     (nbodies x 32, the layout of ``Case.bodies``).  Returns (managed cloud
-    dict with nnb and nbr, (removed, merged, added))."""
+    dict with nnb and nbr, (removed, merged, added), need_state).  With
+    ``decide_only`` g and macro are not passed: the call stops with
+    need_state True as soon as the particle set would change, and otherwise
+    returns the unchanged cloud with rebuilt neighbour lists."""
     lib = _abi.load()
     prm, iprm = _params(case)
     st = np.ascontiguousarray(bodies_state, np.float64).reshape(-1, 32)
@@ -45,22 +49,28 @@ def manage_cloud(case, cloud: dict, bodies_state: np.ndarray, device: int = 0):
         arr[b].size = float(case.body_size[b])
         for k in range(32):
             arr[b].state[k] = float(st[b, k])
-    keep = {k: np.ascontiguousarray(cloud[k], dt) for k, dt in
-            (("xyz", np.float64), ("meshv", np.float64), ("wall", np.float64),
-             ("boundary", np.int32), ("body_id", np.int32), ("g", np.float64),
-             ("macro", np.float64))}
+    names = [("xyz", np.float64), ("meshv", np.float64), ("wall", np.float64),
+             ("boundary", np.int32), ("body_id", np.int32)]
+    if not decide_only:
+        names += [("g", np.float64), ("macro", np.float64)]
+    keep = {k: np.ascontiguousarray(cloud[k], dt) for k, dt in names}
     N = keep["xyz"].shape[0]
-    gs = keep["g"].shape[1]
+    gs = int(case.gstride)
     dummy = np.zeros(1, np.int32)
+    none = ctypes.POINTER(ctypes.c_double)()
     cl = _abi.Cloud(_dp(keep["xyz"]), _dp(keep["meshv"]), _dp(keep["wall"]),
                     _ip(keep["boundary"]), _ip(keep["body_id"]), _ip(dummy), _ip(dummy),
-                    _dp(keep["g"]), _dp(keep["macro"]))
+                    none if decide_only else _dp(keep["g"]),
+                    none if decide_only else _dp(keep["macro"]))
     h = ctypes.c_void_p()
     _check(lib.alebgk_manage_cloud(int(device), _dp(prm), _ip(iprm), nb, arr, N, gs,
                                    ctypes.byref(cl), ctypes.byref(h)))
     try:
-        info = np.zeros(4, np.int32)
+        info = np.zeros(5, np.int32)
         _check(lib.alebgk_managed_info(h, _ip(info)))
+        counts = (int(info[1]), int(info[2]), int(info[3]))
+        if info[4]:
+            return None, counts, True
         n = int(info[0])
         view = _abi.Cloud()
         _check(lib.alebgk_managed_cloud(h, ctypes.byref(view)))
@@ -75,8 +85,8 @@ def manage_cloud(case, cloud: dict, bodies_state: np.ndarray, device: int = 0):
                    body_id=take(view.body_id, n, np.int32, (n,)),
                    nnb=take(view.nnb, n, np.int32, (n,)),
                    nbr=take(view.nbr, n * _abi.MAX_NEIGH, np.int32, (n, _abi.MAX_NEIGH)),
-                   g=take(view.g, n * gs, np.float64, (n, gs)),
-                   macro=take(view.macro, 7 * n, np.float64, (n, 7)))
-        return out, (int(info[1]), int(info[2]), int(info[3]))
+                   g=None if decide_only else take(view.g, n * gs, np.float64, (n, gs)),
+                   macro=None if decide_only else take(view.macro, 7 * n, np.float64, (n, 7)))
+        return out, counts, False
     finally:
         lib.alebgk_managed_free(h)

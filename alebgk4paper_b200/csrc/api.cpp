@@ -332,6 +332,56 @@ int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
     return uploadCloud(c, cl, dt, true);
 }
 
+int alebgk_upload_geometry(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
+{
+    if (!c || !cl) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    const StepParams &p = c->sp;
+    const size_t es = (c->cfg.precision == 64) ? 8 : 4;
+    const size_t fBytes = (size_t)p.N * p.ldf * es;
+    const size_t N = p.N;
+    void *tf = nullptr;
+    double *tm = nullptr;
+    int *tmood = nullptr;
+    StepScalars sc{};
+    auto freeTemps = [&]() {
+        if (tf) cudaFree(tf);
+        if (tm) cudaFree(tm);
+        if (tmood) cudaFree(tmood);
+    };
+    cudaError_t e = cudaMalloc(&tf, fBytes);
+    if (e == cudaSuccess) e = cudaMalloc(&tm, 48 * N);
+    if (e == cudaSuccess) e = cudaMalloc(&tmood, 4 * N);
+    if (e == cudaSuccess) e = cudaMemcpy(tf, c->d.f[c->cur], fBytes, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(tm, c->d.macro[c->cur], 48 * N, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(tmood, c->d.mood, 4 * N, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(&sc, c->d.sc, sizeof sc, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+    {
+        freeTemps();
+        return fail(c, ALEBGK_ECUDA, std::string("geometry upload: ") + cudaGetErrorString(e));
+    }
+    const long long steps = c->hostSteps;
+    int rc = uploadCloud(c, cl, dt, false);
+    if (rc)
+    {
+        freeTemps();
+        return rc;
+    }
+    e = cudaMemcpy(c->d.f[0], tf, fBytes, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(c->d.macro[0], tm, 48 * N, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(c->d.mood, tmood, 4 * N, cudaMemcpyDeviceToDevice);
+    sc.redCount = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(c->d.sc, &sc, sizeof sc, cudaMemcpyHostToDevice);
+    freeTemps();
+    if (e != cudaSuccess)
+        return fail(c, ALEBGK_ECUDA, std::string("geometry upload: ") + cudaGetErrorString(e));
+    c->hostSteps = steps;
+    return ALEBGK_OK;
+}
+
 int alebgk_upload_state(alebgk_ctx *c, const double *g, const double *macro)
 {
     if (!c || !g || !macro) return fail(c, ALEBGK_EINVAL, "null argument");

@@ -182,6 +182,7 @@ struct ManagedCloud
 {
     Cloud2 c;
     int counts[3] = {0, 0, 0};
+    bool needState = false;   // geometry-only run: the particle set would change
 };
 
 // The whole cloud-management block.  Returns a CUDA error or cudaSuccess;
@@ -191,12 +192,20 @@ cudaError_t manageCloud(const ManageParams &mp, const std::vector<Body> &bodies,
                         std::string *bad)
 {
     Cloud2 &c = out.c;
-    c.N = N; c.gs = gs;
+    // Without g and macros the run only decides: it stops with needState as
+    // soon as the particle set would change.
+    const bool haveState = in.g && in.macro;
+    c.N = N; c.gs = haveState ? gs : 0;
     c.xyz.assign(in.xyz, in.xyz + 3 * (size_t)N);
     c.meshv.assign(in.meshv, in.meshv + 3 * (size_t)N);
     c.wall.assign(in.wall, in.wall + 7 * (size_t)N);
-    c.g.assign(in.g, in.g + (size_t)gs * N);
-    c.macro.assign(in.macro, in.macro + 7 * (size_t)N);
+    if (haveState)
+    {
+        c.g.assign(in.g, in.g + (size_t)gs * N);
+        c.macro.assign(in.macro, in.macro + 7 * (size_t)N);
+    }
+    else
+        c.macro.assign(7 * (size_t)N, 0.0);
     c.boundary.assign(in.boundary, in.boundary + N);
     c.bodyId.assign(in.body_id, in.body_id + N);
     const bool d3 = mp.dim == 3;
@@ -300,8 +309,13 @@ cudaError_t manageCloud(const ManageParams &mp, const std::vector<Body> &bodies,
                 }
             if (drop || hug[i]) { keep[i] = 0; ++removed; }
         }
-        c.keep(keep);
         out.counts[0] = removed;
+        if (removed && !haveState)
+        {
+            out.needState = true;
+            return cudaSuccess;
+        }
+        c.keep(keep);
     }
     e = rebuild();
     if (e != cudaSuccess) return e;
@@ -322,6 +336,11 @@ cudaError_t manageCloud(const ManageParams &mp, const std::vector<Body> &bodies,
         if (e == cudaSuccess) e = cudaMemcpy(&any, anyDev, 4, cudaMemcpyDeviceToHost);
         if (anyDev) cudaFree(anyDev);
         if (e != cudaSuccess) return e;
+        if (any && !haveState)
+        {
+            out.needState = true;
+            return cudaSuccess;
+        }
         if (any)
         {
             std::vector<char> dead(c.N, 0);
@@ -466,6 +485,11 @@ cudaError_t manageCloud(const ManageParams &mp, const std::vector<Body> &bodies,
                     T = std::fma(w, m[4], T);
                 }
                 if (wsum < 1e-30) continue;
+                if (!haveState)
+                {
+                    out.needState = true;
+                    return cudaSuccess;
+                }
                 rho /= wsum; ux /= wsum; uy /= wsum; uz /= wsum; T /= wsum;
                 const double p = rho * mp.R * T;
                 c.xyz.insert(c.xyz.end(), {xm, ym, zm});
@@ -544,7 +568,7 @@ int alebgk_manage_cloud(int device, const double *prm, const int *iprm, int nbod
         (nbodies > 0 && !bodies))
         return ALEBGK_EINVAL;
     if (!cloud->xyz || !cloud->meshv || !cloud->wall || !cloud->boundary || !cloud->body_id ||
-        !cloud->g || !cloud->macro)
+        (!cloud->g) != (!cloud->macro))
         return ALEBGK_EINVAL;
     *out = nullptr;
     ManageParams mp;
@@ -589,6 +613,7 @@ int alebgk_managed_info(const alebgk_managed *m, int *info)
     info[1] = m->m.counts[0];
     info[2] = m->m.counts[1];
     info[3] = m->m.counts[2];
+    info[4] = m->m.needState ? 1 : 0;
     return ALEBGK_OK;
 }
 
@@ -599,7 +624,8 @@ int alebgk_managed_cloud(alebgk_managed *m, alebgk_cloud *view)
     view->xyz = c.xyz.data(); view->meshv = c.meshv.data(); view->wall = c.wall.data();
     view->boundary = c.boundary.data(); view->body_id = c.bodyId.data();
     view->nnb = c.nnb.data(); view->nbr = c.nbr.data();
-    view->g = c.g.data(); view->macro = c.macro.data();
+    view->g = c.gs ? c.g.data() : nullptr;
+    view->macro = c.macro.data();
     return ALEBGK_OK;
 }
 

@@ -348,6 +348,13 @@ int alebgk_net_train_step(alebgk_net *net, const float *pts_dev, const float *tg
                           float beta1, float beta2, float eps, float *loss_host);
 int alebgk_net_sync(alebgk_net *net);
 
+/* alebgk_upload for a cloud whose particle set is unchanged: geometry, wall
+ * state, mesh velocity, neighbour lists and tables are replaced, the
+ * distribution, macros and mass bookkeeping stay on the device (cloud->g and
+ * cloud->macro are not read).  For the body steps in which cloud management
+ * leaves the particle set alone. */
+int alebgk_upload_geometry(alebgk_ctx *ctx, const alebgk_cloud *cloud, double dt);
+
 /* Neighbour lists of the context's current device positions (body surface
  * particles included), as Initialization/NeighbourSearch.cpp:17-99 builds
  * them: grid = x0, y0, z0 (box origin), hBox, vBox, wBox (voxel sizes),
@@ -364,7 +371,11 @@ int alebgk_neighbours_device(alebgk_ctx *ctx, const double *grid, const int *box
  * prm = dx, minDist, radius, xleft, xright, ybottom, ytop, zfront, zback,
  * vmin, dv, R, hBox, vBox, wBox; iprm = dim, Nv, nbh, nbv, nbw.  The managed
  * cloud (new N, neighbour lists rebuilt) lives in *out until
- * alebgk_managed_free; alebgk_managed_info gives N, removed, merged, added. */
+ * alebgk_managed_free; alebgk_managed_info gives N, removed, merged, added,
+ * needState.  With cloud->g and cloud->macro NULL the call only decides: it
+ * stops with needState = 1 as soon as the particle set would change (then
+ * call again with the state), and otherwise returns the same cloud with
+ * rebuilt neighbour lists. */
 typedef struct alebgk_managed alebgk_managed;
 int alebgk_manage_cloud(int device, const double *prm, const int *iprm, int nbodies,
                         const alebgk_body *bodies, int N, int gstride,

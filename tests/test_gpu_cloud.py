@@ -60,7 +60,7 @@ def test_cloud_management_equals_reference(name, Nx, Nv, shift):
     b.N = d[0]
     want = _state(b)
     case = Case(name, Nx=Nx, Nv=Nv)
-    got, counts = manage_cloud(case, before, bodies)
+    got, counts, _ = manage_cloud(case, before, bodies)
     assert counts == tuple(cnt), (counts, tuple(cnt))
     assert sum(counts) > 0                       # the shift made work for it
     assert got["xyz"].shape == want["xyz"].shape
@@ -98,7 +98,7 @@ def test_merge_of_close_particles_equals_reference():
     b.L.ref_dims(b.h, d)
     b.N = d[0]
     want = _state(b)
-    got, counts = manage_cloud(Case(name, Nx=Nx, Nv=Nv), before, bodies)
+    got, counts, _ = manage_cloud(Case(name, Nx=Nx, Nv=Nv), before, bodies)
     assert counts == tuple(cnt) and counts[1] >= 1
     for k in ("xyz", "boundary", "body_id", "nnb", "nbr", "g"):
         assert np.array_equal(got[k], want[k]), k
