@@ -160,6 +160,7 @@ SIGNATURES = {
     "alebgk_managed_free": (None, [ctypes.c_void_p]),
     "alebgk_upload_geometry": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Cloud),
                                               ctypes.c_double]),
+    "alebgk_set_coeff_builder": (ctypes.c_int, [ctypes.c_int]),
     "alebgk_moments13": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "alebgk_seed_grad13": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                           c_double_p, c_double_p]),

@@ -19,7 +19,10 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libalebgk_b200.so")
 
-SOURCES = ["step.cu", "march.cu", "body_noalloc.cu", "body_step.cu", "warm.cu", "setup.cu", "cloud.cu", "checkpoint.cpp", "batch.cpp", "slab.cpp", "api.cpp", "coeffs.cpp", "cases.cpp", "march_plan.cpp"]
+SOURCES = ["step.cu", "march.cu", "body_noalloc.cu", "body_step.cu", "warm.cu", "coeffs_dev.cu", "setup.cu", "cloud.cu", "checkpoint.cpp", "batch.cpp", "slab.cpp", "api.cpp", "coeffs.cpp", "cases.cpp", "march_plan.cpp"]
+# The device MLS table builder must round as the host builder (compiled
+# without contraction) does.
+FILE_FLAGS = {"coeffs_dev.cu": ["-fmad=false"]}
 HEADERS = ["ctx.h", "coeffs.h", "cases.h", "march.h", "mbar.cuh", "umma.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -52,7 +55,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
                      "-I" + os.path.join(ROOT, "include")]
     for src in SOURCES:
         obj = os.path.join(objdir, src + ".o")
-        cmd = [nvcc()] + common + ["-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [nvcc()] + common + FILE_FLAGS.get(src, []) + ["-c", os.path.join(CSRC, src), "-o", obj]
         if src.endswith(".cu"):
             cmd += ["-Xptxas", "-v"] if verbose else []
         _run(cmd)

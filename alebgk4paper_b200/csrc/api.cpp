@@ -18,6 +18,7 @@ using namespace alebgk;
 namespace {
 
 std::string gCreateError;
+int gCoeffBuilder = 0;   // 0: tables on the device where possible, 1: host
 
 int fail(alebgk_ctx *c, int code, const std::string &msg)
 {
@@ -194,22 +195,33 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
     in.maxNeigh = ALEBGK_MAX_NEIGH;
     CoeffTables tb, tl;
     std::string err;
-    if (!buildCoefficients(in, tb, &err)) return fail(c, ALEBGK_EINVAL, err);
-    // Linear tables for the MOOD redo (mlsTransportCompute(..., 1, true)),
-    // on the same classes and slot order.
+    // The tables are solved on the device, except where the lattice march
+    // may take the cloud: its plan re-lays the host tables.
+    const bool f64cloud = c->cfg.precision == 64;
+    const bool devTables =
+        gCoeffBuilder == 0 &&
+        !(!f64cloud && c->cfg.transport != 1 &&
+          marchEligible(cl->xyz, N, p.dim, cl->nnb, cl->nbr, ALEBGK_MAX_NEIGH));
     CoeffInput inLin = in;
     inLin.mlsOrder = 1;
-    if (p.limiter == 2)
+    if (devTables)
     {
-        if (!buildCoefficients(inLin, tl, &err)) return fail(c, ALEBGK_EINVAL, err);
-        if (tl.cls != tb.cls || tl.slots != tb.slots || tl.S != tb.S)
-            return fail(c, ALEBGK_EINVAL, "linear and quadratic stencil classes differ");
+        if (!buildClasses(in, tb, &err)) return fail(c, ALEBGK_EINVAL, err);
+    }
+    else
+    {
+        if (!buildCoefficients(in, tb, &err)) return fail(c, ALEBGK_EINVAL, err);
+        // Linear tables for the MOOD redo (mlsTransportCompute(..., 1, true)),
+        // on the same classes and slot order.
+        if (p.limiter == 2)
+        {
+            if (!buildCoefficients(inLin, tl, &err)) return fail(c, ALEBGK_EINVAL, err);
+            if (tl.cls != tb.cls || tl.slots != tb.slots || tl.S != tb.S)
+                return fail(c, ALEBGK_EINVAL, "linear and quadratic stencil classes differ");
+        }
     }
     p.S = tb.S;
     c->ncls = tb.ncls;
-    c->degenerateParticles = 0;
-    for (int k = 0; k < tb.ncls; ++k)
-        if (tb.degenerate[k]) c->degenerateParticles += tb.members[k];
 
     const bool f64 = c->cfg.precision == 64;
     const size_t es = f64 ? 8 : 4;
@@ -228,8 +240,23 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
         for (size_t q = 0; q < ncoef; ++q) cf[q] = (float)src[q];
         return cudaMemcpy(*dst, cf.data(), ncoef * 4, cudaMemcpyHostToDevice);
     };
-    CK(putTable(&d.coef, tb.coef));
-    CK(putTable(&d.coefLin, p.limiter == 2 ? tl.coef : tb.coef));
+    if (devTables)
+    {
+        CK(cudaMalloc(&d.coef, std::max<size_t>(ncoef, 1) * es));
+        CK(cudaMalloc(&d.coefLin, std::max<size_t>(ncoef, 1) * es));
+        CK(buildTablesDevice(in, tb, p.mlsOrder, d.coef, f64, tb.degenerate, c->stream));
+        std::vector<int> degLin;
+        CK(buildTablesDevice(in, tb, p.limiter == 2 ? 1 : p.mlsOrder, d.coefLin, f64, degLin,
+                             c->stream));
+    }
+    else
+    {
+        CK(putTable(&d.coef, tb.coef));
+        CK(putTable(&d.coefLin, p.limiter == 2 ? tl.coef : tb.coef));
+    }
+    c->degenerateParticles = 0;
+    for (int k = 0; k < tb.ncls; ++k)
+        if (tb.degenerate[k]) c->degenerateParticles += tb.members[k];
     CK(dalloc(&d.pos, 3 * (size_t)N));
     CK(dalloc(&d.meshv, 3 * (size_t)N));
     CK(dalloc(&d.wall, 7 * (size_t)N));
@@ -330,6 +357,13 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
 int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
 {
     return uploadCloud(c, cl, dt, true);
+}
+
+int alebgk_set_coeff_builder(int which)
+{
+    if (which != 0 && which != 1) return ALEBGK_EINVAL;
+    gCoeffBuilder = which;
+    return ALEBGK_OK;
 }
 
 int alebgk_upload_geometry(alebgk_ctx *c, const alebgk_cloud *cl, double dt)

@@ -116,7 +116,7 @@ inline int64_t bitsOf(double d)
 
 }  // namespace
 
-bool buildCoefficients(const CoeffInput &in, CoeffTables &out, std::string *err)
+bool buildClasses(const CoeffInput &in, CoeffTables &out, std::string *err)
 {
     const int N = in.N, ndim = in.dim, Nv = in.Nv;
     if (N <= 0 || Nv < 2 || (ndim != 2 && ndim != 3) || in.h <= 0)
@@ -199,12 +199,21 @@ bool buildCoefficients(const CoeffInput &in, CoeffTables &out, std::string *err)
     keys.clear();
     const int ncls = (int)out.rep.size();
     out.ncls = ncls;
-    out.coef.assign((size_t)ncls * S * V, 0.0);
     out.degenerate.assign(ncls, 0);
     out.order.assign(ncls, 0);
     out.members.assign(ncls, 0);
     for (int i = 0; i < N; ++i) out.members[out.cls[i]]++;
+    for (int c = 0; c < ncls; ++c) out.order[c] = in.boundary[out.rep[c]] ? 1 : in.mlsOrder;
+    return true;
+}
 
+bool buildCoefficients(const CoeffInput &in, CoeffTables &out, std::string *err)
+{
+    if (!buildClasses(in, out, err)) return false;
+    const int N = in.N, ndim = in.dim, Nv = in.Nv;
+    (void)N;
+    const int V = out.V, S = out.S, ncls = out.ncls;
+    out.coef.assign((size_t)ncls * S * V, 0.0);
 #pragma omp parallel for schedule(dynamic, 1)
     for (int c = 0; c < ncls; ++c)
     {

@@ -50,6 +50,9 @@ struct CoeffTables
 // Builds classes and coefficients.  Returns false with *err on bad input.
 bool buildCoefficients(const CoeffInput &in, CoeffTables &out, std::string *err);
 
+// The class part alone (cls, nslot, slots, rep, members, order; no coef).
+bool buildClasses(const CoeffInput &in, CoeffTables &out, std::string *err);
+
 // Partial-pivot Gaussian elimination with the reference's |pivot| < 1e-30
 // skip rule (MLSTransport/MLSTransport.cpp:20-62), applied to nrhs
 // right-hand sides at once: A is n x n row-major, B is n x nrhs row-major and

@@ -160,6 +160,12 @@ struct NeighbourGrid
 cudaError_t buildNeighboursDevice(const NeighbourGrid &g, const double *xyz, int N,
                                   const LatticeDev &o, cudaStream_t st);
 cudaError_t launchRestState(alebgk_ctx *c, const double *rowDev, double rho, double T0);
+struct CoeffInput;
+struct CoeffTables;
+// MLS tables of the classes `cls` built on the device (coeffs_dev.cu).
+cudaError_t buildTablesDevice(const CoeffInput &in, const CoeffTables &cls, int order,
+                              void *table, bool f64, std::vector<int> &degenerate,
+                              cudaStream_t st);
 cudaError_t launchSeedGrad13(alebgk_ctx *c, const float *net, int ldnet, const double *scale,
                              const double *shift);
 cudaError_t launchMoments13(alebgk_ctx *c, double *out);

@@ -54,6 +54,11 @@ struct MarchPlan
 
 // Detects the lattice and builds the plan; plan.ok is false when the cloud
 // is not a complete lattice with two-step stencils.
+// Whether a cloud is a complete lattice in generation order with every
+// neighbour within the march's 81-offset template (the test of buildMarchPlan).
+bool marchEligible(const double *xyz, int N, int dim, const int *nnb, const int *nbr,
+                   int maxNeigh);
+
 void buildMarchPlan(const double *xyz, int N, int dim, const int *nnb,
                     const int *nbr, int maxNeigh, const CoeffTables &tb,
                     const CoeffTables *tl, MarchPlan &plan);

@@ -48,6 +48,35 @@ int axisRanks(const double *xyz, int N, int axis, std::vector<int> &rank)
 
 }  // namespace
 
+bool marchEligible(const double *xyz, int N, int dim, const int *nnb, const int *nbr,
+                   int maxNeigh)
+{
+    if (dim != 3 || N < 8) return false;
+    std::vector<int> rx, ry, rz;
+    const int nx = axisRanks(xyz, N, 0, rx);
+    const int ny = axisRanks(xyz, N, 1, ry);
+    const int nz = axisRanks(xyz, N, 2, rz);
+    if ((long long)nx * ny * nz != N || nx < 2 || ny < 2 || nz < 2) return false;
+    const bool zdesc = rz[0] > rz[(size_t)nx * ny];
+    for (int i = 0; i < N; ++i)
+    {
+        const int ix = i % nx, iy = (i / nx) % ny, iz = i / (nx * ny);
+        const int ez = zdesc ? nz - 1 - iz : iz;
+        if (rx[i] != ix || ry[i] != iy || rz[i] != ez) return false;
+    }
+    for (int i = 0; i < N; ++i)
+    {
+        const int xi = i % nx, yi = (i / nx) % ny, zi = i / (nx * ny);
+        for (int s = 0; s < nnb[i]; ++s)
+        {
+            const int j = nbr[(size_t)i * maxNeigh + s];
+            if (templateIndex(j % nx - xi, (j / nx) % ny - yi, j / (nx * ny) - zi) < 0)
+                return false;
+        }
+    }
+    return true;
+}
+
 void buildMarchPlan(const double *xyz, int N, int dim, const int *nnb, const int *nbr,
                     int maxNeigh, const CoeffTables &tb, const CoeffTables *tl,
                     MarchPlan &plan)

@@ -348,6 +348,12 @@ int alebgk_net_train_step(alebgk_net *net, const float *pts_dev, const float *tg
                           float beta1, float beta2, float eps, float *loss_host);
 int alebgk_net_sync(alebgk_net *net);
 
+/* Where alebgk_upload builds the MLS coefficient tables: 0 (default) on the
+ * device, bitwise equal to the host builder, except for clouds the lattice
+ * march takes (its plan needs the host tables); 1 always on the host.
+ * Process-wide; for checks of one against the other. */
+int alebgk_set_coeff_builder(int which);
+
 /* alebgk_upload for a cloud whose particle set is unchanged: geometry, wall
  * state, mesh velocity, neighbour lists and tables are replaced, the
  * distribution, macros and mass bookkeeping stay on the device (cloud->g and
