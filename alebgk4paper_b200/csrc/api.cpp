@@ -198,9 +198,11 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
     // The tables are solved on the device, except where the lattice march
     // may take the cloud: its plan re-lays the host tables.
     const bool f64cloud = c->cfg.precision == 64;
+    bool anyBody = false;
+    for (int i = 0; i < N && !anyBody; ++i) anyBody = cl->body_id[i] >= 0;
     const bool devTables =
         gCoeffBuilder == 0 &&
-        !(!f64cloud && c->cfg.transport != 1 &&
+        !(!f64cloud && c->cfg.transport != 1 && !anyBody &&
           marchEligible(cl->xyz, N, p.dim, cl->nnb, cl->nbr, ALEBGK_MAX_NEIGH));
     CoeffInput inLin = in;
     inLin.mlsOrder = 1;

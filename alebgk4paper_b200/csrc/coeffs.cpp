@@ -146,8 +146,8 @@ bool buildClasses(const CoeffInput &in, CoeffTables &out, std::string *err)
     // geometric difference between distinct stencils and far above the
     // rounding of x_j - x_i, so translated copies of a stencil compare equal.
     const double q = in.h * std::ldexp(1.0, -32);
-    std::unordered_map<std::vector<int64_t>, int, KeyHash> classOf;
     std::vector<std::vector<int64_t>> keys(N);
+    std::vector<uint64_t> hashes(N);
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < N; ++i)
     {
@@ -183,18 +183,25 @@ bool buildClasses(const CoeffInput &in, CoeffTables &out, std::string *err)
             for (int a = 0; a < 7; ++a) k.push_back(bitsOf(in.wall[7 * i + a]));
         for (int s = 0; s < nn; ++s)
             for (int a = 0; a < 3; ++a) k.push_back(nb[s].first[a]);
+        hashes[i] = KeyHash()(k);
     }
+    // Class ids in order of first appearance; keys are hashed in parallel
+    // above and compared in full on a hash hit.
+    std::unordered_map<uint64_t, std::vector<int>> byHash;
+    byHash.reserve(1024);
     for (int i = 0; i < N; ++i)
     {
-        auto it = classOf.find(keys[i]);
-        if (it == classOf.end())
+        std::vector<int> &cand = byHash[hashes[i]];
+        int id = -1;
+        for (int c : cand)
+            if (keys[out.rep[c]] == keys[i]) { id = c; break; }
+        if (id < 0)
         {
-            int id = (int)out.rep.size();
-            classOf.emplace(keys[i], id);
+            id = (int)out.rep.size();
+            cand.push_back(id);
             out.rep.push_back(i);
-            out.cls[i] = id;
         }
-        else out.cls[i] = it->second;
+        out.cls[i] = id;
     }
     keys.clear();
     const int ncls = (int)out.rep.size();

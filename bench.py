@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--workload", default="cavity3d",
-                    choices=["cavity3d", "batched-cavity2d", "warm-start"],
+                    choices=["cavity3d", "batched-cavity2d", "warm-start", "free-body"],
                     help="cavity3d (the headline line), the batched cavity2d workload "
                          "(96 seeded cavities advanced by one graph launch per step), or the "
                          "learned warm start on 32 held-out cavity2d cases")
@@ -521,6 +521,74 @@ def run_ncu(args):
     s.close()
 
 
+def run_free_body(args):
+    """The free-body cube (cavity3d-cube Nx40 Nv10, density 4.4, parabolic lid
+    10 m/s, dt 1.5e-11): --steps steps of fluid step, Heun body step and cloud
+    management, in FP32 and in FP64; per-step wall time, the cube's path and
+    accumulated rotation, and the FP32 run's deviation from the FP64 run."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    import torch
+    torch.cuda.set_device(local)
+    import alebgk4paper_b200 as ab
+    runs = {}
+    for prec in (32, 64):
+        c = ab.Case("cavity3d-cube", 40, 10, -1.0, 2, fixed_body=False)
+        s = ab.Solver(c, precision=prec, device=local)
+        st = c.bodies.copy()
+        path, t_step, t_body, t_refresh, changes = [st.copy()], 0.0, 0.0, 0.0, 0
+        with ClockSampler(local) as clk:
+            for k in range(args.steps):
+                t0 = time.perf_counter()
+                s.cudaStep(1)
+                s.sync()
+                t1 = time.perf_counter()
+                st = s.body_step(st)
+                c.bodies = st
+                t2 = time.perf_counter()
+                changes += sum(s.refresh_geometry())
+                t3 = time.perf_counter()
+                t_step += t1 - t0
+                t_body += t2 - t1
+                t_refresh += t3 - t2
+                path.append(st.copy())
+        s.close()
+        path = np.array(path)[:, 0]
+        R = path[:, 22:31].reshape(-1, 3, 3)
+        R0T = R[0].T
+        ang = [float(np.degrees(np.arccos(np.clip((np.trace(Ri @ R0T) - 1) / 2, -1, 1))))
+               for Ri in R]
+        runs[prec] = dict(path=path, angle=np.array(ang),
+                          s_per_step=(t_step + t_body + t_refresh) / args.steps,
+                          fluid_ms=1e3 * t_step / args.steps, body_ms=1e3 * t_body / args.steps,
+                          refresh_ms=1e3 * t_refresh / args.steps, cloud_changes=changes,
+                          clocks=clk.summary())
+    a, b = runs[32], runs[64]
+    disp64 = b["path"][-1, 0:3] - b["path"][0, 0:3]
+    dev_centre = float(np.abs(a["path"][:, 0:3] - b["path"][:, 0:3]).max())
+    print(json.dumps({
+        "metric": "free-body cube steps/s", "value": 1.0 / a["s_per_step"], "unit": "steps/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": 0, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 fluid, f64 body",
+        "data": "synthetic: the reference's cavity3d-cube free-body case set-up",
+        "config": {"workload": "cavity3d-cube free body Nx=40 Nv=10, rho 4.4, parabolic lid "
+                               "10 m/s, dt 1.5e-11"},
+        "f32": {k: a[k] for k in ("s_per_step", "fluid_ms", "body_ms", "refresh_ms",
+                                  "cloud_changes")},
+        "f64": {k: b[k] for k in ("s_per_step", "fluid_ms", "body_ms", "refresh_ms",
+                                  "cloud_changes")},
+        "rotation_deg": {"f32": float(a["angle"][-1]), "f64": float(b["angle"][-1]),
+                         "rel_diff": float(abs(a["angle"][-1] - b["angle"][-1]) /
+                                           max(abs(b["angle"][-1]), 1e-300))},
+        "displacement_m": {"f64": disp64.tolist(),
+                           "max_centre_diff_m": dev_centre,
+                           "rel_to_displacement": dev_centre / max(np.linalg.norm(disp64),
+                                                                   1e-300)},
+        "clocks": a["clocks"],
+    }))
+
+
 def run_ncu_warm(args):
     """Profiler mode of the warm-start workload: the network kernels alone,
     three inference passes and three training steps on seeded points."""
@@ -548,6 +616,8 @@ def main():
         run_batched(args)
     elif args.workload == "warm-start" and args.impl == "ours":
         run_warm_start(args)
+    elif args.workload == "free-body" and args.impl == "ours":
+        run_free_body(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
