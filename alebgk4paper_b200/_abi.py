@@ -106,6 +106,8 @@ SIGNATURES = {
     "alebgk_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                            ctypes.POINTER(ctypes.c_void_p)]),
     "alebgk_batch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "alebgk_batch_set_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "alebgk_batch_get_mode": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p]),
     "alebgk_batch_residuals": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
     "alebgk_batch_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "alebgk_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),

@@ -76,12 +76,20 @@ class BatchSolver:
     launch shapes are tuned before the batch graph is captured.  With
     ``setup="device"`` each cavity's lattice, neighbour lists and rest state
     are built on the GPU (:class:`LatticeCase`) instead of on the host.
+
+    ``launch="stages"`` (default) advances all cavities by one launch per
+    stage of the step when they qualify (same precision and Chu layers,
+    plain transport and particle kernels); ``launch="branches"`` puts every
+    cavity's own step in the graph as a parallel branch.  Both compute each
+    cavity exactly as it would step alone.
     """
 
     def __init__(self, specs, precision: int = 32, device: int = 0, autotune: bool = False,
-                 tune_steps: int = 3, setup: str = "host"):
+                 tune_steps: int = 3, setup: str = "host", launch: str = "stages"):
         if setup not in ("host", "device"):
             raise ValueError("setup must be 'host' or 'device'")
+        if launch not in ("stages", "branches"):
+            raise ValueError("launch must be 'stages' or 'branches'")
         self.lib = _abi.load()
         self.specs = list(specs)
         self.cases = []
@@ -101,6 +109,17 @@ class BatchSolver:
         _check(self.lib.alebgk_batch_create(n, arr, ctypes.byref(h)), self.solvers[0].ctx)
         self.h = h
         self.steps = 0
+        _check(self.lib.alebgk_batch_set_mode(self.h, 0 if launch == "stages" else 1),
+               self.solvers[0].ctx)
+
+    @property
+    def staged(self) -> bool:
+        """True when the step graph holds one launch per stage over all
+        cavities (known after the first step)."""
+        mode, staged = ctypes.c_int(), ctypes.c_int()
+        _check(self.lib.alebgk_batch_get_mode(self.h, ctypes.byref(mode), ctypes.byref(staged)),
+               self.solvers[0].ctx)
+        return bool(staged.value)
 
     @property
     def updates_per_step(self) -> int:

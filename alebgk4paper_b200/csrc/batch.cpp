@@ -1,11 +1,15 @@
 // batch.cpp -- launch-shape autotuning, the steady residual, and batches of
 // independent cavities advanced by one CUDA graph per step.
 //
-// A batch holds contexts on one device that advance in lockstep.  One graph
-// per ping-pong parity holds every context's whole step (and its residual)
-// as a parallel branch: a master stream forks to each context's stream and
-// joins them again, so one graph launch advances all cavities and the small
-// kernels of different cavities share the SMs.
+// A batch holds contexts on one device that advance in lockstep, one graph
+// launch per step.  When every context has the same precision and Chu
+// layers and runs the plain transport and particle kernels, the graph holds
+// one launch per stage of the step over all contexts (step.cu's batch
+// kernels: a block finds its context from per-stage block offsets), eleven
+// nodes whatever the batch size.  Otherwise one graph per ping-pong parity
+// holds every context's whole step (and its residual) as a parallel branch:
+// a master stream forks to each context's stream and joins them again.
+// Both forms compute each context exactly as its own step does.
 #include <cuda_runtime.h>
 
 #include <string>
@@ -24,6 +28,9 @@ struct alebgk_batch
     std::vector<cudaEvent_t> join;
     double *resid = nullptr;              // device, one per context
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int mode = 0;                         // 0 stage launches when possible, 1 branches
+    bool staged = false;                  // the graphs hold stage launches
+    BatchLaunch bl;
     std::string err;
 };
 
@@ -231,12 +238,26 @@ int alebgk_batch_step(alebgk_batch *b, int nsteps)
     for (int n = 0; n < nsteps; ++n)
     {
         const int from = c->cur;
+        if (!b->graph[from] && !b->graph[1 - from] && b->mode == 0 && !b->bl.desc[0])
+        {
+            const cudaError_t be = buildBatchLaunch(b->ctx.data(), (int)b->ctx.size(), b->resid,
+                                                    b->bl);
+            if (be == cudaSuccess) CKC(prepareBatchLaunch(b->bl));
+            else if (be == cudaErrorNotSupported) freeBatchLaunch(b->bl);
+            else
+            {
+                freeBatchLaunch(b->bl);
+                CKC(be);
+            }
+            b->staged = b->bl.desc[0] != nullptr;
+        }
         if (!b->graph[from])
         {
             cudaGraph_t g = nullptr;
             CKC(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
-            cudaError_t le = cudaEventRecord(b->fork, b->master);
-            for (size_t i = 0; i < b->ctx.size() && le == cudaSuccess; ++i)
+            cudaError_t le = b->staged ? launchBatchStep(b->bl, from, b->master)
+                                       : cudaEventRecord(b->fork, b->master);
+            for (size_t i = 0; i < b->ctx.size() && le == cudaSuccess && !b->staged; ++i)
             {
                 alebgk_ctx *x = b->ctx[i];
                 le = cudaStreamWaitEvent(x->stream, b->fork, 0);
@@ -275,6 +296,30 @@ int alebgk_batch_step(alebgk_batch *b, int nsteps)
     return ALEBGK_OK;
 }
 
+int alebgk_batch_set_mode(alebgk_batch *b, int mode)
+{
+    if (!b || mode < 0 || mode > 1) return ALEBGK_EINVAL;
+    if (mode != b->mode)
+    {
+        cudaSetDevice(b->device);
+        cudaStreamSynchronize(b->master);
+        for (auto &g : b->graph)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        freeBatchLaunch(b->bl);
+        b->staged = false;
+        b->mode = mode;
+    }
+    return ALEBGK_OK;
+}
+
+int alebgk_batch_get_mode(alebgk_batch *b, int *mode, int *staged)
+{
+    if (!b || !mode || !staged) return ALEBGK_EINVAL;
+    *mode = b->mode;
+    *staged = b->staged ? 1 : 0;
+    return ALEBGK_OK;
+}
+
 int alebgk_batch_residuals(alebgk_batch *b, double *out)
 {
     if (!b || !out) return ALEBGK_EINVAL;
@@ -301,6 +346,7 @@ int alebgk_batch_destroy(alebgk_batch *b)
     if (b->master) cudaStreamSynchronize(b->master);
     for (auto &g : b->graph)
         if (g) cudaGraphExecDestroy(g);
+    freeBatchLaunch(b->bl);
     for (auto &e : b->join)
         if (e) cudaEventDestroy(e);
     if (b->fork) cudaEventDestroy(b->fork);

@@ -137,6 +137,23 @@ cudaError_t launchMassInit(alebgk_ctx *c);
 // Slab groups (slab.cpp): one segment of the split step (0..3) on stream st,
 // the cross-slab combine of a segment's partial sums (phase 0..3, 4 = set-up
 // mass), and the owned-range mass of a freshly uploaded slab into slabPart[1].
+// Batches of clouds stepped by one launch per stage (step.cu): per-parity
+// device descriptors, per-stage block offsets, launch sizes.
+struct BatchLaunch
+{
+    void *desc[2] = {nullptr, nullptr};
+    int *off = nullptr;
+    int n = 0, L = 1;
+    bool f64 = false;
+    size_t smemParticle = 0, smemRedo = 0;
+    int blocks[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+};
+// cudaErrorNotSupported when the clouds cannot share launches (mixed
+// precision or layers, the streamed particle kernel or the lattice march).
+cudaError_t buildBatchLaunch(alebgk_ctx *const *cs, int n, double *resid, BatchLaunch &bl);
+cudaError_t prepareBatchLaunch(const BatchLaunch &bl);
+cudaError_t launchBatchStep(const BatchLaunch &bl, int from, cudaStream_t st);
+void freeBatchLaunch(BatchLaunch &bl);
 cudaError_t launchSlabSegment(alebgk_ctx *c, int from, int seg, cudaStream_t st);
 cudaError_t launchSlabCombine(StepScalars *const *scs, int n, int phase, cudaStream_t st);
 cudaError_t launchSlabInitSum(alebgk_ctx *c, cudaStream_t st);

@@ -109,15 +109,11 @@ __device__ __forceinline__ double minImage(double d, double L)
 // by the stored-state scale so that gt carries the true magnitude.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(kNT)
-k_transport(const T *__restrict__ f, T *__restrict__ g,
+__device__ __forceinline__ void transportNode(const T *__restrict__ f, T *__restrict__ g,
             const T *__restrict__ coef, const int *__restrict__ cls,
             const int *__restrict__ nslot, const int *__restrict__ slots,
-            int S, int V, int L, int ldf, const StepScalars *__restrict__ sc)
+            int S, int V, int L, int ldf, const StepScalars *__restrict__ sc, int i, int k)
 {
-    const int i = blockIdx.x;
-    const int k = blockIdx.y * blockDim.x + threadIdx.x;
-    if (k >= V) return;
     const T scale = T(sc->scale);
     const int c = cls[i], ns = nslot[i];
     const T *cc = coef + (size_t)c * S * V + k;
@@ -144,6 +140,42 @@ k_transport(const T *__restrict__ f, T *__restrict__ g,
         }
         g[(size_t)i * ldf + k] = a0 * scale;
     }
+}
+
+// Tile = 2 particles per warp of consecutive particles x 32 velocities (one
+// per lane).  The particles of a tile share most of their neighbours, so the
+// tile's gathers of neighbour rows hit L1 after the first; the velocity
+// chunks of a tile are consecutive blocks and meet the same rows in L2.
+constexpr int kTransportPPW = 2;
+
+template <typename T>
+__device__ __forceinline__ void k_transport_body(const T *__restrict__ f, T *__restrict__ g,
+            const T *__restrict__ coef, const int *__restrict__ cls,
+            const int *__restrict__ nslot, const int *__restrict__ slots,
+            int S, int N, int V, int L, int ldf, const StepScalars *__restrict__ sc, int chunk,
+            int tile)
+{
+    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int k = chunk * 32 + (threadIdx.x & 31);
+    if (k >= V) return;
+    const int i0 = tile * nw * kTransportPPW;
+    for (int j = warp; j < nw * kTransportPPW; j += nw)
+    {
+        const int i = i0 + j;
+        if (i >= N) break;
+        transportNode(f, g, coef, cls, nslot, slots, S, V, L, ldf, sc, i, k);
+    }
+}
+
+// Grid (velocity chunks of 32, particle tiles).
+template <typename T>
+__global__ void __launch_bounds__(kNT)
+k_transport(const T *__restrict__ f, T *__restrict__ g,
+            const T *__restrict__ coef, const int *__restrict__ cls,
+            const int *__restrict__ nslot, const int *__restrict__ slots,
+            int S, int N, int V, int L, int ldf, const StepScalars *__restrict__ sc)
+{
+    k_transport_body(f, g, coef, cls, nslot, slots, S, N, V, L, ldf, sc, blockIdx.x, blockIdx.y);
 }
 
 // Walks the nodes k = lane, lane + 32, ... of a particle row and keeps the
@@ -467,14 +499,14 @@ __device__ int screen(const ParticleArgs<T> &a, const StepParams &p, int i, int 
 // screen flags is listed for k_redo and left as is.
 // ---------------------------------------------------------------------------
 template <typename T, int L>
-__global__ void __launch_bounds__(kNT)
-k_particle(ParticleArgs<T> a, StepParams p, int warpsPerBlock)
+__device__ __forceinline__ void k_particle_body(const ParticleArgs<T> &a, const StepParams &p,
+                                                int warpsPerBlock, int bx)
 {
     __shared__ double tab[kNT / 32][3][kMaxNv];
     extern __shared__ __align__(16) unsigned char rowSmem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp >= warpsPerBlock) return;
-    const int i = blockIdx.x * warpsPerBlock + warp;
+    const int i = bx * warpsPerBlock + warp;
     if (i >= p.N) return;                        // warp-uniform
     T *buf = reinterpret_cast<T *>(rowSmem) + (size_t)warp * L * p.V;
     RowRegs<T, L> r(a.g + (size_t)i * p.ldf, buf, p, lane);
@@ -493,6 +525,13 @@ k_particle(ParticleArgs<T> a, StepParams p, int warpsPerBlock)
     }
     if (flagged) return;
     finishParticle(a, p, i, r, pv, tab[warp]);
+}
+
+template <typename T, int L>
+__global__ void __launch_bounds__(kNT)
+k_particle(ParticleArgs<T> a, StepParams p, int warpsPerBlock)
+{
+    k_particle_body<T, L>(a, p, warpsPerBlock, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -947,14 +986,14 @@ k_particle_stream(ParticleArgs<T> a, StepParams p, int wpb)
 // state, one block per particle, then positivity and finish on warp 0.
 // ---------------------------------------------------------------------------
 template <typename T, int L>
-__global__ void __launch_bounds__(kNT)
-k_redo(ParticleArgs<T> a, StepParams p)
+__device__ __forceinline__ void k_redo_body(const ParticleArgs<T> &a, const StepParams &p, int bx,
+                                            int gx)
 {
     __shared__ double tab[3][kMaxNv];
     extern __shared__ __align__(16) unsigned char rowSmem[];
     const int nflag = a.sc->nflag;
     const T scale = T(a.sc->scale);
-    for (int li = blockIdx.x; li < nflag; li += gridDim.x)
+    for (int li = bx; li < nflag; li += gx)
     {
         const int i = a.flagList[li];
         const int ns = a.nslot[i];
@@ -990,19 +1029,26 @@ k_redo(ParticleArgs<T> a, StepParams p)
     }
 }
 
+template <typename T, int L>
+__global__ void __launch_bounds__(kNT)
+k_redo(ParticleArgs<T> a, StepParams p)
+{
+    k_redo_body<T, L>(a, p, blockIdx.x, gridDim.x);
+}
+
 // Finishes the listed particles once sigma is known, on true magnitudes:
 // moments (kept from the previous step when the row has no positive mass,
 // Moments.cpp:89), collision, moments; stored as h = g / sigma with the
 // macros' density and pressure divided by sigma, as k_scale_mood expects.
 template <typename T>
-__global__ void __launch_bounds__(kNT)
-k_fixup(ParticleArgs<T> a, StepParams p)
+__device__ __forceinline__ void k_fixup_body(const ParticleArgs<T> &a, const StepParams &p, int bx,
+                                             int gx)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ndeg = a.sc->ndeg;
     const double sigma = a.sc->sigma;
     const int V = p.V, dim = p.dim;
-    for (int li = blockIdx.x * (kNT / 32) + warp; li < ndeg; li += gridDim.x * (kNT / 32))
+    for (int li = bx * (kNT / 32) + warp; li < ndeg; li += gx * (kNT / 32))
     {
         const int i = a.degList[li];
         T *row = a.g + (size_t)i * p.ldf;
@@ -1088,6 +1134,13 @@ k_fixup(ParticleArgs<T> a, StepParams p)
     }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(kNT)
+k_fixup(ParticleArgs<T> a, StepParams p)
+{
+    k_fixup_body(a, p, blockIdx.x, gridDim.x);
+}
+
 // Deterministic single-block sums: thread t sums elements t, t + nt, ...
 // (coalesced) into four interleaved partial sums, combined in a fixed order.
 template <int K>
@@ -1124,13 +1177,14 @@ constexpr int kRedBlocks = 64;
 constexpr int kRedThreads = 256;
 
 __device__ bool gridSumLast(const double *__restrict__ a, int N, double *partial,
-                            StepScalars *sc, double *total)
+                            StepScalars *sc, double *total, int bx = -1, int gx = -1)
 {
     __shared__ double sh[32];
     __shared__ bool last;
-    const int t = threadIdx.x, stride = gridDim.x * blockDim.x;
+    if (bx < 0) { bx = blockIdx.x; gx = gridDim.x; }
+    const int t = threadIdx.x, stride = gx * blockDim.x;
     double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-    int i = blockIdx.x * blockDim.x + t;
+    int i = bx * blockDim.x + t;
     for (; i + 3 * stride < N; i += 4 * stride)
     {
         s0 += a[i];
@@ -1143,15 +1197,15 @@ __device__ bool gridSumLast(const double *__restrict__ a, int N, double *partial
     blockSums<1>(v, sh);
     if (t == 0)
     {
-        partial[blockIdx.x] = v[0];
+        partial[bx] = v[0];
         __threadfence();
-        last = atomicAdd(&sc->redCount, 1u) == gridDim.x - 1;
+        last = atomicAdd(&sc->redCount, 1u) == (unsigned)gx - 1;
     }
     __syncthreads();
     if (!last || t != 0) return false;
     __threadfence();
     double s = 0.0;
-    for (int b = 0; b < (int)gridDim.x; ++b) s += ((volatile double *)partial)[b];
+    for (int b = 0; b < gx; ++b) s += ((volatile double *)partial)[b];
     sc->redCount = 0;
     *total = s;
     return true;
@@ -1187,11 +1241,11 @@ k_mass_sum(const double *__restrict__ massEnd, int N, double *partial, StepScala
 
 // Applies sigma to the macros and runs moodCheck (Conservation.cpp:16-38,
 // MLSBasis.hpp:208-222) on the true values.
-__global__ void k_scale_mood(StepParams p, const int *__restrict__ boundary,
+__device__ __forceinline__ void k_scale_mood_body(const StepParams &p, const int *__restrict__ boundary,
                              double *__restrict__ macNew, const double *__restrict__ minG,
-                             int *__restrict__ mood, StepScalars *sc)
+                             int *__restrict__ mood, StepScalars *sc, int bx)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = bx * blockDim.x + threadIdx.x;
     if (i >= p.N) return;
     const double sigma = sc->sigma;
     double *mac = macNew + 6 * (size_t)i;
@@ -1206,16 +1260,23 @@ __global__ void k_scale_mood(StepParams p, const int *__restrict__ boundary,
     if (fail) atomicOr(&sc->moodfail, 1);
 }
 
+__global__ void 
+k_scale_mood(StepParams p, const int *__restrict__ boundary,
+                             double *__restrict__ macNew, const double *__restrict__ minG,
+                             int *__restrict__ mood, StepScalars *sc)
+{
+    k_scale_mood_body(p, boundary, macNew, minG, mood, sc, blockIdx.x);
+}
+
 // Second collision + moments of every interior particle when moodCheck
 // failed (Solver/Solver.cpp:685-693).  Exits at once otherwise.
 template <typename T>
-__global__ void __launch_bounds__(kNT)
-k_recollide(T *__restrict__ g, StepParams p, const int *__restrict__ boundary,
-            double *__restrict__ macNew, double *__restrict__ massEnd, StepScalars *sc)
+__device__ __forceinline__ void k_recollide_body(T *__restrict__ g, const StepParams &p, const int *__restrict__ boundary,
+            double *__restrict__ macNew, double *__restrict__ massEnd, StepScalars *sc, int bx, int gx)
 {
     if (sc->moodfail == 0) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int i = blockIdx.x * (kNT / 32) + warp; i < p.N; i += gridDim.x * (kNT / 32))
+    for (int i = bx * (kNT / 32) + warp; i < p.N; i += gx * (kNT / 32))
     {
     if (boundary[i]) continue;
     const double sigma = sc->sigma;
@@ -1273,6 +1334,14 @@ k_recollide(T *__restrict__ g, StepParams p, const int *__restrict__ boundary,
         massEnd[i] = N0 / sigma;
     }
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kNT)
+k_recollide(T *__restrict__ g, StepParams p, const int *__restrict__ boundary,
+            double *__restrict__ macNew, double *__restrict__ massEnd, StepScalars *sc)
+{
+    k_recollide_body(g, p, boundary, macNew, massEnd, sc, blockIdx.x, gridDim.x);
 }
 
 // Mass at the end of a step whose moodCheck failed (after k_recollide).
@@ -1532,9 +1601,8 @@ __global__ void k_convert_out(const T *src, double *dst, int N, int gs, int ldf,
 // convergence measure of a run to steady state.  One block, fixed order:
 // deterministic.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024)
-k_residual(const double *__restrict__ macNew, const double *__restrict__ macOld,
-           const int *__restrict__ boundary, int N, double R, double *out)
+__device__ __forceinline__ void k_residual_body(const double *__restrict__ macNew, const double *__restrict__ macOld,
+           const int *__restrict__ boundary, int N, double R, double *out, int unused)
 {
     __shared__ double sh[8 * 32];
     double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -1564,6 +1632,13 @@ k_residual(const double *__restrict__ macNew, const double *__restrict__ macOld,
             if (v[4 + q] > 0.0) r = fmax(r, sqrt(v[q] / v[4 + q]));
         *out = r;
     }
+}
+
+__global__ void __launch_bounds__(1024)
+k_residual(const double *__restrict__ macNew, const double *__restrict__ macOld,
+           const int *__restrict__ boundary, int N, double R, double *out)
+{
+    k_residual_body(macNew, macOld, boundary, N, R, out, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -1631,9 +1706,10 @@ static cudaError_t stepT(alebgk_ctx *c, int from, cudaEvent_t *ev)
     else
     {
         const int tt = c->tune.transportThreads;
-        dim3 gt(p.N, (p.V + tt - 1) / tt);
+        const int tileP = (tt / 32) * kTransportPPW;
+        dim3 gt((p.V + 31) / 32, (p.N + tileP - 1) / tileP);
         k_transport<T><<<gt, tt, 0, st>>>(fa, fb, static_cast<const T *>(d.coef),
-                                           d.cls, d.nslot, d.slots, p.S, p.V, p.L,
+                                           d.cls, d.nslot, d.slots, p.S, p.N, p.V, p.L,
                                            p.ldf, d.sc);
     }
     mark();
@@ -1738,6 +1814,339 @@ cudaError_t launchStep(alebgk_ctx *c, int from, cudaEvent_t *ev)
                                     : stepT<float>(c, from, ev);
 }
 
+// ---------------------------------------------------------------------------
+// Batches of small clouds: one launch per stage of the step over every cloud
+// of the batch.  Block b of a stage belongs to the cloud c with
+// off[c] <= b < off[c + 1] and runs that cloud's kernel body with the
+// virtual block index b - off[c] and the cloud's own grid size, so every
+// cloud computes exactly what its own launches compute (same bodies, same
+// block-sum order); only the number of launches changes.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct BatchCtx
+{
+    ParticleArgs<T> pa;        // parity `from`: pa.g = f[1 - from], pa.fold = f[from]
+    StepParams p;
+    const T *coef;
+    double *redPartial;
+    double *resid;
+    int *mood;
+    int wpb;                   // particles (warps) per block of the particle stage
+};
+
+constexpr int kBatchStages = 11;
+constexpr int kBatchTT = 256;  // transport threads per block in a batch
+constexpr int kBatchTile = (kBatchTT / 32) * kTransportPPW;
+
+__device__ __forceinline__ int batchCtxOf(const int *__restrict__ off, int n, int b)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= b) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// The block's cloud descriptor is copied to shared memory: its fields are
+// then read from there as needed instead of occupying registers.
+template <typename T>
+__device__ __forceinline__ const BatchCtx<T> &batchStage(const BatchCtx<T> *__restrict__ ctx,
+                                                         const int *__restrict__ off, int n,
+                                                         int stage, int &vb, int &vg)
+{
+    __shared__ __align__(16) unsigned char raw[sizeof(BatchCtx<T>)];
+    static_assert(sizeof(BatchCtx<T>) % 8 == 0, "descriptor words");
+    const int *o = off + stage * (n + 1);
+    const int c = batchCtxOf(o, n, blockIdx.x);
+    vb = blockIdx.x - o[c];
+    vg = o[c + 1] - o[c];
+    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(ctx + c);
+    unsigned long long *dst = reinterpret_cast<unsigned long long *>(raw);
+    for (int w = threadIdx.x; w < (int)(sizeof(BatchCtx<T>) / 8); w += blockDim.x)
+        dst[w] = src[w];
+    __syncthreads();
+    return *reinterpret_cast<const BatchCtx<T> *>(raw);
+}
+
+#define BATCH_CTX(stage)                                                          \
+    int vb, vg;                                                                    \
+    const BatchCtx<T> &B = batchStage<T>(ctx, off, n, (stage), vb, vg);            \
+    (void)vg
+
+template <typename T>
+__global__ void __launch_bounds__(kNT)
+k_batch_begin(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ off, int n)
+{
+    BATCH_CTX(0);
+    if (vb == 0 && threadIdx.x == 0)
+    {
+        StepScalars *sc = B.pa.sc;
+        sc->nflag = 0;
+        sc->ndeg = 0;
+        sc->nfix = 0;
+        sc->moodfail = 0;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBatchTT)
+k_batch_transport(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ off, int n)
+{
+    BATCH_CTX(1);
+    const StepParams &p = B.p;
+    const int chunks = (p.V + 31) / 32;
+    k_transport_body<T>(B.pa.fold, B.pa.g, B.coef, B.pa.cls, B.pa.nslot, B.pa.slots, p.S, p.N,
+                        p.V, p.L, p.ldf, B.pa.sc, vb % chunks, vb / chunks);
+}
+
+template <typename T, int L>
+__global__ void __launch_bounds__(kNT, 4)
+k_batch_particle(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ off, int n)
+{
+    BATCH_CTX(2);
+    k_particle_body<T, L>(B.pa, B.p, B.wpb, vb);
+}
+
+template <typename T, int L>
+__global__ void __launch_bounds__(kNT)
+k_batch_redo(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ off, int n)
+{
+    BATCH_CTX(3);
+    k_redo_body<T, L>(B.pa, B.p, vb, vg);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads)
+k_batch_sigma(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ off, int n)
+{
+    BATCH_CTX(4);
+    StepScalars *sc = B.pa.sc;
+    double m;
+    if (gridSumLast(B.pa.massPos, B.p.N, B.redPartial, sc, &m, vb, vg))
+    {
+        sc->massNew = m;
+        sc->sigma = (m > 1.0e-30) ? sc->massOld / m : 1.0;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kNT)
+k_batch_fixup(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ off, int n)
+{
+    BATCH_CTX(5);
+    k_fixup_body<T>(B.pa, B.p, vb, vg);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads)
+k_batch_mass_sum(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ off, int n)
+{
+    BATCH_CTX(6);
+    StepScalars *sc = B.pa.sc;
+    double m;
+    if (gridSumLast(B.pa.massEnd, B.p.N, B.redPartial, sc, &m, vb, vg))
+    {
+        const double sigma = sc->sigma;
+        sc->massEnd = sigma * m;
+        sc->massOld = sc->massEnd;
+        sc->scale = sigma;
+        sc->steps += 1;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_batch_scale_mood(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ off, int n)
+{
+    BATCH_CTX(7);
+    k_scale_mood_body(B.p, B.pa.boundary, B.pa.macNew, B.pa.minG, B.mood, B.pa.sc, vb);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kNT)
+k_batch_recollide(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ off, int n)
+{
+    BATCH_CTX(8);
+    k_recollide_body<T>(B.pa.g, B.p, B.pa.boundary, B.pa.macNew, B.pa.massEnd, B.pa.sc, vb, vg);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads)
+k_batch_mass_end(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ off, int n)
+{
+    BATCH_CTX(9);
+    StepScalars *sc = B.pa.sc;
+    if (sc->moodfail == 0) return;
+    double m;
+    if (gridSumLast(B.pa.massEnd, B.p.N, B.redPartial, sc, &m, vb, vg))
+    {
+        sc->massEnd = sc->sigma * m;
+        sc->massOld = sc->massEnd;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024)
+k_batch_residual(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ off, int n)
+{
+    BATCH_CTX(10);
+    k_residual_body(B.pa.macNew, B.pa.macPrev, B.pa.boundary, B.p.N, B.p.R, B.resid, 0);
+}
+
+#undef BATCH_CTX
+
+template <typename T>
+static cudaError_t buildBatchT(alebgk_ctx *const *cs, int n, double *resid, BatchLaunch &bl)
+{
+    const int L = cs[0]->sp.L;
+    std::vector<BatchCtx<T>> h[2];
+    std::vector<int> off((size_t)kBatchStages * (n + 1), 0);
+    size_t smemP = 0, smemR = 0;
+    for (int i = 0; i < n; ++i)
+    {
+        alebgk_ctx *c = cs[i];
+        const StepParams &p = c->sp;
+        DeviceBuffers &d = c->d;
+        const size_t rowBytes = (size_t)p.L * p.V * sizeof(T);
+        // A batch has parallelism enough in its clouds: every particle block
+        // holds as many particles as fit (the launch shape changes no result).
+        const int wpb = particleWarpsPerBlock(p, sizeof(T));
+        smemP = std::max(smemP, wpb * rowBytes);
+        smemR = std::max(smemR, rowBytes);
+        const int pBlocks = (p.N + kNT / 32 - 1) / (kNT / 32);
+        const int blocks[kBatchStages] = {1,
+                                          ((p.V + 31) / 32) *
+                                              ((p.N + kBatchTile - 1) / kBatchTile),
+                                          (p.N + wpb - 1) / wpb,
+                                          std::min(p.N, 296),
+                                          kRedBlocks,
+                                          std::min(pBlocks, 296),
+                                          kRedBlocks,
+                                          (p.N + 255) / 256,
+                                          p.limiter == 2 ? std::min(pBlocks, 592) : 0,
+                                          p.limiter == 2 ? kRedBlocks : 0,
+                                          1};
+        for (int s = 0; s < kBatchStages; ++s)
+            off[(size_t)s * (n + 1) + i + 1] = off[(size_t)s * (n + 1) + i] + blocks[s];
+        for (int from = 0; from < 2; ++from)
+        {
+            BatchCtx<T> b{};
+            ParticleArgs<T> &pa = b.pa;
+            pa.g = static_cast<T *>(d.f[1 - from]);
+            pa.fold = static_cast<const T *>(d.f[from]);
+            pa.coefLin = static_cast<const T *>(d.coefLin);
+            pa.boundary = d.boundary; pa.cls = d.cls; pa.nslot = d.nslot; pa.slots = d.slots;
+            pa.wall = d.wall; pa.macPrev = d.macro[from]; pa.macNew = d.macro[1 - from];
+            pa.massPos = d.massPos; pa.massEnd = d.massEnd; pa.minG = d.minG; pa.dpx = d.dpx;
+            pa.flag = d.flag; pa.flagList = d.flagList; pa.degList = d.degList; pa.sc = d.sc;
+            pa.nad = d.nad;
+            b.p = p;
+            b.mood = d.mood;
+            b.coef = static_cast<const T *>(d.coef);
+            b.redPartial = d.redPartial;
+            b.resid = resid + i;
+            b.wpb = wpb;
+            h[from].push_back(b);
+        }
+    }
+    for (int s = 0; s < kBatchStages; ++s) bl.blocks[s] = off[(size_t)s * (n + 1) + n];
+    cudaError_t e = cudaSuccess;
+    for (int from = 0; from < 2 && e == cudaSuccess; ++from)
+    {
+        e = cudaMalloc(&bl.desc[from], sizeof(BatchCtx<T>) * n);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(bl.desc[from], h[from].data(), sizeof(BatchCtx<T>) * n,
+                           cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = cudaMalloc(&bl.off, sizeof(int) * off.size());
+    if (e == cudaSuccess)
+        e = cudaMemcpy(bl.off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice);
+    bl.n = n;
+    bl.L = L;
+    bl.smemParticle = smemP;
+    bl.smemRedo = smemR;
+    return e;
+}
+
+cudaError_t buildBatchLaunch(alebgk_ctx *const *cs, int n, double *resid, BatchLaunch &bl)
+{
+    bl = BatchLaunch();
+    if (n < 1) return cudaErrorInvalidValue;
+    alebgk_ctx *c0 = cs[0];
+    for (int i = 0; i < n; ++i)
+    {
+        alebgk_ctx *c = cs[i];
+        if (c->cfg.precision != c0->cfg.precision || c->sp.L != c0->sp.L || c->pStream ||
+            c->march.enabled || c->cfg.device != c0->cfg.device)
+            return cudaErrorNotSupported;
+    }
+    bl.f64 = c0->cfg.precision == 64;
+    return bl.f64 ? buildBatchT<double>(cs, n, resid, bl) : buildBatchT<float>(cs, n, resid, bl);
+}
+
+template <typename T, int L>
+static cudaError_t batchStepT(const BatchLaunch &bl, int from, cudaStream_t st)
+{
+    const BatchCtx<T> *ctx = static_cast<const BatchCtx<T> *>(bl.desc[from]);
+    const int n = bl.n;
+    const int *off = bl.off;
+    auto go = [&](int s) { return bl.blocks[s] > 0; };
+    if (go(0)) k_batch_begin<T><<<bl.blocks[0], kNT, 0, st>>>(ctx, off, n);
+    if (go(1)) k_batch_transport<T><<<bl.blocks[1], kBatchTT, 0, st>>>(ctx, off, n);
+    if (go(2)) k_batch_particle<T, L><<<bl.blocks[2], kNT, bl.smemParticle, st>>>(ctx, off, n);
+    if (go(3)) k_batch_redo<T, L><<<bl.blocks[3], kNT, bl.smemRedo, st>>>(ctx, off, n);
+    if (go(4)) k_batch_sigma<T><<<bl.blocks[4], kRedThreads, 0, st>>>(ctx, off, n);
+    if (go(5)) k_batch_fixup<T><<<bl.blocks[5], kNT, 0, st>>>(ctx, off, n);
+    if (go(6)) k_batch_mass_sum<T><<<bl.blocks[6], kRedThreads, 0, st>>>(ctx, off, n);
+    if (go(7)) k_batch_scale_mood<T><<<bl.blocks[7], 256, 0, st>>>(ctx, off, n);
+    if (go(8)) k_batch_recollide<T><<<bl.blocks[8], kNT, 0, st>>>(ctx, off, n);
+    if (go(9)) k_batch_mass_end<T><<<bl.blocks[9], kRedThreads, 0, st>>>(ctx, off, n);
+    if (go(10)) k_batch_residual<T><<<bl.blocks[10], 1024, 0, st>>>(ctx, off, n);
+    return cudaGetLastError();
+}
+
+template <typename T, int L>
+static cudaError_t batchPrepareT(const BatchLaunch &bl)
+{
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    auto set = [&](const void *fn, size_t bytes) {
+        cudaFuncAttributes fa{};
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
+        const size_t cap = (size_t)optin - fa.sharedSizeBytes;
+        if (e == cudaSuccess && bytes > cap) e = cudaErrorInvalidValue;
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
+    };
+    set((const void *)k_batch_particle<T, L>, bl.smemParticle);
+    set((const void *)k_batch_redo<T, L>, bl.smemRedo);
+    return e;
+}
+
+cudaError_t prepareBatchLaunch(const BatchLaunch &bl)
+{
+    if (bl.f64) return bl.L == 2 ? batchPrepareT<double, 2>(bl) : batchPrepareT<double, 1>(bl);
+    return bl.L == 2 ? batchPrepareT<float, 2>(bl) : batchPrepareT<float, 1>(bl);
+}
+
+cudaError_t launchBatchStep(const BatchLaunch &bl, int from, cudaStream_t st)
+{
+    if (bl.f64) return bl.L == 2 ? batchStepT<double, 2>(bl, from, st)
+                                 : batchStepT<double, 1>(bl, from, st);
+    return bl.L == 2 ? batchStepT<float, 2>(bl, from, st) : batchStepT<float, 1>(bl, from, st);
+}
+
+void freeBatchLaunch(BatchLaunch &bl)
+{
+    for (void *p : {bl.desc[0], bl.desc[1], (void *)bl.off})
+        if (p) cudaFree(p);
+    bl = BatchLaunch();
+}
+
 template <typename T>
 static cudaError_t massInitT(alebgk_ctx *c)
 {
@@ -1785,9 +2194,11 @@ static cudaError_t slabSegT(alebgk_ctx *c, int from, int seg, cudaStream_t st)
         else
         {
             const int tt = c->tune.transportThreads;
-            dim3 gt(p.N, (p.V + tt - 1) / tt);
+            const int tileP = (tt / 32) * kTransportPPW;
+            dim3 gt((p.V + 31) / 32, (p.N + tileP - 1) / tileP);
             k_transport<T><<<gt, tt, 0, st>>>(fa, fb, static_cast<const T *>(d.coef), d.cls,
-                                               d.nslot, d.slots, p.S, p.V, p.L, p.ldf, d.sc);
+                                               d.nslot, d.slots, p.S, p.N, p.V, p.L, p.ldf,
+                                               d.sc);
         }
         const int wmax = particleWarpsPerBlock(p, sizeof(T));
         const int wpb = (c->tune.particleWarps > 0 && c->tune.particleWarps < wmax)

@@ -291,12 +291,17 @@ int alebgk_residual(alebgk_ctx *ctx, double *res);
 int alebgk_residual_interval(alebgk_ctx *ctx, double *res);
 
 /* Independent cavities on one device advanced in lockstep by one CUDA graph
- * launch per step: each context's whole step and residual is a parallel
- * branch of the graph.  The contexts stay usable on their own between
- * batch calls, as long as they stay in step. */
+ * launch per step, with each context's residual.  The contexts stay usable
+ * on their own between batch calls, as long as they stay in step. */
 typedef struct alebgk_batch alebgk_batch;
 int alebgk_batch_create(int n, alebgk_ctx **ctxs, alebgk_batch **out);
 int alebgk_batch_step(alebgk_batch *b, int nsteps);
+/* mode 0 (default): one launch per step stage over all contexts when they
+ * share precision and Chu layers and run the plain kernels, else mode 1;
+ * mode 1: every context's own step as a branch of one graph.  staged reports
+ * which form the captured graphs hold (1 stage launches, 0 branches). */
+int alebgk_batch_set_mode(alebgk_batch *b, int mode);
+int alebgk_batch_get_mode(alebgk_batch *b, int *mode, int *staged);
 int alebgk_batch_residuals(alebgk_batch *b, double *out);   /* n residuals */
 int alebgk_batch_sync(alebgk_batch *b);
 int alebgk_batch_destroy(alebgk_batch *b);

@@ -95,3 +95,37 @@ def test_uneven_batch_with_smallest_rows_last(gpu):
         np.testing.assert_array_equal(s.cudaDownloadFull()[0], a.solvers[0].cudaDownloadFull()[0])
         a.close()
     b.close()
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+def test_stage_launches_equal_each_cavity_alone(gpu, precision):
+    """Uneven 2-D cavities of the batched workload advanced by one launch per
+    stage over the whole batch: every cavity's distribution, macros and
+    residual are bitwise those of its own step, and the same as the graph of
+    per-cavity branches."""
+    specs = batched_cavity2d(5, seed=7)
+    b = BatchSolver(specs, precision=precision)
+    br = BatchSolver(specs, precision=precision, launch="branches")
+    b.step(6)
+    br.step(6)
+    assert b.staged and not br.staged
+    res, res_br = b.residuals(), br.residuals()
+    for i, sp in enumerate(specs):
+        g0, m0, r0 = _alone(sp, precision, 6)
+        g1, m1 = b.solvers[i].cudaDownloadFull()
+        g2, m2 = br.solvers[i].cudaDownloadFull()
+        np.testing.assert_array_equal(g1, g0)
+        np.testing.assert_array_equal(m1, m0)
+        np.testing.assert_array_equal(g2, g0)
+        assert res[i] == r0 and res_br[i] == r0
+    b.close()
+    br.close()
+
+
+def test_mixed_batch_falls_back_to_branches(gpu):
+    """2-D and 3-D cavities (one and two Chu layers) cannot share stage
+    launches; the batch uses per-cavity branches."""
+    b = BatchSolver(SPECS, precision=32)
+    b.step(1)
+    assert not b.staged
+    b.close()
