@@ -108,6 +108,9 @@ SIGNATURES = {
     "alebgk_batch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "alebgk_batch_set_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "alebgk_batch_get_mode": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p]),
+    "alebgk_batch_set_groups": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "alebgk_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                             ctypes.POINTER(ctypes.c_float)]),
     "alebgk_batch_residuals": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
     "alebgk_batch_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "alebgk_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),

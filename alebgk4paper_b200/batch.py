@@ -111,15 +111,32 @@ class BatchSolver:
         self.steps = 0
         _check(self.lib.alebgk_batch_set_mode(self.h, 0 if launch == "stages" else 1),
                self.solvers[0].ctx)
+        self.batch_tuned_ms = None
+        if autotune:
+            self.batch_tuned_ms = self.autotune(tune_steps)
+
+    def autotune(self, steps: int = 3) -> float:
+        """Times the batch's launch forms (stage launches in 1, 2, 4, 8
+        groups; per-cavity branches) and keeps the fastest.  The timed steps
+        are real steps of the batch (every form computes the same states)."""
+        ms = ctypes.c_float()
+        _check(self.lib.alebgk_batch_autotune(self.h, int(steps), ctypes.byref(ms)),
+               self.solvers[0].ctx)
+        forms = 1 + sum(1 for g in (1, 2, 4, 8) if g <= len(self.solvers))
+        self.steps += forms * (int(steps) + 2)
+        return float(ms.value)
 
     @property
-    def staged(self) -> bool:
-        """True when the step graph holds one launch per stage over all
-        cavities (known after the first step)."""
+    def staged(self) -> int:
+        """Stage groups of the step graph (0: per-cavity branches; known
+        after the first step)."""
         mode, staged = ctypes.c_int(), ctypes.c_int()
         _check(self.lib.alebgk_batch_get_mode(self.h, ctypes.byref(mode), ctypes.byref(staged)),
                self.solvers[0].ctx)
-        return bool(staged.value)
+        return int(staged.value)
+
+    def set_groups(self, groups: int):
+        _check(self.lib.alebgk_batch_set_groups(self.h, int(groups)), self.solvers[0].ctx)
 
     @property
     def updates_per_step(self) -> int:

@@ -3,13 +3,17 @@
 //
 // A batch holds contexts on one device that advance in lockstep, one graph
 // launch per step.  When every context has the same precision and Chu
-// layers and runs the plain transport and particle kernels, the graph holds
-// one launch per stage of the step over all contexts (step.cu's batch
-// kernels: a block finds its context from per-stage block offsets), eleven
-// nodes whatever the batch size.  Otherwise one graph per ping-pong parity
-// holds every context's whole step (and its residual) as a parallel branch:
-// a master stream forks to each context's stream and joins them again.
-// Both forms compute each context exactly as its own step does.
+// layers and runs the plain transport and particle kernels, the contexts
+// are split into up to four groups of about equal work, and the graph holds
+// per group one launch per stage of the step over the group's contexts
+// (step.cu's batch kernels: a block finds its context from per-stage block
+// offsets), each group on its own branch: a few dozen nodes whatever the
+// batch size, and the short stages of one group overlap the long ones of
+// another.  Otherwise one graph per ping-pong parity holds every context's
+// whole step (and its residual) as a parallel branch: a master stream forks
+// to each context's stream and joins them again.  Both forms compute each
+// context exactly as its own step does.
+#include <algorithm>
 #include <cuda_runtime.h>
 
 #include <string>
@@ -30,7 +34,10 @@ struct alebgk_batch
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int mode = 0;                         // 0 stage launches when possible, 1 branches
     bool staged = false;                  // the graphs hold stage launches
-    BatchLaunch bl;
+    bool planned = false;                 // the stage groups were tried
+    std::vector<BatchLaunch> groups;      // stage launches per group
+    std::vector<int> groupStream;         // context whose stream runs the group
+    int ngroups = 4;                      // stage groups wanted
     std::string err;
 };
 
@@ -56,6 +63,57 @@ void dropGraphs(alebgk_ctx *c)
         if (g) { cudaGraphExecDestroy(g); g = nullptr; }
 }
 
+void freeGroups(alebgk_batch *b)
+{
+    for (BatchLaunch &bl : b->groups) freeBatchLaunch(bl);
+    b->groups.clear();
+    b->groupStream.clear();
+    b->staged = false;
+    b->planned = false;
+}
+
+// Splits the contexts into groups of about equal work (particles x nodes x
+// layers; largest first onto the lightest group) and builds each group's
+// stage launches.  cudaErrorNotSupported when the contexts cannot share
+// stage launches.
+cudaError_t planGroups(alebgk_batch *b)
+{
+    const int n = (int)b->ctx.size();
+    const int G = std::max(1, std::min(b->ngroups, n));
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    auto cost = [&](int i) {
+        const StepParams &p = b->ctx[i]->sp;
+        return (double)p.N * p.V * p.L;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost(x) > cost(y); });
+    std::vector<std::vector<int>> member(G);
+    std::vector<double> load(G, 0.0);
+    for (int i : order)
+    {
+        const int g = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        member[g].push_back(i);
+        load[g] += cost(i);
+    }
+    b->groups.assign(G, BatchLaunch());
+    for (int g = 0; g < G; ++g)
+    {
+        std::sort(member[g].begin(), member[g].end());
+        std::vector<alebgk_ctx *> cs;
+        std::vector<double *> rs;
+        for (int i : member[g])
+        {
+            cs.push_back(b->ctx[i]);
+            rs.push_back(b->resid + i);
+        }
+        cudaError_t e = buildBatchLaunch(cs.data(), (int)cs.size(), rs.data(), b->groups[g]);
+        if (e == cudaSuccess) e = prepareBatchLaunch(b->groups[g]);
+        if (e != cudaSuccess) return e;
+        b->groupStream.push_back(member[g][0]);
+    }
+    return cudaSuccess;
+}
+
 }  // namespace
 
 extern "C" {
@@ -63,8 +121,11 @@ extern "C" {
 int alebgk_set_launch(alebgk_ctx *c, int transport_threads, int particle_warps)
 {
     if (!c) return ALEBGK_EINVAL;
-    if (transport_threads < 32 || transport_threads > 256 || transport_threads % 32)
-        return failc(c, ALEBGK_EINVAL, "transport threads: a multiple of 32 in 32..256");
+    if (transport_threads != 0 &&
+        (transport_threads < 32 || transport_threads > 256 || transport_threads % 32))
+        return failc(c, ALEBGK_EINVAL,
+                     "transport threads: 0 (fused into the particle kernel) or a multiple of 32 "
+                     "in 32..256");
     if (particle_warps < 0 || particle_warps > 8)
         return failc(c, ALEBGK_EINVAL, "particle warps: 0 (as many as fit) or 1..8");
     if (c->tune.transportThreads != transport_threads || c->tune.particleWarps != particle_warps)
@@ -115,7 +176,7 @@ int alebgk_autotune(alebgk_ctx *c, int steps, float *best_ms)
         if (r == cudaSuccess) r = cudaMemcpy(c->d.sc, snapSc, sizeof(StepScalars), cudaMemcpyDeviceToDevice);
         return r;
     };
-    const int tts[] = {64, 128, 256};
+    const int tts[] = {0, 64, 128, 256};
     const int pws[] = {1, 2, 4, 0};
     float best = -1.0f;
     int bestT = c->tune.transportThreads, bestW = c->tune.particleWarps;
@@ -238,25 +299,30 @@ int alebgk_batch_step(alebgk_batch *b, int nsteps)
     for (int n = 0; n < nsteps; ++n)
     {
         const int from = c->cur;
-        if (!b->graph[from] && !b->graph[1 - from] && b->mode == 0 && !b->bl.desc[0])
+        if (b->mode == 0 && !b->planned)
         {
-            const cudaError_t be = buildBatchLaunch(b->ctx.data(), (int)b->ctx.size(), b->resid,
-                                                    b->bl);
-            if (be == cudaSuccess) CKC(prepareBatchLaunch(b->bl));
-            else if (be == cudaErrorNotSupported) freeBatchLaunch(b->bl);
-            else
+            const cudaError_t be = planGroups(b);
+            if (be != cudaSuccess)
             {
-                freeBatchLaunch(b->bl);
-                CKC(be);
+                freeGroups(b);
+                if (be != cudaErrorNotSupported) CKC(be);
             }
-            b->staged = b->bl.desc[0] != nullptr;
+            else b->staged = true;
+            b->planned = true;
         }
         if (!b->graph[from])
         {
             cudaGraph_t g = nullptr;
             CKC(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
-            cudaError_t le = b->staged ? launchBatchStep(b->bl, from, b->master)
-                                       : cudaEventRecord(b->fork, b->master);
+            cudaError_t le = cudaEventRecord(b->fork, b->master);
+            for (size_t q = 0; q < b->groups.size() && le == cudaSuccess && b->staged; ++q)
+            {
+                cudaStream_t gs = b->ctx[b->groupStream[q]]->stream;
+                le = cudaStreamWaitEvent(gs, b->fork, 0);
+                if (le == cudaSuccess) le = launchBatchStep(b->groups[q], from, gs);
+                if (le == cudaSuccess) le = cudaEventRecord(b->join[q], gs);
+                if (le == cudaSuccess) le = cudaStreamWaitEvent(b->master, b->join[q], 0);
+            }
             for (size_t i = 0; i < b->ctx.size() && le == cudaSuccess && !b->staged; ++i)
             {
                 alebgk_ctx *x = b->ctx[i];
@@ -305,8 +371,7 @@ int alebgk_batch_set_mode(alebgk_batch *b, int mode)
         cudaStreamSynchronize(b->master);
         for (auto &g : b->graph)
             if (g) { cudaGraphExecDestroy(g); g = nullptr; }
-        freeBatchLaunch(b->bl);
-        b->staged = false;
+        freeGroups(b);
         b->mode = mode;
     }
     return ALEBGK_OK;
@@ -316,8 +381,74 @@ int alebgk_batch_get_mode(alebgk_batch *b, int *mode, int *staged)
 {
     if (!b || !mode || !staged) return ALEBGK_EINVAL;
     *mode = b->mode;
-    *staged = b->staged ? 1 : 0;
+    *staged = b->staged ? (int)b->groups.size() : 0;
     return ALEBGK_OK;
+}
+
+int alebgk_batch_set_groups(alebgk_batch *b, int groups)
+{
+    if (!b || groups < 1 || groups > 64) return ALEBGK_EINVAL;
+    if (groups != b->ngroups)
+    {
+        cudaSetDevice(b->device);
+        cudaStreamSynchronize(b->master);
+        for (auto &g : b->graph)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        freeGroups(b);
+        b->ngroups = groups;
+    }
+    return ALEBGK_OK;
+}
+
+int alebgk_batch_autotune(alebgk_batch *b, int steps, float *best_ms)
+{
+    if (!b || steps < 1) return ALEBGK_EINVAL;
+    alebgk_ctx *c = b->ctx[0];
+    CKC(cudaSetDevice(b->device));
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    CKC(cudaEventCreate(&t0));
+    CKC(cudaEventCreate(&t1));
+    // candidates: stage launches in 1, 2, 4, 8 groups, then branches
+    struct Cand { int mode, groups; };
+    std::vector<Cand> cands;
+    for (int g : {1, 2, 4, 8})
+        if (g <= (int)b->ctx.size()) cands.push_back({0, g});
+    cands.push_back({1, b->ngroups});
+    float best = -1.0f;
+    Cand pick = {b->mode, b->ngroups};
+    int rc = ALEBGK_OK;
+    for (const Cand &cd : cands)
+    {
+        rc = alebgk_batch_set_mode(b, cd.mode);
+        if (rc == ALEBGK_OK) rc = alebgk_batch_set_groups(b, cd.groups);
+        if (rc == ALEBGK_OK) rc = alebgk_batch_step(b, 2);     // captures both graphs
+        if (rc != ALEBGK_OK) break;
+        // (contexts that cannot share stage launches run as branches here)
+        float ms = 0.0f;
+        cudaError_t e = cudaEventRecord(t0, b->master);
+        if (e == cudaSuccess) rc = alebgk_batch_step(b, steps);
+        if (rc != ALEBGK_OK) break;
+        if (e == cudaSuccess) e = cudaEventRecord(t1, b->master);
+        if (e == cudaSuccess) e = cudaEventSynchronize(t1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, t0, t1);
+        if (e != cudaSuccess)
+        {
+            rc = failc(c, ALEBGK_ECUDA, std::string("batch autotune: ") + cudaGetErrorString(e));
+            break;
+        }
+        if (best < 0 || ms < best)
+        {
+            best = ms;
+            pick = cd;
+        }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (rc != ALEBGK_OK) return rc;
+    rc = alebgk_batch_set_mode(b, pick.mode);
+    if (rc == ALEBGK_OK) rc = alebgk_batch_set_groups(b, pick.groups);
+    if (best_ms) *best_ms = best / steps;
+    return rc;
 }
 
 int alebgk_batch_residuals(alebgk_batch *b, double *out)
@@ -346,7 +477,7 @@ int alebgk_batch_destroy(alebgk_batch *b)
     if (b->master) cudaStreamSynchronize(b->master);
     for (auto &g : b->graph)
         if (g) cudaGraphExecDestroy(g);
-    freeBatchLaunch(b->bl);
+    freeGroups(b);
     for (auto &e : b->join)
         if (e) cudaEventDestroy(e);
     if (b->fork) cudaEventDestroy(b->fork);

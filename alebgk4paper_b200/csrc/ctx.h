@@ -111,7 +111,7 @@ struct alebgk_ctx
     // Launch shapes of the general kernels (alebgk_set_launch / autotune).
     struct
     {
-        int transportThreads = 256;   // coefficient-gather transport, per block
+        int transportThreads = 0;     // coefficient-gather transport per block; 0 fused
         int particleWarps = 0;        // warp-per-particle kernel; 0 = as many as fit
     } tune;
     // Streamed particle kernel: on, warps per block, blocks, dynamic smem.
@@ -150,7 +150,8 @@ struct BatchLaunch
 };
 // cudaErrorNotSupported when the clouds cannot share launches (mixed
 // precision or layers, the streamed particle kernel or the lattice march).
-cudaError_t buildBatchLaunch(alebgk_ctx *const *cs, int n, double *resid, BatchLaunch &bl);
+cudaError_t buildBatchLaunch(alebgk_ctx *const *cs, int n, double *const *resid,
+                             BatchLaunch &bl);
 cudaError_t prepareBatchLaunch(const BatchLaunch &bl);
 cudaError_t launchBatchStep(const BatchLaunch &bl, int from, cudaStream_t st);
 void freeBatchLaunch(BatchLaunch &bl);

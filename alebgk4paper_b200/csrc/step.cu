@@ -104,50 +104,119 @@ __device__ __forceinline__ double minImage(double d, double L)
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// Transport: coefficient gather.  Thread = (particle, node); the node's
-// coefficients are shared by both Chu layers in 2-D.  The output is scaled
-// by the stored-state scale so that gt carries the true magnitude.
+// Transport: coefficient gather.  Warp = one particle and one chunk of its
+// velocity nodes; lane = nodes k = k0 + lane + 32 q for q < qn <= kTransportQ,
+// so one slot's row index and coefficient row serve qn nodes per lane and
+// qn (or 2 qn in 2-D) independent loads are in flight per slot.  The node's
+// coefficients are shared by both Chu layers in 2-D.  Every node sums its
+// slots in slot order, whatever the chunking.  The output is scaled by the
+// stored-state scale so that gt carries the true magnitude.
 // ---------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ void transportNode(const T *__restrict__ f, T *__restrict__ g,
-            const T *__restrict__ coef, const int *__restrict__ cls,
-            const int *__restrict__ nslot, const int *__restrict__ slots,
-            int S, int V, int L, int ldf, const StepScalars *__restrict__ sc, int i, int k)
+constexpr int kTransportQ = 8;
+
+// Chunks of a row: the 32-node groups of V split as evenly as possible into
+// chunks of at most kTransportQ groups.
+__host__ __device__ __forceinline__ int transportChunks(int V)
 {
-    const T scale = T(sc->scale);
-    const int c = cls[i], ns = nslot[i];
-    const T *cc = coef + (size_t)c * S * V + k;
-    const int *sl = slots + (size_t)i * S;
-    T a0 = T(0), a1 = T(0);
-    if (L == 2)
+    const int groups = (V + 31) / 32;
+    return (groups + kTransportQ - 1) / kTransportQ;
+}
+
+// Accumulates the slots of one chunk of a row: nodes k0 + 32 q for q < qn
+// (k0 = first node of the chunk + lane), both Chu layers when L = 2.
+template <typename T, int L>
+__device__ __forceinline__ void gatherChunk(const T *__restrict__ f, const T *__restrict__ cc,
+                                            const int *__restrict__ sl, int ns, int V, int ldf,
+                                            int k0, int qn, T (&a0)[kTransportQ],
+                                            T (&a1)[kTransportQ])
+{
+#pragma unroll
+    for (int q = 0; q < kTransportQ; ++q) { a0[q] = T(0); a1[q] = T(0); }
+    // the lanes past V in the last group neither load nor store
+    const bool tail = k0 + 32 * (qn - 1) >= V;
+    for (int s = 0; s < ns; ++s)
     {
-        for (int s = 0; s < ns; ++s)
+        const T *cs = cc + (size_t)s * V;
+        const T *fr = f + (size_t)__ldg(sl + s) * ldf + k0;
+#pragma unroll
+        for (int q = 0; q < kTransportQ; ++q)
         {
-            const T cs = __ldg(cc + (size_t)s * V);
-            const T *fr = f + (size_t)__ldg(sl + s) * ldf + k;
-            a0 = fma(cs, __ldg(fr), a0);
-            a1 = fma(cs, __ldg(fr + V), a1);
+            if (q < qn && (!tail || k0 + 32 * q < V))
+            {
+                const T w = __ldg(cs + 32 * q);
+                a0[q] = fma(w, __ldg(fr + 32 * q), a0[q]);
+                if (L == 2) a1[q] = fma(w, __ldg(fr + V + 32 * q), a1[q]);
+            }
         }
-        g[(size_t)i * ldf + k] = a0 * scale;
-        g[(size_t)i * ldf + V + k] = a1 * scale;
-    }
-    else
-    {
-        for (int s = 0; s < ns; ++s)
-        {
-            const T cs = __ldg(cc + (size_t)s * V);
-            a0 = fma(cs, __ldg(f + (size_t)__ldg(sl + s) * ldf + k), a0);
-        }
-        g[(size_t)i * ldf + k] = a0 * scale;
     }
 }
 
-// Tile = 2 particles per warp of consecutive particles x 32 velocities (one
-// per lane).  The particles of a tile share most of their neighbours, so the
-// tile's gathers of neighbour rows hit L1 after the first; the velocity
-// chunks of a tile are consecutive blocks and meet the same rows in L2.
-constexpr int kTransportPPW = 2;
+// One chunk of particle i's transported row, stored to out = row of g.
+template <typename T, int L>
+__device__ __forceinline__ void transportRow(const T *__restrict__ f, T *__restrict__ g,
+            const T *__restrict__ coef, const int *__restrict__ cls,
+            const int *__restrict__ nslot, const int *__restrict__ slots,
+            int S, int V, int ldf, T scale, int i, int chunk, int nch, int lane)
+{
+    const int groups = (V + 31) / 32;
+    const int per = (groups + nch - 1) / nch;
+    const int g0 = chunk * per;
+    const int qn = min(per, groups - g0);        // warp-uniform
+    if (qn <= 0) return;
+    const int k0 = g0 * 32 + lane;
+    const int c = __ldg(cls + i), ns = __ldg(nslot + i);
+    T a0[kTransportQ], a1[kTransportQ];
+    gatherChunk<T, L>(f, coef + (size_t)c * S * V + k0, slots + (size_t)i * S, ns, V, ldf, k0,
+                      qn, a0, a1);
+    T *out = g + (size_t)i * ldf + k0;
+#pragma unroll
+    for (int q = 0; q < kTransportQ; ++q)
+    {
+        if (q < qn && k0 + 32 * q < V)
+        {
+            out[32 * q] = a0[q] * scale;
+            if (L == 2) out[V + 32 * q] = a1[q] * scale;
+        }
+    }
+}
 
+// Particle i's whole transported row into a warp's shared-memory row copy
+// (the fused transport of the particle kernel): the same sums as
+// transportRow, chunk by chunk.
+template <typename T, int L>
+__device__ __forceinline__ void transportRowShared(const T *__restrict__ f, T *__restrict__ buf,
+            const T *__restrict__ coef, const int *__restrict__ cls,
+            const int *__restrict__ nslot, const int *__restrict__ slots,
+            int S, int V, int ldf, T scale, int i, int lane)
+{
+    const int groups = (V + 31) / 32;
+    const int nch = transportChunks(V);
+    const int per = (groups + nch - 1) / nch;
+    const int c = __ldg(cls + i), ns = __ldg(nslot + i);
+    const T *cc = coef + (size_t)c * S * V;
+    const int *sl = slots + (size_t)i * S;
+    for (int g0 = 0; g0 < groups; g0 += per)
+    {
+        const int qn = min(per, groups - g0);
+        const int k0 = g0 * 32 + lane;
+        T a0[kTransportQ], a1[kTransportQ];
+        gatherChunk<T, L>(f, cc + k0, sl, ns, V, ldf, k0, qn, a0, a1);
+#pragma unroll
+        for (int q = 0; q < kTransportQ; ++q)
+        {
+            if (q < qn && k0 + 32 * q < V)
+            {
+                buf[k0 + 32 * q] = a0[q] * scale;
+                if (L == 2) buf[V + k0 + 32 * q] = a1[q] * scale;
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// Block = consecutive particles, one per warp, at one velocity chunk: the
+// particles share most of their neighbours, so the block's gathers of
+// neighbour rows hit L1 after the first.
 template <typename T>
 __device__ __forceinline__ void k_transport_body(const T *__restrict__ f, T *__restrict__ g,
             const T *__restrict__ coef, const int *__restrict__ cls,
@@ -156,18 +225,19 @@ __device__ __forceinline__ void k_transport_body(const T *__restrict__ f, T *__r
             int tile)
 {
     const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int k = chunk * 32 + (threadIdx.x & 31);
-    if (k >= V) return;
-    const int i0 = tile * nw * kTransportPPW;
-    for (int j = warp; j < nw * kTransportPPW; j += nw)
-    {
-        const int i = i0 + j;
-        if (i >= N) break;
-        transportNode(f, g, coef, cls, nslot, slots, S, V, L, ldf, sc, i, k);
-    }
+    const int i = tile * nw + warp;
+    if (i >= N) return;
+    const T scale = T(sc->scale);
+    const int nch = transportChunks(V);
+    if (L == 2)
+        transportRow<T, 2>(f, g, coef, cls, nslot, slots, S, V, ldf, scale, i, chunk, nch,
+                           threadIdx.x & 31);
+    else
+        transportRow<T, 1>(f, g, coef, cls, nslot, slots, S, V, ldf, scale, i, chunk, nch,
+                           threadIdx.x & 31);
 }
 
-// Grid (velocity chunks of 32, particle tiles).
+// Grid (velocity chunks, particle tiles of blockDim.x / 32).
 template <typename T>
 __global__ void __launch_bounds__(kNT)
 k_transport(const T *__restrict__ f, T *__restrict__ g,
@@ -250,6 +320,7 @@ struct ParticleArgs
 {
     T *g;                     // in: gt (true scale); out: h (unscaled by sigma)
     const T *fold;            // previous stored h (scale sc->scale)
+    const T *coef;            // MLS tables (the fused transport)
     const T *coefLin;         // linear MLS tables (MOOD redo)
     const int *boundary, *cls, *nslot, *slots;
     const double *wall, *macPrev;
@@ -326,9 +397,12 @@ __device__ __forceinline__ void regSigns(RowRegs<T, L> &r, const StepParams &p,
 // its previous (absolute) macros, which breaks homogeneity, so the particle
 // is left untouched, listed, and finished by k_fixup once sigma is known.
 // Maxwellians are evaluated as products of per-axis exponentials.
+// With flushDeferred the row of a deferred particle is written back first
+// (its staged copy was never in g: the fused transport built it in place).
 template <typename T, int L>
 __device__ void finishParticle(const ParticleArgs<T> &a, const StepParams &p, int i,
-                               RowRegs<T, L> &r, const Positivity &pv, double (*tb)[kMaxNv])
+                               RowRegs<T, L> &r, const Positivity &pv, double (*tb)[kMaxNv],
+                               bool flushDeferred = false)
 {
     const int lane = r.lane;
     const int Nv = p.Nv, dim = p.dim;
@@ -408,6 +482,7 @@ __device__ void finishParticle(const ParticleArgs<T> &a, const StepParams &p, in
         // No positive mass (macros kept from the previous step), or a
         // relaxation time tau(rho, T) that is not homogeneous in rho: the
         // particle is finished on true magnitudes once sigma is known.
+        if (flushDeferred) r.flush();
         if (lane == 0) a.degList[atomicAdd(&a.sc->ndeg, 1)] = i;
         return;
     }
@@ -496,9 +571,13 @@ __device__ int screen(const ParticleArgs<T> &a, const StepParams &p, int i, int 
 
 // ---------------------------------------------------------------------------
 // Positivity + MOOD screen + finish, one warp per particle.  A particle the
-// screen flags is listed for k_redo and left as is.
+// screen flags is listed for k_redo and left as is.  Fused: the warp first
+// builds the particle's transported row in its shared-memory copy
+// (transportRowShared, the sums of k_transport) instead of loading it from
+// g; a flagged particle's row is then not stored (k_redo rebuilds it), a
+// deferred one's is.
 // ---------------------------------------------------------------------------
-template <typename T, int L>
+template <typename T, int L, bool Fused = false>
 __device__ __forceinline__ void k_particle_body(const ParticleArgs<T> &a, const StepParams &p,
                                                 int warpsPerBlock, int bx)
 {
@@ -509,7 +588,11 @@ __device__ __forceinline__ void k_particle_body(const ParticleArgs<T> &a, const 
     const int i = bx * warpsPerBlock + warp;
     if (i >= p.N) return;                        // warp-uniform
     T *buf = reinterpret_cast<T *>(rowSmem) + (size_t)warp * L * p.V;
-    RowRegs<T, L> r(a.g + (size_t)i * p.ldf, buf, p, lane);
+    if (Fused)
+        transportRowShared<T, L>(a.fold, buf, a.coef, a.cls, a.nslot, a.slots, p.S, p.V, p.ldf,
+                                 T(a.sc->scale), i, lane);
+    RowRegs<T, L> r = Fused ? RowRegs<T, L>(a.g + (size_t)i * p.ldf, buf, p, lane, true)
+                            : RowRegs<T, L>(a.g + (size_t)i * p.ldf, buf, p, lane);
     double pos, neg;
     bool bad;
     regSigns(r, p, pos, neg, bad);
@@ -524,14 +607,14 @@ __device__ __forceinline__ void k_particle_body(const ParticleArgs<T> &a, const 
         else a.massPos[i] = m * p.dvN;
     }
     if (flagged) return;
-    finishParticle(a, p, i, r, pv, tab[warp]);
+    finishParticle(a, p, i, r, pv, tab[warp], Fused);
 }
 
-template <typename T, int L>
+template <typename T, int L, bool Fused>
 __global__ void __launch_bounds__(kNT)
 k_particle(ParticleArgs<T> a, StepParams p, int warpsPerBlock)
 {
-    k_particle_body<T, L>(a, p, warpsPerBlock, blockIdx.x);
+    k_particle_body<T, L, Fused>(a, p, warpsPerBlock, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1668,6 +1751,7 @@ static cudaError_t stepT(alebgk_ctx *c, int from, cudaEvent_t *ev)
     double *macA = d.macro[from], *macB = d.macro[1 - from];
     ParticleArgs<T> pa;
     pa.g = fb; pa.fold = fa; pa.coefLin = static_cast<const T *>(d.coefLin);
+    pa.coef = static_cast<const T *>(d.coef);
     pa.boundary = d.boundary; pa.cls = d.cls; pa.nslot = d.nslot; pa.slots = d.slots;
     pa.wall = d.wall; pa.macPrev = macA; pa.macNew = macB;
     pa.massPos = d.massPos; pa.massEnd = d.massEnd; pa.minG = d.minG; pa.dpx = d.dpx;
@@ -1698,16 +1782,20 @@ static cudaError_t stepT(alebgk_ctx *c, int from, cudaEvent_t *ev)
         k_step_begin<<<nadOn ? nadBlocks : 1, kNT, 0, st>>>(
             d.sc, 1, macA, d.boundary, d.nslot, d.slots, p.S, p.N, nadOn ? d.nad : nullptr);
     mark();
-    if (sizeof(T) == 4 && c->march.enabled)
+    const bool march = sizeof(T) == 4 && c->march.enabled;
+    // Transport fused into the particle kernel (transport threads 0), except
+    // when stages are timed: then it runs as its own kernel, with the same
+    // sums, so that its time is seen.
+    const bool fused = !march && !c->pStream && c->tune.transportThreads == 0 && !ev;
+    if (march)
     {
         cudaError_t e = launchMarch(c, from, reinterpret_cast<float *>(fb), st);
         if (e != cudaSuccess) return e;
     }
-    else
+    else if (!fused)
     {
-        const int tt = c->tune.transportThreads;
-        const int tileP = (tt / 32) * kTransportPPW;
-        dim3 gt((p.V + 31) / 32, (p.N + tileP - 1) / tileP);
+        const int tt = c->tune.transportThreads > 0 ? c->tune.transportThreads : kNT;
+        dim3 gt(transportChunks(p.V), (p.N + tt / 32 - 1) / (tt / 32));
         k_transport<T><<<gt, tt, 0, st>>>(fa, fb, static_cast<const T *>(d.coef),
                                            d.cls, d.nslot, d.slots, p.S, p.N, p.V, p.L,
                                            p.ldf, d.sc);
@@ -1722,8 +1810,13 @@ static cudaError_t stepT(alebgk_ctx *c, int from, cudaEvent_t *ev)
     if (c->pStream)
         k_particle_stream<T><<<c->pStreamBlocks, kNT, c->pStreamSmem, st>>>(pa, p,
                                                                           c->pStreamWpb);
-    else if (p.L == 2) k_particle<T, 2><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
-    else k_particle<T, 1><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
+    else if (fused)
+    {
+        if (p.L == 2) k_particle<T, 2, true><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
+        else k_particle<T, 1, true><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
+    }
+    else if (p.L == 2) k_particle<T, 2, false><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
+    else k_particle<T, 1, false><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
     mark();
     if (p.L == 2) k_redo<T, 2><<<listBlocks, kNT, rowBytes, st>>>(pa, p);
     else k_redo<T, 1><<<listBlocks, kNT, rowBytes, st>>>(pa, p);
@@ -1768,8 +1861,10 @@ static cudaError_t prepareT(alebgk_ctx *c)
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
     };
-    set((const void *)k_particle<T, 1>, wpb * rowBytes);
-    set((const void *)k_particle<T, 2>, wpb * rowBytes);
+    set((const void *)k_particle<T, 1, false>, wpb * rowBytes);
+    set((const void *)k_particle<T, 2, false>, wpb * rowBytes);
+    set((const void *)k_particle<T, 1, true>, wpb * rowBytes);
+    set((const void *)k_particle<T, 2, true>, wpb * rowBytes);
     set((const void *)k_redo<T, 1>, rowBytes);
     set((const void *)k_redo<T, 2>, rowBytes);
 
@@ -1836,7 +1931,7 @@ struct BatchCtx
 
 constexpr int kBatchStages = 11;
 constexpr int kBatchTT = 256;  // transport threads per block in a batch
-constexpr int kBatchTile = (kBatchTT / 32) * kTransportPPW;
+constexpr int kBatchTile = kBatchTT / 32;      // particles per transport block
 
 __device__ __forceinline__ int batchCtxOf(const int *__restrict__ off, int n, int b)
 {
@@ -1896,17 +1991,17 @@ k_batch_transport(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ o
 {
     BATCH_CTX(1);
     const StepParams &p = B.p;
-    const int chunks = (p.V + 31) / 32;
+    const int chunks = transportChunks(p.V);
     k_transport_body<T>(B.pa.fold, B.pa.g, B.coef, B.pa.cls, B.pa.nslot, B.pa.slots, p.S, p.N,
                         p.V, p.L, p.ldf, B.pa.sc, vb % chunks, vb / chunks);
 }
 
 template <typename T, int L>
-__global__ void __launch_bounds__(kNT, 4)
+__global__ void __launch_bounds__(kNT)
 k_batch_particle(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ off, int n)
 {
     BATCH_CTX(2);
-    k_particle_body<T, L>(B.pa, B.p, B.wpb, vb);
+    k_particle_body<T, L, true>(B.pa, B.p, B.wpb, vb);
 }
 
 template <typename T, int L>
@@ -1998,7 +2093,8 @@ k_batch_residual(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ of
 #undef BATCH_CTX
 
 template <typename T>
-static cudaError_t buildBatchT(alebgk_ctx *const *cs, int n, double *resid, BatchLaunch &bl)
+static cudaError_t buildBatchT(alebgk_ctx *const *cs, int n, double *const *resid,
+                               BatchLaunch &bl)
 {
     const int L = cs[0]->sp.L;
     std::vector<BatchCtx<T>> h[2];
@@ -2016,16 +2112,19 @@ static cudaError_t buildBatchT(alebgk_ctx *const *cs, int n, double *resid, Batc
         smemP = std::max(smemP, wpb * rowBytes);
         smemR = std::max(smemR, rowBytes);
         const int pBlocks = (p.N + kNT / 32 - 1) / (kNT / 32);
+        // the transport runs fused in the particle stage (stage 1 is empty)
         const int blocks[kBatchStages] = {1,
-                                          ((p.V + 31) / 32) *
-                                              ((p.N + kBatchTile - 1) / kBatchTile),
+                                          0,
                                           (p.N + wpb - 1) / wpb,
-                                          std::min(p.N, 296),
+                                          // the list stages mostly find empty
+                                          // lists: few blocks per cloud (any
+                                          // count gives the same results)
+                                          std::min(p.N, 32),
                                           kRedBlocks,
-                                          std::min(pBlocks, 296),
+                                          std::min(pBlocks, 16),
                                           kRedBlocks,
                                           (p.N + 255) / 256,
-                                          p.limiter == 2 ? std::min(pBlocks, 592) : 0,
+                                          p.limiter == 2 ? std::min(pBlocks, 64) : 0,
                                           p.limiter == 2 ? kRedBlocks : 0,
                                           1};
         for (int s = 0; s < kBatchStages; ++s)
@@ -2037,6 +2136,7 @@ static cudaError_t buildBatchT(alebgk_ctx *const *cs, int n, double *resid, Batc
             pa.g = static_cast<T *>(d.f[1 - from]);
             pa.fold = static_cast<const T *>(d.f[from]);
             pa.coefLin = static_cast<const T *>(d.coefLin);
+            pa.coef = static_cast<const T *>(d.coef);
             pa.boundary = d.boundary; pa.cls = d.cls; pa.nslot = d.nslot; pa.slots = d.slots;
             pa.wall = d.wall; pa.macPrev = d.macro[from]; pa.macNew = d.macro[1 - from];
             pa.massPos = d.massPos; pa.massEnd = d.massEnd; pa.minG = d.minG; pa.dpx = d.dpx;
@@ -2046,7 +2146,7 @@ static cudaError_t buildBatchT(alebgk_ctx *const *cs, int n, double *resid, Batc
             b.mood = d.mood;
             b.coef = static_cast<const T *>(d.coef);
             b.redPartial = d.redPartial;
-            b.resid = resid + i;
+            b.resid = resid[i];
             b.wpb = wpb;
             h[from].push_back(b);
         }
@@ -2070,7 +2170,8 @@ static cudaError_t buildBatchT(alebgk_ctx *const *cs, int n, double *resid, Batc
     return e;
 }
 
-cudaError_t buildBatchLaunch(alebgk_ctx *const *cs, int n, double *resid, BatchLaunch &bl)
+cudaError_t buildBatchLaunch(alebgk_ctx *const *cs, int n, double *const *resid,
+                             BatchLaunch &bl)
 {
     bl = BatchLaunch();
     if (n < 1) return cudaErrorInvalidValue;
@@ -2171,6 +2272,7 @@ static cudaError_t slabSegT(alebgk_ctx *c, int from, int seg, cudaStream_t st)
     double *macA = d.macro[from], *macB = d.macro[1 - from];
     ParticleArgs<T> pa;
     pa.g = fb; pa.fold = fa; pa.coefLin = static_cast<const T *>(d.coefLin);
+    pa.coef = static_cast<const T *>(d.coef);
     pa.boundary = d.boundary; pa.cls = d.cls; pa.nslot = d.nslot; pa.slots = d.slots;
     pa.wall = d.wall; pa.macPrev = macA; pa.macNew = macB;
     pa.massPos = d.massPos; pa.massEnd = d.massEnd; pa.minG = d.minG; pa.dpx = d.dpx;
@@ -2186,16 +2288,17 @@ static cudaError_t slabSegT(alebgk_ctx *c, int from, int seg, cudaStream_t st)
         const int nadBlocks = min((p.N + kNT / 32 - 1) / (kNT / 32), 1184);
         k_step_begin<<<nadOn ? nadBlocks : 1, kNT, 0, st>>>(
             d.sc, 1, macA, d.boundary, d.nslot, d.slots, p.S, p.N, nadOn ? d.nad : nullptr);
-        if (sizeof(T) == 4 && c->march.enabled)
+        const bool march = sizeof(T) == 4 && c->march.enabled;
+        const bool fused = !march && !c->pStream && c->tune.transportThreads == 0;
+        if (march)
         {
             cudaError_t e = launchMarch(c, from, reinterpret_cast<float *>(fb), st);
             if (e != cudaSuccess) return e;
         }
-        else
+        else if (!fused)
         {
-            const int tt = c->tune.transportThreads;
-            const int tileP = (tt / 32) * kTransportPPW;
-            dim3 gt((p.V + 31) / 32, (p.N + tileP - 1) / tileP);
+            const int tt = c->tune.transportThreads > 0 ? c->tune.transportThreads : kNT;
+            dim3 gt(transportChunks(p.V), (p.N + tt / 32 - 1) / (tt / 32));
             k_transport<T><<<gt, tt, 0, st>>>(fa, fb, static_cast<const T *>(d.coef), d.cls,
                                                d.nslot, d.slots, p.S, p.N, p.V, p.L, p.ldf,
                                                d.sc);
@@ -2207,8 +2310,12 @@ static cudaError_t slabSegT(alebgk_ctx *c, int from, int seg, cudaStream_t st)
         if (c->pStream)
             k_particle_stream<T><<<c->pStreamBlocks, kNT, c->pStreamSmem, st>>>(
                 pa, p, c->pStreamWpb);
-        else if (p.L == 2) k_particle<T, 2><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
-        else k_particle<T, 1><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
+        else if (fused && p.L == 2)
+            k_particle<T, 2, true><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
+        else if (fused) k_particle<T, 1, true><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
+        else if (p.L == 2)
+            k_particle<T, 2, false><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
+        else k_particle<T, 1, false><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
         if (p.L == 2) k_redo<T, 2><<<listBlocks, kNT, rowBytes, st>>>(pa, p);
         else k_redo<T, 1><<<listBlocks, kNT, rowBytes, st>>>(pa, p);
         k_sum_range<<<kRedBlocks, kRedThreads, 0, st>>>(d.massPos + lo, n, d.redPartial, d.sc,

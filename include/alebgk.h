@@ -265,7 +265,9 @@ int alebgk_body_set_surface_velocity(alebgk_ctx *ctx, int nbodies,
  * No reference counterpart: the reference runs one cavity per process. */
 
 /* Launch shapes of the general kernels: threads per block of the
- * coefficient-gather transport (a multiple of 32 in 32..256) and particles
+ * coefficient-gather transport (a multiple of 32 in 32..256, or 0: the
+ * transport runs inside the particle kernel, each warp building its
+ * particle's row in shared memory; same sums, same results) and particles
  * (warps) per block of the warp-per-particle kernel (1..8; 0 = as many as
  * their shared-memory rows allow).  The lattice march and the streamed
  * particle kernel have fixed shapes.  Drops the captured step graphs. */
@@ -296,12 +298,24 @@ int alebgk_residual_interval(alebgk_ctx *ctx, double *res);
 typedef struct alebgk_batch alebgk_batch;
 int alebgk_batch_create(int n, alebgk_ctx **ctxs, alebgk_batch **out);
 int alebgk_batch_step(alebgk_batch *b, int nsteps);
-/* mode 0 (default): one launch per step stage over all contexts when they
- * share precision and Chu layers and run the plain kernels, else mode 1;
- * mode 1: every context's own step as a branch of one graph.  staged reports
- * which form the captured graphs hold (1 stage launches, 0 branches). */
+/* mode 0 (default): the contexts split into groups of about equal work,
+ * each group stepped by one launch per step stage over its contexts (the
+ * groups are parallel branches of the graph), when the contexts share
+ * precision and Chu layers and run the plain kernels; else mode 1.
+ * mode 1: every context's own step as a branch of one graph.  staged
+ * reports the form the captured graphs hold (the number of stage groups,
+ * 0 for per-context branches).  set_groups sets the stage groups wanted
+ * (default 4).  All forms give every context exactly the state of its own
+ * steps. */
 int alebgk_batch_set_mode(alebgk_batch *b, int mode);
 int alebgk_batch_get_mode(alebgk_batch *b, int *mode, int *staged);
+int alebgk_batch_set_groups(alebgk_batch *b, int groups);
+/* Times `steps` steps of each form (stage launches in 1, 2, 4 and 8
+ * groups, per-context branches) and keeps the fastest; *best_ms = its time
+ * per step.  The timed steps are real steps: the batch advances by
+ * (steps + 2) per form tried, (forms = 1 + the group counts in 1, 2, 4, 8
+ * not above the number of contexts). */
+int alebgk_batch_autotune(alebgk_batch *b, int steps, float *best_ms);
 int alebgk_batch_residuals(alebgk_batch *b, double *out);   /* n residuals */
 int alebgk_batch_sync(alebgk_batch *b);
 int alebgk_batch_destroy(alebgk_batch *b);

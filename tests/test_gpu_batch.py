@@ -57,12 +57,30 @@ def test_autotune_changes_only_launch_shapes(gpu):
     ms = t.autotune(2)
     assert ms > 0
     tt, pw = t.get_launch()
-    assert tt in (64, 128, 256) and pw in (0, 1, 2, 4)
+    assert tt in (0, 64, 128, 256) and pw in (0, 1, 2, 4)
     a.cudaStep(5)
     t.cudaStep(5)
     np.testing.assert_array_equal(t.cudaDownloadFull()[0], a.cudaDownloadFull()[0])
     a.close()
     t.close()
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+@pytest.mark.parametrize("name", ["cavity2d", "cavity3d"])
+def test_fused_transport_equals_separate_kernels(gpu, precision, name):
+    """Transport inside the particle kernel (transport threads 0) gives the
+    bitwise state of the separate transport kernel, MOOD redos included."""
+    sp = dict(SPECS[1] if name == "cavity2d" else SPECS[2])
+    sp.pop("name")
+    out = []
+    for tt in (0, 128):
+        s = ab.Solver(ab.Case(name, **sp), precision=precision)
+        s.set_launch(tt, 0)
+        s.cudaStep(6)
+        out.append(s.cudaDownloadFull())
+        s.close()
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
 
 
 def test_small_batch_runs_to_steady(gpu):
@@ -128,4 +146,22 @@ def test_mixed_batch_falls_back_to_branches(gpu):
     b = BatchSolver(SPECS, precision=32)
     b.step(1)
     assert not b.staged
+    b.close()
+
+
+def test_batch_autotune_keeps_states_exact(gpu):
+    """The batch autotuner's timed steps (stage groups 1, 2, 4 and per-cavity
+    branches) are real steps: afterwards every cavity holds exactly the state
+    of as many steps on its own."""
+    specs = batched_cavity2d(5, seed=11)
+    b = BatchSolver(specs, precision=32)
+    ms = b.autotune(2)
+    assert ms > 0
+    assert b.steps == 4 * (2 + 2)
+    b.step(1)
+    for i, sp in enumerate(specs):
+        g0, m0, _ = _alone(sp, 32, b.steps)
+        g1, m1 = b.solvers[i].cudaDownloadFull()
+        np.testing.assert_array_equal(g1, g0)
+        np.testing.assert_array_equal(m1, m0)
     b.close()
