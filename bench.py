@@ -51,6 +51,11 @@ def parse():
                          "(96 seeded cavities advanced by one graph launch per step), or the "
                          "learned warm start on 32 held-out cavity2d cases")
     ap.add_argument("--batch", type=int, default=96)
+    ap.add_argument("--batch-form", default="auto", choices=["auto", "stages", "branches"],
+                    help="batched-cavity2d graph form: autotuned, stage groups (4), or "
+                         "per-cavity branches")
+    ap.add_argument("--no-steady", action="store_true",
+                    help="batched-cavity2d: skip the run to the steady residual")
     ap.add_argument("--ncu", action="store_true",
                     help="profiler mode: --warmup steps then --steps steps, no timing "
                          "and no JSON (for ncu launch lists and captures)")
@@ -429,8 +434,10 @@ def run_batched(args):
     from alebgk4paper_b200.batch import BatchSolver, batched_cavity2d, partition_lpt
     specs = batched_cavity2d(args.batch, seed=0)
     mine = partition_lpt([s["Nx"] ** 2 * s["Nv"] ** 2 for s in specs], world)[rank]
-    b = BatchSolver([specs[i] for i in mine], precision=args.precision, device=local)
-    b.autotune(3)
+    b = BatchSolver([specs[i] for i in mine], precision=args.precision, device=local,
+                    launch="branches" if args.batch_form == "branches" else "stages")
+    if args.batch_form == "auto":
+        b.autotune(3)
     with ClockSampler(local) as clk:
         b.step(max(3, args.warmup))
         b.sync()
@@ -443,14 +450,17 @@ def run_batched(args):
     b.close()
     # Steps and wall time to steady from the Maxwellian at rest: a fresh
     # batch, timed from before its autotuning (the host set-up excluded).
-    b = BatchSolver([specs[i] for i in mine], precision=args.precision, device=local,
-                    autotune=False)
-    b.sync()
-    t1 = time.perf_counter()
-    b.autotune(3)
-    done = b.run_to_steady(tol=1e-6, check_every=100, max_steps=50000)
-    t_steady = time.perf_counter() - t1
-    b.close()
+    done, t_steady = np.zeros(1, np.int64), None
+    if not args.no_steady:
+        b = BatchSolver([specs[i] for i in mine], precision=args.precision, device=local,
+                        launch="branches" if args.batch_form == "branches" else "stages")
+        b.sync()
+        t1 = time.perf_counter()
+        if args.batch_form == "auto":
+            b.autotune(3)
+        done = b.run_to_steady(tol=1e-6, check_every=100, max_steps=50000)
+        t_steady = time.perf_counter() - t1
+        b.close()
     if rank != 0:
         return
     print(json.dumps({
@@ -461,14 +471,15 @@ def run_batched(args):
         "dtype": "f32" if args.precision == 32 else "f64",
         "data": "synthetic: seeded batched cavity2d instances (Nx, Nv, lid, density)",
         "config": {"workload": f"batched cavity2d, {len(mine)} of {args.batch} instances on "
-                               f"rank 0, one CUDA graph launch per step, autotuned "
-                               f"launch form", "instances": len(mine),
+                               f"rank 0, one CUDA graph launch per step, launch form "
+                               f"{args.batch_form}", "instances": len(mine),
                    "launch_form": (f"stage launches in {form} groups" if form
                                    else "per-cavity graph branches")},
         "timing": "wall clock around synchronised graph launches",
-        "steady": {"tol": 1e-6, "max_steps_to_steady": int(done.max()),
-                   "all_steady": bool((done > 0).all()), "seconds": t_steady,
-                   "seconds_cover": "autotuning and every step from the Maxwellian at rest"},
+        "steady": None if args.no_steady else {
+            "tol": 1e-6, "max_steps_to_steady": int(done.max()),
+            "all_steady": bool((done > 0).all()), "seconds": t_steady,
+            "seconds_cover": "autotuning and every step from the Maxwellian at rest"},
         "clocks": clk.summary(),
     }))
 
