@@ -137,6 +137,7 @@ int alebgk_destroy(alebgk_ctx *c)
     cudaSetDevice(c->cfg.device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     freeBuffers(c);
+    freeClassScratch(c->clsScratch);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->stream2) cudaStreamDestroy(c->stream2);
     if (c->evFork) cudaEventDestroy(c->evFork);
@@ -242,6 +243,8 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
         for (size_t q = 0; q < ncoef; ++q) cf[q] = (float)src[q];
         return cudaMemcpy(*dst, cf.data(), ncoef * 4, cudaMemcpyHostToDevice);
     };
+    c->coefCap = std::max<size_t>(ncoef, 1);
+    c->slotsCap = (size_t)N * tb.S;
     if (devTables)
     {
         CK(cudaMalloc(&d.coef, std::max<size_t>(ncoef, 1) * es));
@@ -286,6 +289,7 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
     c->surfHost.clear();
     for (int i = 0; i < N; ++i)
         if (cl->boundary[i] && cl->body_id[i] >= 0) c->surfHost.push_back(i);
+    c->surfCap = std::max<size_t>(c->surfHost.size(), 1);
     CK(dalloc(&d.surfList, c->surfHost.size()));
     CK(dalloc(&d.bodyIO, (size_t)kBodyIOHead + 13 * c->surfHost.size()));
     if (!c->surfHost.empty())
@@ -368,12 +372,145 @@ int alebgk_set_coeff_builder(int which)
     return ALEBGK_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Geometry refresh in place: the distribution, macros, moodCheck flags,
+// step scalars and every per-particle buffer stay where they are; the
+// geometry arrays, stencil classes and slot lists (built on the device from
+// the uploaded geometry) and MLS tables (solved on the device) are written
+// over the old ones, and only buffers that must grow are reallocated.  Returns 1 (nothing done) where it does not apply: tables the
+// host builds, or a cloud the lattice march takes.
+int refreshGeometryInPlace(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
+{
+    StepParams &p = c->sp;
+    const int N = p.N;
+    if (gCoeffBuilder != 0 || c->march.enabled) return 1;
+    bool anyBody = false;
+    for (int i = 0; i < N && !anyBody; ++i) anyBody = cl->body_id[i] >= 0;
+    const bool f64 = c->cfg.precision == 64;
+    if (!f64 && c->cfg.transport != 1 && !anyBody &&
+        marchEligible(cl->xyz, N, p.dim, cl->nnb, cl->nbr, ALEBGK_MAX_NEIGH))
+        return 1;
+    for (int i = 0; i < N; ++i)
+    {
+        if (cl->nnb[i] < 0 || cl->nnb[i] > ALEBGK_MAX_NEIGH)
+            return fail(c, ALEBGK_EINVAL, "neighbour count out of range at particle " +
+                                              std::to_string(i));
+        for (int s = 0; s < cl->nnb[i]; ++s)
+        {
+            int j = cl->nbr[(size_t)i * ALEBGK_MAX_NEIGH + s];
+            if (j < 0 || j >= N || j == i)
+                return fail(c, ALEBGK_EINVAL, "neighbour index out of range at particle " +
+                                                  std::to_string(i));
+        }
+    }
+    p.dt = dt;
+    p.lam = dt / p.tau;
+    p.c1 = 1.0 / (1.0 + p.lam);
+    CoeffInput in;
+    in.dim = p.dim; in.N = N; in.Nv = p.Nv; in.mlsOrder = p.mlsOrder;
+    in.dt = dt; in.h = p.h; in.vmin = p.vmin; in.dv = p.dv;
+    for (int a = 0; a < 3; ++a) { in.periodic[a] = p.periodic[a] != 0; in.L[a] = p.Lp[a]; }
+    in.xyz = cl->xyz; in.meshv = cl->meshv; in.wall = cl->wall;
+    in.boundary = cl->boundary; in.nnb = cl->nnb; in.nbr = cl->nbr;
+    in.maxNeigh = ALEBGK_MAX_NEIGH;
+    CoeffTables tb;
+    std::string err;
+    DeviceBuffers &d = c->d;
+    const size_t es = f64 ? 8 : 4;
+    // Geometry first: the class keys are computed from the device copy.
+    CK(cudaMemcpy(d.pos, cl->xyz, 24 * (size_t)N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.meshv, cl->meshv, 24 * (size_t)N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.wall, cl->wall, 56 * (size_t)N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.boundary, cl->boundary, 4 * (size_t)N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.bodyId, cl->body_id, 4 * (size_t)N, cudaMemcpyHostToDevice));
+    int maxnn = 0;
+    for (int i = 0; i < N; ++i) maxnn = std::max(maxnn, cl->nnb[i]);
+    if ((size_t)N * (1 + maxnn) > c->slotsCap)
+    {
+        cudaFree(d.slots);
+        d.slots = nullptr;
+        CK(dalloc(&d.slots, (size_t)N * (1 + maxnn)));
+        c->slotsCap = (size_t)N * (1 + maxnn);
+    }
+    bool collision = false;
+    CK(buildClassesDevice(in, d.pos, d.meshv, d.wall, d.boundary, d.cls, d.nslot, d.slots,
+                          c->slotsCap, c->clsScratch, tb, collision, c->stream));
+    if (collision)
+    {
+        // two keys share a hash: the host builder compares every key
+        if (!buildClasses(in, tb, &err)) return fail(c, ALEBGK_EINVAL, err);
+        CK(cudaMemcpy(d.cls, tb.cls.data(), 4 * (size_t)N, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.nslot, tb.nslot.data(), 4 * (size_t)N, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.slots, tb.slots.data(), 4 * (size_t)N * tb.S, cudaMemcpyHostToDevice));
+    }
+    const size_t ncoef = std::max<size_t>((size_t)tb.ncls * tb.S * tb.V, 1);
+    if (ncoef > c->coefCap)
+    {
+        cudaFree(d.coef);
+        cudaFree(d.coefLin);
+        d.coef = d.coefLin = nullptr;
+        CK(cudaMalloc(&d.coef, ncoef * es));
+        CK(cudaMalloc(&d.coefLin, ncoef * es));
+        c->coefCap = ncoef;
+    }
+    p.S = tb.S;
+    c->ncls = tb.ncls;
+    CK(buildTablesDevice(in, tb, p.mlsOrder, d.coef, f64, tb.degenerate, c->stream));
+    std::vector<int> degLin;
+    CK(buildTablesDevice(in, tb, p.limiter == 2 ? 1 : p.mlsOrder, d.coefLin, f64, degLin,
+                         c->stream));
+    c->degenerateParticles = 0;
+    for (int k = 0; k < tb.ncls; ++k)
+        if (tb.degenerate[k]) c->degenerateParticles += tb.members[k];
+    c->surfHost.clear();
+    for (int i = 0; i < N; ++i)
+        if (cl->boundary[i] && cl->body_id[i] >= 0) c->surfHost.push_back(i);
+    if (c->surfHost.size() > c->surfCap)
+    {
+        cudaFree(d.surfList);
+        cudaFree(d.bodyIO);
+        d.surfList = nullptr;
+        d.bodyIO = nullptr;
+        CK(dalloc(&d.surfList, c->surfHost.size()));
+        CK(dalloc(&d.bodyIO, (size_t)kBodyIOHead + 13 * c->surfHost.size()));
+        c->surfCap = c->surfHost.size();
+    }
+    if (!c->surfHost.empty())
+        CK(cudaMemcpy(d.surfList, c->surfHost.data(), 4 * c->surfHost.size(),
+                      cudaMemcpyHostToDevice));
+    CK(cudaStreamSynchronize(c->stream));
+    // The step graphs hold the old slot stride and table pointers.
+    for (auto &g : c->graph)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    if (c->macSnap) { cudaFree(c->macSnap); c->macSnap = nullptr; }
+    c->snapSteps = -1;
+    c->bodyIdHost.assign(cl->body_id, cl->body_id + N);
+    c->boundaryHost.assign(cl->boundary, cl->boundary + N);
+    c->geometryDirty = false;
+    return ALEBGK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int alebgk_upload_geometry(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
 {
     if (!c || !cl) return fail(c, ALEBGK_EINVAL, "null argument");
     if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    if (!cl->xyz || !cl->meshv || !cl->wall || !cl->boundary || !cl->body_id || !cl->nnb ||
+        !cl->nbr)
+        return fail(c, ALEBGK_EINVAL, "alebgk_upload_geometry needs the geometry members");
+    if (!(dt > 0)) return fail(c, ALEBGK_EINVAL, "dt must be > 0");
     CK(cudaSetDevice(c->cfg.device));
     CK(cudaStreamSynchronize(c->stream));
+    {
+        const int r = refreshGeometryInPlace(c, cl, dt);
+        if (r != 1) return r;
+    }
     const StepParams &p = c->sp;
     const size_t es = (c->cfg.precision == 64) ? 8 : 4;
     const size_t fBytes = (size_t)p.N * p.ldf * es;

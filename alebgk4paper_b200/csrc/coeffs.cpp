@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <unordered_map>
 
 namespace alebgk {
@@ -95,12 +96,12 @@ inline int basis(double dx, double dy, double dz, int ndim, double h,
 
 struct KeyHash
 {
-    size_t operator()(const std::vector<int64_t> &v) const
+    size_t operator()(const int64_t *v, size_t n) const
     {
         uint64_t h = 1469598103934665603ULL;
-        for (int64_t x : v)
+        for (size_t q = 0; q < n; ++q)
         {
-            h ^= (uint64_t)x + 0x9e3779b97f4a7c15ULL + (h << 6) + (h >> 2);
+            h ^= (uint64_t)v[q] + 0x9e3779b97f4a7c15ULL + (h << 6) + (h >> 2);
             h *= 1099511628211ULL;
         }
         return (size_t)h;
@@ -146,47 +147,61 @@ bool buildClasses(const CoeffInput &in, CoeffTables &out, std::string *err)
     // geometric difference between distinct stencils and far above the
     // rounding of x_j - x_i, so translated copies of a stencil compare equal.
     const double q = in.h * std::ldexp(1.0, -32);
-    std::vector<std::vector<int64_t>> keys(N);
-    std::vector<uint64_t> hashes(N);
-#pragma omp parallel for schedule(static)
+    // Every particle's key (boundary flag, order, count, mesh velocity bits,
+    // wall bits for wall particles, quantised sorted displacements) in one
+    // flat array; keys are hashed in parallel and compared in full on a hash
+    // hit.
+    std::vector<size_t> koff((size_t)N + 1, 0);
     for (int i = 0; i < N; ++i)
+        koff[i + 1] = koff[i] + 6 + (in.boundary[i] ? 7 : 0) + 3 * (size_t)in.nnb[i];
+    // (uninitialised: every entry is written below, in parallel)
+    std::unique_ptr<int64_t[]> keys(new int64_t[std::max<size_t>(koff[N], 1)]);
+    std::vector<uint64_t> hashes(N);
+#pragma omp parallel
     {
-        const int nn = in.nnb[i];
-        std::vector<std::pair<std::array<int64_t, 3>, int>> nb(nn);
-        for (int s = 0; s < nn; ++s)
+        std::vector<std::pair<std::array<int64_t, 3>, int>> nb(std::max(maxnn, 1));
+#pragma omp for schedule(static)
+        for (int i = 0; i < N; ++i)
         {
-            int j = in.nbr[(size_t)i * in.maxNeigh + s];
-            double d[3];
-            for (int a = 0; a < 3; ++a)
+            const int nn = in.nnb[i];
+            for (int s = 0; s < nn; ++s)
             {
-                d[a] = (a < ndim) ? in.xyz[3 * j + a] - in.xyz[3 * i + a] : 0.0;
-                if (a < ndim && in.periodic[a]) d[a] = minImage(d[a], in.L[a]);
+                int j = in.nbr[(size_t)i * in.maxNeigh + s];
+                double d[3];
+                for (int a = 0; a < 3; ++a)
+                {
+                    d[a] = (a < ndim) ? in.xyz[3 * j + a] - in.xyz[3 * i + a] : 0.0;
+                    if (a < ndim && in.periodic[a]) d[a] = minImage(d[a], in.L[a]);
+                }
+                nb[s].first = {std::llround(d[2] / q), std::llround(d[1] / q),
+                               std::llround(d[0] / q)};
+                nb[s].second = j;
             }
-            nb[s].first = {std::llround(d[2] / q), std::llround(d[1] / q),
-                           std::llround(d[0] / q)};
-            nb[s].second = j;
+            std::sort(nb.begin(), nb.begin() + nn);
+            int *sl = &out.slots[(size_t)i * S];
+            sl[0] = i;
+            for (int s = 0; s < nn; ++s) sl[1 + s] = nb[s].second;
+            for (int s = 1 + nn; s < S; ++s) sl[s] = i;   // padding, coefficient 0
+            out.nslot[i] = 1 + nn;
+            int64_t *k = &keys[koff[i]];
+            size_t w = 0;
+            const int order = in.boundary[i] ? 1 : in.mlsOrder;
+            k[w++] = in.boundary[i];
+            k[w++] = order;
+            k[w++] = nn;
+            for (int a = 0; a < 3; ++a) k[w++] = bitsOf(in.meshv[3 * i + a]);
+            if (in.boundary[i])
+                for (int a = 0; a < 7; ++a) k[w++] = bitsOf(in.wall[7 * i + a]);
+            for (int s = 0; s < nn; ++s)
+                for (int a = 0; a < 3; ++a) k[w++] = nb[s].first[a];
+            hashes[i] = KeyHash()(k, w);
         }
-        std::sort(nb.begin(), nb.end());
-        int *sl = &out.slots[(size_t)i * S];
-        sl[0] = i;
-        for (int s = 0; s < nn; ++s) sl[1 + s] = nb[s].second;
-        for (int s = 1 + nn; s < S; ++s) sl[s] = i;   // padding, coefficient 0
-        out.nslot[i] = 1 + nn;
-        std::vector<int64_t> &k = keys[i];
-        int order = in.boundary[i] ? 1 : in.mlsOrder;
-        k.reserve(3 * nn + 12);
-        k.push_back(in.boundary[i]);
-        k.push_back(order);
-        k.push_back(nn);
-        for (int a = 0; a < 3; ++a) k.push_back(bitsOf(in.meshv[3 * i + a]));
-        if (in.boundary[i])
-            for (int a = 0; a < 7; ++a) k.push_back(bitsOf(in.wall[7 * i + a]));
-        for (int s = 0; s < nn; ++s)
-            for (int a = 0; a < 3; ++a) k.push_back(nb[s].first[a]);
-        hashes[i] = KeyHash()(k);
     }
-    // Class ids in order of first appearance; keys are hashed in parallel
-    // above and compared in full on a hash hit.
+    // Class ids in order of first appearance.
+    auto sameKey = [&](int x, int y) {
+        const size_t lx = koff[x + 1] - koff[x], ly = koff[y + 1] - koff[y];
+        return lx == ly && std::memcmp(&keys[koff[x]], &keys[koff[y]], lx * 8) == 0;
+    };
     std::unordered_map<uint64_t, std::vector<int>> byHash;
     byHash.reserve(1024);
     for (int i = 0; i < N; ++i)
@@ -194,7 +209,7 @@ bool buildClasses(const CoeffInput &in, CoeffTables &out, std::string *err)
         std::vector<int> &cand = byHash[hashes[i]];
         int id = -1;
         for (int c : cand)
-            if (keys[out.rep[c]] == keys[i]) { id = c; break; }
+            if (sameKey(out.rep[c], i)) { id = c; break; }
         if (id < 0)
         {
             id = (int)out.rep.size();
@@ -203,7 +218,6 @@ bool buildClasses(const CoeffInput &in, CoeffTables &out, std::string *err)
         }
         out.cls[i] = id;
     }
-    keys.clear();
     const int ncls = (int)out.rep.size();
     out.ncls = ncls;
     out.degenerate.assign(ncls, 0);

@@ -45,6 +45,10 @@ struct CoeffTables
     std::vector<int> degenerate;    // ncls: nodes with a skipped pivot
     std::vector<int> order;         // ncls: MLS order used
     std::vector<int> members;       // ncls: particles in the class
+    // Set by the device class builder instead of nslot/slots (which stay
+    // on the device): the slot count and slot row of each representative.
+    std::vector<int> repNslot;      // ncls
+    std::vector<int> repSlots;      // ncls*S
 };
 
 // Builds classes and coefficients.  Returns false with *err on bad input.

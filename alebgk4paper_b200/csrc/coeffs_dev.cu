@@ -205,11 +205,12 @@ cudaError_t buildTablesDevice(const CoeffInput &in, const CoeffTables &cls, int 
     {
         const int r = cls.rep[c];
         bnd[c] = in.boundary[r];
-        nsl[c] = cls.nslot[r];
+        const bool packed = cls.slots.empty();
+        nsl[c] = packed ? cls.repNslot[c] : cls.nslot[r];
         double *o = &rep[13 * (size_t)c];
         for (int q = 0; q < 3; ++q) { o[q] = in.xyz[3 * (size_t)r + q]; o[3 + q] = in.meshv[3 * (size_t)r + q]; }
         for (int q = 0; q < 7; ++q) o[6 + q] = in.wall[7 * (size_t)r + q];
-        const int *sl = &cls.slots[(size_t)r * S];
+        const int *sl = packed ? &cls.repSlots[(size_t)c * S] : &cls.slots[(size_t)r * S];
         for (int s = 1; s < nsl[c]; ++s)
             for (int q = 0; q < 3; ++q) pos[((size_t)c * S + s) * 3 + q] = in.xyz[3 * (size_t)sl[s] + q];
     }

@@ -94,6 +94,20 @@ struct StepParams
 
 }  // namespace alebgk
 
+namespace alebgk {
+// Device scratch of the stencil-class builder (classes_dev.cu), kept by a
+// context between geometry refreshes; caps in elements.
+struct ClassScratch
+{
+    int *nnb = nullptr, *nbr = nullptr, *first = nullptr, *same = nullptr, *rep = nullptr;
+    int *repSlots = nullptr, *repNslot = nullptr;
+    long long *koff = nullptr, *keys = nullptr;
+    unsigned long long *hashes = nullptr;
+    size_t capN = 0, capNbr = 0, capFirst = 0, capSame = 0, capRep = 0, capRepSlots = 0;
+    size_t capRepNslot = 0, capKoff = 0, capKeys = 0, capHash = 0;
+};
+}  // namespace alebgk
+
 struct alebgk_ctx
 {
     alebgk_config cfg{};
@@ -126,6 +140,10 @@ struct alebgk_ctx
     long long hostSteps = 0;     // steps enqueued since the upload
     double *macSnap = nullptr;   // macros at the last interval residual (N x 6)
     long long snapSteps = -1;    // hostSteps of that snapshot (-1: none)
+    // Allocated elements of the buffers that a geometry refresh may resize:
+    // each MLS table, the slot lists, the surface list.
+    size_t coefCap = 0, slotsCap = 0, surfCap = 0;
+    alebgk::ClassScratch clsScratch;
 };
 
 namespace alebgk {
@@ -184,6 +202,16 @@ struct CoeffTables;
 cudaError_t buildTablesDevice(const CoeffInput &in, const CoeffTables &cls, int order,
                               void *table, bool f64, std::vector<int> &degenerate,
                               cudaStream_t st);
+// Stencil classes of a cloud whose geometry is on the device (classes_dev.cu):
+// writes the slot counts, slot lists (stride 1 + max neighbours) and class
+// ids on the device and fills `out` as buildClasses does (with the
+// representatives' slot rows in repSlots/repNslot instead of slots/nslot).
+// `collision` set: two different keys share a hash; use buildClasses.
+cudaError_t buildClassesDevice(const CoeffInput &in, const double *dXyz, const double *dMeshv,
+                               const double *dWall, const int *dBoundary, int *dCls,
+                               int *dNslot, int *dSlots, size_t slotsCap, ClassScratch &scr,
+                               CoeffTables &out, bool &collision, cudaStream_t st);
+void freeClassScratch(ClassScratch &s);
 cudaError_t launchSeedGrad13(alebgk_ctx *c, const float *net, int ldnet, const double *scale,
                              const double *shift);
 cudaError_t launchMoments13(alebgk_ctx *c, double *out);
