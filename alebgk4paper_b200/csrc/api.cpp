@@ -357,6 +357,7 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
     c->boundaryHost.assign(cl->boundary, cl->boundary + N);
     c->cur = 0;
     c->uploaded = true;
+    ++c->epoch;
     return withState ? alebgk_upload_state(c, cl->g, cl->macro) : ALEBGK_OK;
 }
 
@@ -490,6 +491,7 @@ int refreshGeometryInPlace(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
     c->bodyIdHost.assign(cl->body_id, cl->body_id + N);
     c->boundaryHost.assign(cl->boundary, cl->boundary + N);
     c->geometryDirty = false;
+    ++c->epoch;
     return ALEBGK_OK;
 }
 

@@ -38,6 +38,7 @@ struct alebgk_batch
     std::vector<BatchLaunch> groups;      // stage launches per group
     std::vector<int> groupStream;         // context whose stream runs the group
     int ngroups = 4;                      // stage groups wanted
+    std::vector<unsigned long long> epochs;   // the contexts' epochs of the captured graphs
     std::string err;
 };
 
@@ -294,8 +295,21 @@ int alebgk_batch_step(alebgk_batch *b, int nsteps)
     alebgk_ctx *c = b->ctx[0];
     CKC(cudaSetDevice(b->device));
     for (alebgk_ctx *x : b->ctx)
-        if (x->geometryDirty || x->cur != c->cur)
+        if (!x->uploaded || x->geometryDirty || x->cur != c->cur)
             return failc(x, ALEBGK_ESTATE, "a context of the batch left the lockstep");
+    // A context uploaded or refreshed since the capture: its buffers and slot
+    // stride may have changed, so the graphs and stage launches are rebuilt.
+    bool stale = b->epochs.size() != b->ctx.size();
+    for (size_t i = 0; i < b->ctx.size() && !stale; ++i) stale = b->epochs[i] != b->ctx[i]->epoch;
+    if (stale)
+    {
+        CKC(cudaStreamSynchronize(b->master));
+        for (auto &g : b->graph)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        freeGroups(b);
+        b->epochs.clear();
+        for (alebgk_ctx *x : b->ctx) b->epochs.push_back(x->epoch);
+    }
     for (int n = 0; n < nsteps; ++n)
     {
         const int from = c->cur;

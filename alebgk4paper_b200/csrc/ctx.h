@@ -144,6 +144,9 @@ struct alebgk_ctx
     // each MLS table, the slot lists, the surface list.
     size_t coefCap = 0, slotsCap = 0, surfCap = 0;
     alebgk::ClassScratch clsScratch;
+    // Counts the uploads and geometry refreshes: captured batch graphs and
+    // stage descriptors hold device pointers and slot strides of one epoch.
+    unsigned long long epoch = 0;
 };
 
 namespace alebgk {

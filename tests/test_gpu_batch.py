@@ -165,3 +165,22 @@ def test_batch_autotune_keeps_states_exact(gpu):
         np.testing.assert_array_equal(g1, g0)
         np.testing.assert_array_equal(m1, m0)
     b.close()
+
+
+@pytest.mark.parametrize("launch", ["stages", "branches"])
+def test_batch_recaptures_after_a_context_is_uploaded_again(gpu, launch):
+    """A context uploaded again between batch steps has new buffers: the
+    batch notices (upload epoch) and rebuilds its graphs, so the cavity
+    restarts from its upload and the others carry on, each exactly as alone."""
+    specs = batched_cavity2d(3, seed=5)
+    b = BatchSolver(specs, precision=32, launch=launch)
+    b.step(2)
+    b.sync()
+    b.solvers[0].cudaUploadCloud(b.cases[0])
+    b.step(2)
+    g0, m0, _ = _alone(specs[0], 32, 2)
+    np.testing.assert_array_equal(b.solvers[0].cudaDownloadFull()[0], g0)
+    for i in (1, 2):
+        gi, mi, _ = _alone(specs[i], 32, 4)
+        np.testing.assert_array_equal(b.solvers[i].cudaDownloadFull()[0], gi)
+    b.close()
