@@ -207,9 +207,34 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
           marchEligible(cl->xyz, N, p.dim, cl->nnb, cl->nbr, ALEBGK_MAX_NEIGH));
     CoeffInput inLin = in;
     inLin.mlsOrder = 1;
+    DeviceBuffers &d = c->d;
+    // With tables solved on the device, the geometry goes up first and the
+    // stencil classes and slot lists are built there too.
+    bool devClasses = false;
     if (devTables)
     {
-        if (!buildClasses(in, tb, &err)) return fail(c, ALEBGK_EINVAL, err);
+        int maxnn = 0;
+        for (int i = 0; i < N; ++i) maxnn = std::max(maxnn, cl->nnb[i]);
+        const size_t slotsN = (size_t)N * (1 + maxnn);
+        CK(dalloc(&d.pos, 3 * (size_t)N));
+        CK(dalloc(&d.meshv, 3 * (size_t)N));
+        CK(dalloc(&d.wall, 7 * (size_t)N));
+        CK(dalloc(&d.boundary, N));
+        CK(dalloc(&d.bodyId, N));
+        CK(dalloc(&d.cls, N));
+        CK(dalloc(&d.nslot, N));
+        CK(dalloc(&d.slots, slotsN));
+        CK(cudaMemcpy(d.pos, cl->xyz, 24 * (size_t)N, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.meshv, cl->meshv, 24 * (size_t)N, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.wall, cl->wall, 56 * (size_t)N, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.boundary, cl->boundary, 4 * (size_t)N, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.bodyId, cl->body_id, 4 * (size_t)N, cudaMemcpyHostToDevice));
+        bool collision = false;
+        CK(buildClassesDevice(in, d.pos, d.meshv, d.wall, d.boundary, d.cls, d.nslot, d.slots,
+                              slotsN, c->clsScratch, tb, collision, c->stream));
+        devClasses = !collision;
+        // two keys share a hash: the host builder compares every key
+        if (collision && !buildClasses(in, tb, &err)) return fail(c, ALEBGK_EINVAL, err);
     }
     else
     {
@@ -228,7 +253,6 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
 
     const bool f64 = c->cfg.precision == 64;
     const size_t es = f64 ? 8 : 4;
-    DeviceBuffers &d = c->d;
     const size_t fBytes = (size_t)N * p.ldf * es;
     CK(cudaMalloc(&d.f[0], fBytes));
     CK(cudaMalloc(&d.f[1], fBytes));
@@ -262,14 +286,17 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
     c->degenerateParticles = 0;
     for (int k = 0; k < tb.ncls; ++k)
         if (tb.degenerate[k]) c->degenerateParticles += tb.members[k];
-    CK(dalloc(&d.pos, 3 * (size_t)N));
-    CK(dalloc(&d.meshv, 3 * (size_t)N));
-    CK(dalloc(&d.wall, 7 * (size_t)N));
-    CK(dalloc(&d.boundary, N));
-    CK(dalloc(&d.bodyId, N));
-    CK(dalloc(&d.cls, N));
-    CK(dalloc(&d.nslot, N));
-    CK(dalloc(&d.slots, (size_t)N * tb.S));
+    if (!devTables)
+    {
+        CK(dalloc(&d.pos, 3 * (size_t)N));
+        CK(dalloc(&d.meshv, 3 * (size_t)N));
+        CK(dalloc(&d.wall, 7 * (size_t)N));
+        CK(dalloc(&d.boundary, N));
+        CK(dalloc(&d.bodyId, N));
+        CK(dalloc(&d.cls, N));
+        CK(dalloc(&d.nslot, N));
+        CK(dalloc(&d.slots, (size_t)N * tb.S));
+    }
     CK(dalloc(&d.macro[0], 6 * (size_t)N));
     CK(dalloc(&d.macro[1], 6 * (size_t)N));
     CK(dalloc(&d.mood, N));
@@ -296,14 +323,20 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
         CK(cudaMemcpy(d.surfList, c->surfHost.data(), 4 * c->surfHost.size(),
                       cudaMemcpyHostToDevice));
     c->geometryDirty = false;
-    CK(cudaMemcpy(d.pos, cl->xyz, 24 * (size_t)N, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d.meshv, cl->meshv, 24 * (size_t)N, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d.wall, cl->wall, 56 * (size_t)N, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d.boundary, cl->boundary, 4 * (size_t)N, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d.bodyId, cl->body_id, 4 * (size_t)N, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d.cls, tb.cls.data(), 4 * (size_t)N, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d.nslot, tb.nslot.data(), 4 * (size_t)N, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d.slots, tb.slots.data(), 4 * (size_t)N * tb.S, cudaMemcpyHostToDevice));
+    if (!devTables)
+    {
+        CK(cudaMemcpy(d.pos, cl->xyz, 24 * (size_t)N, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.meshv, cl->meshv, 24 * (size_t)N, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.wall, cl->wall, 56 * (size_t)N, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.boundary, cl->boundary, 4 * (size_t)N, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.bodyId, cl->body_id, 4 * (size_t)N, cudaMemcpyHostToDevice));
+    }
+    if (!devClasses)
+    {
+        CK(cudaMemcpy(d.cls, tb.cls.data(), 4 * (size_t)N, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.nslot, tb.nslot.data(), 4 * (size_t)N, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d.slots, tb.slots.data(), 4 * (size_t)N * tb.S, cudaMemcpyHostToDevice));
+    }
     CK(cudaMemset(d.dpx, 0, 8 * (size_t)N));
     CK(cudaMemset(d.sc, 0, sizeof(StepScalars)));
     CK(prepareKernels(c));
@@ -311,8 +344,9 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
         return fail(c, ALEBGK_EINVAL,
                     "the streamed particle kernel needs a 3-D cloud whose rows fit in "
                     "shared memory");
-    // Lattice-marching transport (FP32, complete 3-D lattice).
-    if (!f64 && c->cfg.transport != 1)
+    // Lattice-marching transport (FP32, complete 3-D lattice; such clouds
+    // always take the host tables, which the plan re-lays).
+    if (!f64 && c->cfg.transport != 1 && !devTables)
     {
         MarchPlan plan;
         buildMarchPlan(cl->xyz, N, p.dim, cl->nnb, cl->nbr, ALEBGK_MAX_NEIGH, tb,
