@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from conftest import golden
-from tests.golden.make_golden import STEPS
+from tests.golden.make_golden import LONG_STEPS, STEPS
 
 import alebgk4paper_b200 as ab
 from oracle.oracle import Oracle
@@ -93,6 +93,28 @@ def test_gpu_matches_reference_fixtures(gpu, tag, case, Nx, Nv, order, steps, fu
     assert rel(g.sum(axis=1), fx["gsum"]) < 1e-10
     if full:
         assert rel(g, fx["g"]) < 1e-10
+    s.close()
+
+
+@pytest.mark.parametrize("tag,case,Nx,Nv,order,steps,full", LONG_STEPS)
+def test_gpu_matches_reference_over_the_full_run(gpu, tag, case, Nx, Nv, order, steps, full):
+    """The plain cavity2d (Nx 20, Nv 16, quadratic, default dt) over its 500
+    steps in FP64 against the reference's own run: the same transport-flag
+    and moodCheck decisions at every step, and rho, u, v, T within 1e-6
+    relative (L2), the FP64 contract."""
+    fx = golden(f"step_{tag}.npz")
+    c = ab.Case(case, Nx, Nv, -1.0, order, fixed_body=True)
+    s = ab.Solver(c, precision=64)
+    flags = []
+    for _ in range(steps):
+        s.cudaStep(1)
+        cnt = s.counters()
+        flags.append([cnt["transport_flags"], cnt["mood_fail"]])
+    np.testing.assert_array_equal(np.array(flags), fx["flags"])
+    _, m = s.cudaDownloadFull()
+    for q in (0, 1, 2, 4):
+        d = np.linalg.norm(m[:, q] - fx["macro"][:, q]) / np.linalg.norm(fx["macro"][:, q])
+        assert d < 1e-6, (q, d)
     s.close()
 
 
