@@ -46,7 +46,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--workload", default="cavity3d",
-                    choices=["cavity3d", "batched-cavity2d", "warm-start", "free-body"],
+                    choices=["cavity3d", "batched-cavity2d", "warm-start", "free-body",
+                             "fp32-error"],
                     help="cavity3d (the headline line), the batched cavity2d workload "
                          "(96 seeded cavities advanced by one graph launch per step), or the "
                          "learned warm start on 32 held-out cavity2d cases")
@@ -543,6 +544,58 @@ def run_ncu(args):
     s.close()
 
 
+def run_fp32_error(args):
+    """cavity3d Nx40 Nv10 from rest in FP32 (the bench's mode) and in FP64 on
+    the device, side by side for --steps steps (the configuration's length
+    is 2000): the relative L2 error of every macroscopic field and of f
+    against the FP64 run, at checkpoints along the way."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    import torch
+    torch.cuda.set_device(local)
+    import alebgk4paper_b200 as ab
+    steps = args.steps
+    c = ab.Case(WORKLOAD["case"], WORKLOAD["Nx"], WORKLOAD["Nv"], -1.0, WORKLOAD["mls_order"])
+    s32 = ab.Solver(c, precision=32, device=local)
+    s64 = ab.Solver(c, precision=64, device=local)
+    names = ("rho", "ux", "uy", "uz", "T", "p")
+    marks = sorted({k for k in (1, 10, 100, 250, 500, 1000, 1500, 2000) if k <= steps} | {steps})
+    rows, done = [], 0
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+    with ClockSampler(local) as clk:
+        for k in marks:
+            s32.cudaStep(k - done)
+            s64.cudaStep(k - done)
+            done = k
+            g32, m32 = s32.cudaDownloadFull()
+            g64, m64 = s64.cudaDownloadFull()
+            row = {"step": k, "f": rel(g32, g64)}
+            for j, n in enumerate(names):
+                if n in ("ux", "uy", "uz"):
+                    # velocities against the thermal speed sqrt(R T) of the FP64 run
+                    th = np.sqrt(208.0 * m64[:, 4])
+                    row[n] = float(np.linalg.norm((m32[:, j] - m64[:, j]) / th) /
+                                   np.sqrt(len(th)))
+                else:
+                    row[n] = rel(m32[:, j], m64[:, j])
+            rows.append(row)
+    s32.close()
+    s64.close()
+    print(json.dumps({
+        "metric": "FP32 field error against the FP64 device run", "value": rows[-1]["rho"],
+        "unit": "relative L2 (rho)", "n_gpus": 1, "steps": steps, "warmup": 0,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 against f64", "data": "synthetic: the reference's cavity3d case from rest",
+        "config": {"workload": "cavity3d Nx=40 Nv=10 quadratic MLS, 64000 x 1000",
+                   "velocity_error": "RMS of (u32 - u64) / sqrt(R T64) over particles"},
+        "errors": rows, "clocks": clk.summary(),
+    }))
+
+
 def run_free_body(args):
     """The free-body cube (cavity3d-cube Nx40 Nv10, density 4.4, parabolic lid
     10 m/s, dt 1.5e-11): --warmup untimed then --steps timed steps of fluid
@@ -643,6 +696,8 @@ def main():
         run_warm_start(args)
     elif args.workload == "free-body" and args.impl == "ours":
         run_free_body(args)
+    elif args.workload == "fp32-error" and args.impl == "ours":
+        run_fp32_error(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
