@@ -18,7 +18,8 @@ using namespace alebgk;
 namespace {
 
 std::string gCreateError;
-int gCoeffBuilder = 0;   // 0: tables on the device where possible, 1: host
+int gCoeffBuilder = 0;   // 0: classes and tables on the device where possible, 1: host,
+                         // 2: host classes with device tables (the hash-collision path)
 
 int fail(alebgk_ctx *c, int code, const std::string &msg)
 {
@@ -202,7 +203,7 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
     bool anyBody = false;
     for (int i = 0; i < N && !anyBody; ++i) anyBody = cl->body_id[i] >= 0;
     const bool devTables =
-        gCoeffBuilder == 0 &&
+        (gCoeffBuilder == 0 || gCoeffBuilder == 2) &&
         !(!f64cloud && c->cfg.transport != 1 && !anyBody &&
           marchEligible(cl->xyz, N, p.dim, cl->nnb, cl->nbr, ALEBGK_MAX_NEIGH));
     CoeffInput inLin = in;
@@ -230,8 +231,11 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
         CK(cudaMemcpy(d.boundary, cl->boundary, 4 * (size_t)N, cudaMemcpyHostToDevice));
         CK(cudaMemcpy(d.bodyId, cl->body_id, 4 * (size_t)N, cudaMemcpyHostToDevice));
         bool collision = false;
-        CK(buildClassesDevice(in, d.pos, d.meshv, d.wall, d.boundary, d.cls, d.nslot, d.slots,
-                              slotsN, c->clsScratch, tb, collision, c->stream));
+        if (gCoeffBuilder == 2)
+            collision = true;
+        else
+            CK(buildClassesDevice(in, d.pos, d.meshv, d.wall, d.boundary, d.cls, d.nslot,
+                                  d.slots, slotsN, c->clsScratch, tb, collision, c->stream));
         devClasses = !collision;
         // two keys share a hash: the host builder compares every key
         if (collision && !buildClasses(in, tb, &err)) return fail(c, ALEBGK_EINVAL, err);
@@ -402,7 +406,7 @@ int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
 
 int alebgk_set_coeff_builder(int which)
 {
-    if (which != 0 && which != 1) return ALEBGK_EINVAL;
+    if (which < 0 || which > 2) return ALEBGK_EINVAL;
     gCoeffBuilder = which;
     return ALEBGK_OK;
 }
@@ -421,7 +425,7 @@ int refreshGeometryInPlace(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
 {
     StepParams &p = c->sp;
     const int N = p.N;
-    if (gCoeffBuilder != 0 || c->march.enabled) return 1;
+    if (gCoeffBuilder == 1 || c->march.enabled) return 1;
     bool anyBody = false;
     for (int i = 0; i < N && !anyBody; ++i) anyBody = cl->body_id[i] >= 0;
     const bool f64 = c->cfg.precision == 64;
@@ -470,9 +474,10 @@ int refreshGeometryInPlace(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
         CK(dalloc(&d.slots, (size_t)N * (1 + maxnn)));
         c->slotsCap = (size_t)N * (1 + maxnn);
     }
-    bool collision = false;
-    CK(buildClassesDevice(in, d.pos, d.meshv, d.wall, d.boundary, d.cls, d.nslot, d.slots,
-                          c->slotsCap, c->clsScratch, tb, collision, c->stream));
+    bool collision = gCoeffBuilder == 2;
+    if (!collision)
+        CK(buildClassesDevice(in, d.pos, d.meshv, d.wall, d.boundary, d.cls, d.nslot, d.slots,
+                              c->slotsCap, c->clsScratch, tb, collision, c->stream));
     if (collision)
     {
         // two keys share a hash: the host builder compares every key

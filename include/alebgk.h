@@ -367,10 +367,12 @@ int alebgk_net_train_step(alebgk_net *net, const float *pts_dev, const float *tg
                           float beta1, float beta2, float eps, float *loss_host);
 int alebgk_net_sync(alebgk_net *net);
 
-/* Where alebgk_upload builds the MLS coefficient tables: 0 (default) on the
- * device, bitwise equal to the host builder, except for clouds the lattice
- * march takes (its plan needs the host tables); 1 always on the host.
- * Process-wide; for checks of one against the other. */
+/* Where alebgk_upload and alebgk_upload_geometry build the stencil classes
+ * and MLS coefficient tables: 0 (default) both on the device, bitwise equal
+ * to the host builders, except for clouds the lattice march takes (its plan
+ * needs the host tables); 1 always on the host; 2 host classes with device
+ * tables (the path a hash collision of two different stencil keys takes).
+ * Process-wide; for checks of one against another. */
 int alebgk_set_coeff_builder(int which);
 
 /* alebgk_upload for a cloud whose particle set is unchanged: geometry, wall
