@@ -33,3 +33,45 @@ def test_lpt_partition_covers_every_instance_and_balances():
         # LPT is within 4/3 of the optimum; the mean is a lower bound of it
         assert max(loads) <= 4.0 / 3.0 * max(np.mean(loads), max(cost)) + 1e-9
         assert partition_lpt(cost, n) == parts
+
+
+def test_batch_solver_rejects_unknown_forms_before_any_device_work():
+    """The graph form and the set-up mode are checked first, so a typo fails
+    on the host with a clear message."""
+    import pytest
+    from alebgk4paper_b200.batch import BatchSolver
+    with pytest.raises(ValueError, match="launch"):
+        BatchSolver([], launch="persistent")
+    with pytest.raises(ValueError, match="setup"):
+        BatchSolver([], setup="gpu")
+
+
+def test_batch_and_launch_entry_points_are_exported():
+    """The C-ABI of the batch forms, the batch autotuner and the launch
+    shapes is declared in the header and exported by the library."""
+    import os
+    from alebgk4paper_b200 import _abi
+    lib = _abi.load()
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    header = open(os.path.join(root, "include", "alebgk.h")).read()
+    for name in ("alebgk_batch_set_mode", "alebgk_batch_get_mode", "alebgk_batch_set_groups",
+                 "alebgk_batch_autotune", "alebgk_set_launch", "alebgk_get_launch",
+                 "alebgk_upload_geometry", "alebgk_set_coeff_builder"):
+        assert f"{name}(" in header, name
+        assert hasattr(lib, name), name
+    # only 0, 1, 2 are builder modes; the setting is restored
+    assert lib.alebgk_set_coeff_builder(3) != 0
+    assert lib.alebgk_set_coeff_builder(-1) != 0
+    assert lib.alebgk_set_coeff_builder(0) == 0
+
+
+def test_bench_parses_the_batch_and_error_workloads():
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "bench.py", "--help"], cwd=root, capture_output=True,
+                         text=True, timeout=120)
+    assert out.returncode == 0
+    for flag in ("--batch-form", "--no-steady", "fp32-error"):
+        assert flag in out.stdout, flag
