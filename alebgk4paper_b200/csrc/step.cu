@@ -1922,16 +1922,17 @@ struct BatchCtx
 {
     ParticleArgs<T> pa;        // parity `from`: pa.g = f[1 - from], pa.fold = f[from]
     StepParams p;
-    const T *coef;
     double *redPartial;
     double *resid;
     int *mood;
     int wpb;                   // particles (warps) per block of the particle stage
 };
 
+// Stages: 0 begin, 1 transport (empty: fused into the particle stage, the
+// slot keeps the numbering of the cloud's own launch order), 2 particle,
+// 3 redo, 4 sigma, 5 fixup, 6 mass sum, 7 scale + moodCheck, 8 recollide,
+// 9 end mass, 10 residual.
 constexpr int kBatchStages = 11;
-constexpr int kBatchTT = 256;  // transport threads per block in a batch
-constexpr int kBatchTile = kBatchTT / 32;      // particles per transport block
 
 __device__ __forceinline__ int batchCtxOf(const int *__restrict__ off, int n, int b)
 {
@@ -1985,17 +1986,6 @@ k_batch_begin(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ off, 
         sc->nfix = 0;
         sc->moodfail = 0;
     }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kBatchTT)
-k_batch_transport(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ off, int n)
-{
-    BATCH_CTX(1);
-    const StepParams &p = B.p;
-    const int chunks = transportChunks(p.V);
-    k_transport_body<T>(B.pa.fold, B.pa.g, B.coef, B.pa.cls, B.pa.nslot, B.pa.slots, p.S, p.N,
-                        p.V, p.L, p.ldf, B.pa.sc, vb % chunks, vb / chunks);
 }
 
 template <typename T, int L>
@@ -2146,7 +2136,6 @@ static cudaError_t buildBatchT(alebgk_ctx *const *cs, int n, double *const *resi
             pa.nad = d.nad;
             b.p = p;
             b.mood = d.mood;
-            b.coef = static_cast<const T *>(d.coef);
             b.redPartial = d.redPartial;
             b.resid = resid[i];
             b.wpb = wpb;
@@ -2197,7 +2186,6 @@ static cudaError_t batchStepT(const BatchLaunch &bl, int from, cudaStream_t st)
     const int *off = bl.off;
     auto go = [&](int s) { return bl.blocks[s] > 0; };
     if (go(0)) k_batch_begin<T><<<bl.blocks[0], kNT, 0, st>>>(ctx, off, n);
-    if (go(1)) k_batch_transport<T><<<bl.blocks[1], kBatchTT, 0, st>>>(ctx, off, n);
     if (go(2)) k_batch_particle<T, L><<<bl.blocks[2], kNT, bl.smemParticle, st>>>(ctx, off, n);
     if (go(3)) k_batch_redo<T, L><<<bl.blocks[3], kNT, bl.smemRedo, st>>>(ctx, off, n);
     if (go(4)) k_batch_sigma<T><<<bl.blocks[4], kRedThreads, 0, st>>>(ctx, off, n);
