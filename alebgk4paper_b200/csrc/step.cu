@@ -4,6 +4,9 @@
 //   k_step_begin      reset the step's counters (and the NAD neighbour ranges
 //                     of the streamed particle kernel)
 //   k_transport       gt[i][k] = scale * sum_s coef[class][s][k] * h[slot s][k]
+//                     (k_march in march.cu for lattice clouds; by default the
+//                     gather runs inside k_particle, each warp building its
+//                     particle's row in shared memory)
 //   k_particle        per particle (one warp; k_particle_stream for 3-D clouds):
 //                     positivity repair, MOOD PAD/NAD
 //                     screen with linear redo, diffuse wall or moments + BGK
@@ -12,6 +15,8 @@
 //   k_scale_mood      sigma on the macros, moodCheck
 //   k_recollide       second collision when moodCheck failed (else exits)
 //   k_mass_end        end-of-step mass after a second collision (else exits)
+// k_batch_* run the same stage bodies for a batch of clouds, one launch per
+// stage over all of them (a block finds its cloud from block offsets).
 // The stored state h is the true distribution divided by StepScalars::scale.
 // All reductions are FP64 and in a fixed order, so a step is bitwise
 // reproducible.  No kernel waits on another block, so none can hang.
