@@ -379,7 +379,11 @@ int alebgk_set_coeff_builder(int which);
  * state, mesh velocity, neighbour lists and tables are replaced, the
  * distribution, macros and mass bookkeeping stay on the device (cloud->g and
  * cloud->macro are not read).  For the body steps in which cloud management
- * leaves the particle set alone. */
+ * leaves the particle set alone.  Where the tables are solved on the device
+ * the refresh is in place: the stencil classes and slot lists are built on
+ * the device from the uploaded geometry and the context's buffers are kept
+ * (only tables that must grow are reallocated).  The context's captured
+ * step graphs are dropped, and a batch holding it rebuilds its own. */
 int alebgk_upload_geometry(alebgk_ctx *ctx, const alebgk_cloud *cloud, double dt);
 
 /* Neighbour lists of the context's current device positions (body surface
