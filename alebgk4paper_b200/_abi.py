@@ -155,6 +155,14 @@ SIGNATURES = {
     "alebgk_slab_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "alebgk_slab_sync": (ctypes.c_int, [ctypes.c_void_p]),
     "alebgk_slab_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "alebgk_rank_slab_init": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int, c_double_p]),
+    "alebgk_rank_slab_segment": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p]),
+    "alebgk_rank_slab_combine": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                                c_double_p]),
+    "alebgk_rank_slab_rows": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_void_p, c_double_p, ctypes.c_int]),
+    "alebgk_rank_slab_finish": (ctypes.c_int, [ctypes.c_void_p]),
     "alebgk_neighbours_device": (ctypes.c_int, [ctypes.c_void_p, c_double_p, c_int_p, c_int_p,
                                                 c_int_p]),
     "alebgk_manage_cloud": (ctypes.c_int, [ctypes.c_int, c_double_p, c_int_p, ctypes.c_int,

@@ -47,7 +47,7 @@ void freeBuffers(alebgk_ctx *c)
     void *ptrs[] = {d.f[0], d.f[1], d.coef, d.coefLin, d.pos, d.meshv, d.wall,
                     d.boundary, d.bodyId, d.cls, d.nslot, d.slots, d.macro[0],
                     d.macro[1], d.mood, d.flag, d.flagList, d.degList, d.massPos, d.massEnd, d.minG, d.nad, d.redPartial,
-                    d.dpx, d.bodyTmp, d.bodyOut, d.stage, d.surfList, d.bodyIO, d.sc};
+                    d.dpx, d.bodyTmp, d.bodyOut, d.stage, d.surfList, d.bodyIO, d.rankAll, d.sc};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     d = DeviceBuffers();

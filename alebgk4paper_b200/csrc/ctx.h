@@ -71,6 +71,8 @@ struct DeviceBuffers
     double *stage = nullptr;           // N x gs FP64 host-transfer staging
     int *surfList = nullptr;           // body-surface particles (boundary, bodyId >= 0)
     double *bodyIO = nullptr;          // body-step staging: kBodyIOHead + 13 per surface particle
+    double *rankAll = nullptr;         // multi-process slab: every rank's 4 combine words
+    int rankAllCap = 0;                // ranks rankAll holds
     StepScalars *sc = nullptr;
 };
 
@@ -179,6 +181,11 @@ void freeBatchLaunch(BatchLaunch &bl);
 cudaError_t launchSlabSegment(alebgk_ctx *c, int from, int seg, cudaStream_t st);
 cudaError_t launchSlabCombine(StepScalars *const *scs, int n, int phase, cudaStream_t st);
 cudaError_t launchSlabInitSum(alebgk_ctx *c, cudaStream_t st);
+// One slab of a multi-process run: the combine of the slab group for this
+// slab alone, from every rank's words all[4 r + q] (slabPart[q], q < 3, and
+// moodfail at q = 3) in rank order (step.cu).
+cudaError_t launchRankCombine(alebgk_ctx *c, const double *allDev, int n, int phase,
+                              cudaStream_t st);
 struct CaseParams;
 // Device arrays of the lattice set-up (setup.cu).
 struct LatticeDev

@@ -13,6 +13,14 @@
 // 405-466) by one copy per ghost block.  Contexts on different devices read
 // each other's scalars and rows over peer access (NVLink); the combine runs
 // on the first slab's device.
+//
+// Multi-process runs (alebgk_rank_slab_*): each process holds one slab.  The
+// host runs a segment, reads the slab's four combine words (owned-range
+// partial sums and the moodCheck flag), exchanges them with the other ranks
+// (an all-gather in rank order, MPI_Allgather in the reference), and hands
+// every rank's words back; the combine kernel then applies, for this slab,
+// exactly what the single-process combine writes.  Ghost rows travel
+// through host buffers between the last segment and the end of the step.
 #include <cuda_runtime.h>
 
 #include <string>
@@ -223,6 +231,102 @@ int alebgk_slab_step(alebgk_slab *g, int nsteps)
             ++x->hostSteps;
         }
     }
+    return ALEBGK_OK;
+}
+
+int alebgk_rank_slab_init(alebgk_ctx *c, int nranks, int own_lo, int own_hi, double *words)
+{
+    if (!c || !words || nranks < 1) return ALEBGK_EINVAL;
+    if (!c->uploaded) return failS(c, ALEBGK_ESTATE, "upload the slab first");
+    if (own_lo < 0 || own_hi <= own_lo || own_hi > c->sp.N)
+        return failS(c, ALEBGK_EINVAL, "owned range out of bounds");
+    for (int b : c->bodyIdHost)
+        if (b >= 0) return failS(c, ALEBGK_EINVAL, "slabs take clouds without bodies");
+    CKS(cudaSetDevice(c->cfg.device));
+    CKS(cudaStreamSynchronize(c->stream));
+    DeviceBuffers &d = c->d;
+    if (d.rankAllCap < nranks)
+    {
+        if (d.rankAll) cudaFree(d.rankAll);
+        d.rankAll = nullptr;
+        d.rankAllCap = 0;
+        CKS(cudaMalloc(&d.rankAll, 32 * (size_t)nranks));
+        d.rankAllCap = nranks;
+    }
+    c->sp.ownLo = own_lo;
+    c->sp.ownHi = own_hi;
+    for (auto &gr : c->graph)
+        if (gr) { cudaGraphExecDestroy(gr); gr = nullptr; }
+    CKS(launchSlabInitSum(c, c->stream));
+    StepScalars sc{};
+    CKS(cudaMemcpyAsync(&sc, d.sc, sizeof sc, cudaMemcpyDeviceToHost, c->stream));
+    CKS(cudaStreamSynchronize(c->stream));
+    for (int q = 0; q < 3; ++q) words[q] = sc.slabPart[q];
+    words[3] = sc.moodfail;
+    return ALEBGK_OK;
+}
+
+int alebgk_rank_slab_segment(alebgk_ctx *c, int seg, double *words)
+{
+    if (!c || !words || seg < 0 || seg > 3) return ALEBGK_EINVAL;
+    if (c->sp.ownHi <= c->sp.ownLo || c->d.rankAllCap < 1)
+        return failS(c, ALEBGK_ESTATE, "alebgk_rank_slab_init first");
+    CKS(cudaSetDevice(c->cfg.device));
+    CKS(launchSlabSegment(c, c->cur, seg, c->stream));
+    StepScalars sc{};
+    CKS(cudaMemcpyAsync(&sc, c->d.sc, sizeof sc, cudaMemcpyDeviceToHost, c->stream));
+    CKS(cudaStreamSynchronize(c->stream));
+    for (int q = 0; q < 3; ++q) words[q] = sc.slabPart[q];
+    words[3] = sc.moodfail;
+    return ALEBGK_OK;
+}
+
+int alebgk_rank_slab_combine(alebgk_ctx *c, int phase, int nranks, const double *all)
+{
+    if (!c || !all || phase < 0 || phase > 4 || nranks < 1) return ALEBGK_EINVAL;
+    if (nranks > c->d.rankAllCap)
+        return failS(c, ALEBGK_EINVAL, "more ranks than alebgk_rank_slab_init was given");
+    CKS(cudaSetDevice(c->cfg.device));
+    CKS(cudaMemcpyAsync(c->d.rankAll, all, 32 * (size_t)nranks, cudaMemcpyHostToDevice,
+                        c->stream));
+    CKS(launchRankCombine(c, c->d.rankAll, nranks, phase, c->stream));
+    CKS(cudaStreamSynchronize(c->stream));
+    return ALEBGK_OK;
+}
+
+int alebgk_rank_slab_rows(alebgk_ctx *c, int start, int count, void *f_rows,
+                          double *macro_rows, int put)
+{
+    if (!c || !f_rows || !macro_rows || count < 1 || start < 0) return ALEBGK_EINVAL;
+    if (!c->uploaded || start + count > c->sp.N)
+        return failS(c, ALEBGK_EINVAL, "rows out of bounds");
+    CKS(cudaSetDevice(c->cfg.device));
+    CKS(cudaStreamSynchronize(c->stream));
+    const int buf = 1 - c->cur;        // the state the step in progress writes
+    const size_t es = (c->cfg.precision == 64) ? 8 : 4;
+    const size_t row = (size_t)c->sp.ldf * es;
+    char *f = static_cast<char *>(c->d.f[buf]) + row * start;
+    double *m = c->d.macro[buf] + 6 * (size_t)start;
+    if (put)
+    {
+        CKS(cudaMemcpy(f, f_rows, row * count, cudaMemcpyHostToDevice));
+        CKS(cudaMemcpy(m, macro_rows, 48 * (size_t)count, cudaMemcpyHostToDevice));
+    }
+    else
+    {
+        CKS(cudaMemcpy(f_rows, f, row * count, cudaMemcpyDeviceToHost));
+        CKS(cudaMemcpy(macro_rows, m, 48 * (size_t)count, cudaMemcpyDeviceToHost));
+    }
+    return ALEBGK_OK;
+}
+
+int alebgk_rank_slab_finish(alebgk_ctx *c)
+{
+    if (!c) return ALEBGK_EINVAL;
+    CKS(cudaSetDevice(c->cfg.device));
+    CKS(cudaStreamSynchronize(c->stream));
+    c->cur = 1 - c->cur;
+    ++c->hostSteps;
     return ALEBGK_OK;
 }
 

@@ -1514,6 +1514,57 @@ __global__ void k_slab_combine(StepScalars *const *scs, int n, int phase)
     }
 }
 
+// One slab of a multi-process slab run: k_slab_combine's arithmetic for
+// this slab alone.  The totals add every rank's word in rank order, as
+// k_slab_combine adds the slabs; massOld, sigma and moodfail are the same in
+// every slab when a phase starts, so the slab's own copies stand in for
+// slab 0's.
+__global__ void k_rank_combine(StepScalars *sc, const double *__restrict__ all, int n, int phase)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    auto total = [&](int q) {
+        double m = 0.0;
+        for (int i = 0; i < n; ++i) m += all[4 * i + q];
+        return m;
+    };
+    if (phase == 0)
+    {
+        const double m = total(0);
+        sc->sigma = (m > 1.0e-30) ? sc->massOld / m : 1.0;
+        sc->massNew = m;
+    }
+    else if (phase == 1)
+    {
+        const double sigma = sc->sigma;
+        const double me = sigma * total(1);
+        sc->massEnd = me;
+        sc->massOld = me;
+        sc->scale = sigma;
+        sc->steps += 1;
+    }
+    else if (phase == 2)
+    {
+        int f = 0;
+        for (int i = 0; i < n; ++i) f |= all[4 * i + 3] != 0.0;
+        sc->moodfail = f;
+    }
+    else if (phase == 3)
+    {
+        if (sc->moodfail == 0) return;
+        const double me = sc->sigma * total(2);
+        sc->massEnd = me;
+        sc->massOld = me;
+    }
+    else
+    {
+        const double m = total(1);
+        sc->massOld = m;
+        sc->massEnd = m;
+        sc->scale = 1.0;
+        sc->sigma = 1.0;
+    }
+}
+
 // Resets the step's counters; with a NAD range buffer also computes the
 // neighbour density ranges of the streamed particle kernel.
 __global__ void __launch_bounds__(kNT)
@@ -2344,6 +2395,13 @@ cudaError_t launchSlabSegment(alebgk_ctx *c, int from, int seg, cudaStream_t st)
 cudaError_t launchSlabCombine(StepScalars *const *scs, int n, int phase, cudaStream_t st)
 {
     k_slab_combine<<<1, 32, 0, st>>>(scs, n, phase);
+    return cudaGetLastError();
+}
+
+cudaError_t launchRankCombine(alebgk_ctx *c, const double *allDev, int n, int phase,
+                              cudaStream_t st)
+{
+    k_rank_combine<<<1, 32, 0, st>>>(c->d.sc, allDev, n, phase);
     return cudaGetLastError();
 }
 

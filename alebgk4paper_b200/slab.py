@@ -18,9 +18,9 @@ import math
 import numpy as np
 
 from . import _abi
-from . import Case, Solver, _check
+from . import Case, Solver, _check, _dp
 
-__all__ = ["plan_slabs", "SlabGroup"]
+__all__ = ["plan_slabs", "SlabGroup", "RankSlab", "rank_halo_plan"]
 
 
 def _rows(case):
@@ -159,3 +159,134 @@ class SlabGroup:
             self.close()
         except Exception:
             pass
+
+
+def rank_halo_plan(plan: dict, rank: int):
+    """This rank's part of the ghost copies: (sends, receives), each a list
+    of (peer rank, local start, count) -- sends read the rank's own rows,
+    receives write its ghost rows (MpiExchange.cpp:405-466)."""
+    sends, recvs = [], []
+    for dst, dst_start, src, src_start, count in plan["copies"]:
+        if src == rank:
+            sends.append((dst, src_start, count))
+        if dst == rank:
+            recvs.append((src, dst_start, count))
+    return sends, recvs
+
+
+class RankSlab:
+    """One slab of a lattice cavity per process of a ``torch.distributed``
+    group: the reference's MPI decomposed mode (Solver/MpiExchange.cpp:
+    199-466).  Rank r steps slab r of ``plan_slabs(case, world)``.  Between
+    the four segments of a step the slabs' combine words (owned-range partial
+    sums and the moodCheck flag) are all-gathered in rank order
+    (MomentCalculations/Conservation.cpp:33-36,76-84); after the last
+    segment the ghost rows are exchanged with the neighbouring ranks.  The
+    combine is the single-process slab group's, so the run gives that
+    group's state.  The exchanges go through host buffers, as CPU tensors for
+    ``gloo`` and as device tensors for ``nccl``.
+
+    ``lib`` and ``solver_factory`` default to the compiled library and
+    :class:`Solver`; tests replace them."""
+
+    def __init__(self, case, precision: int = 32, device: int = 0, group=None, lib=None,
+                 solver_factory=None):
+        import torch.distributed as dist
+        self.dist = dist
+        self.group = group
+        self.rank = dist.get_rank(group)
+        self.world = dist.get_world_size(group)
+        self.plan = plan_slabs(case, self.world)
+        st = self.plan["stride"]
+        sl = self.plan["slabs"][self.rank]
+        self.sub = _SlabCase(case, sl["k0"], sl["k1"], st)
+        self.lib = lib or _abi.load()
+        make = solver_factory or (lambda c: Solver(c, precision=precision, device=device))
+        self.solver = make(self.sub)
+        self.ctx = self.solver.ctx
+        self.own = sl["own"]
+        self.sends, self.recvs = rank_halo_plan(self.plan, self.rank)
+        ldf, es = ctypes.c_int(), ctypes.c_int()
+        _check(self.lib.alebgk_device_state(self.ctx, None, ctypes.byref(ldf), ctypes.byref(es)),
+               self.ctx)
+        self.row_bytes = ldf.value * es.value
+        self.device = device
+        words = np.zeros(4)
+        _check(self.lib.alebgk_rank_slab_init(self.ctx, self.world, int(self.own[0]),
+                                              int(self.own[1]), _dp(words)), self.ctx)
+        self._combine(4, words)
+        self.steps = 0
+
+    def _nccl(self) -> bool:
+        return self.dist.get_backend(self.group) == "nccl"
+
+    def _tensor(self, a):
+        import torch
+        t = torch.from_numpy(np.ascontiguousarray(a))
+        return t.cuda(self.device) if self._nccl() else t
+
+    def _combine(self, phase: int, words: np.ndarray):
+        import torch
+        mine = self._tensor(words.astype(np.float64))
+        out = [torch.zeros_like(mine) for _ in range(self.world)]
+        self.dist.all_gather(out, mine, group=self.group)
+        allw = np.concatenate([o.cpu().numpy() for o in out]).astype(np.float64)
+        _check(self.lib.alebgk_rank_slab_combine(self.ctx, int(phase), self.world, _dp(allw)),
+               self.ctx)
+
+    def _rows(self, start: int, count: int, f=None, m=None, put: bool = False):
+        if f is None:
+            f = np.zeros(count * self.row_bytes, np.uint8)
+            m = np.zeros(count * 6)
+        _check(self.lib.alebgk_rank_slab_rows(self.ctx, int(start), int(count),
+                                              f.ctypes.data_as(ctypes.c_void_p), _dp(m),
+                                              1 if put else 0), self.ctx)
+        return f, m
+
+    def _halo(self):
+        """Ghost rows of the state being written, from their owners."""
+        import torch
+        reqs, inbox = [], []
+        for peer, start, count in self.recvs:
+            f = self._tensor(np.zeros(count * self.row_bytes, np.uint8))
+            m = self._tensor(np.zeros(count * 6))
+            reqs += [self.dist.irecv(f, peer, group=self.group),
+                     self.dist.irecv(m, peer, group=self.group)]
+            inbox.append((start, count, f, m))
+        keep = []
+        for peer, start, count in self.sends:
+            f, m = self._rows(start, count)
+            tf, tm = self._tensor(f), self._tensor(m)
+            keep.append((tf, tm))
+            reqs += [self.dist.isend(tf, peer, group=self.group),
+                     self.dist.isend(tm, peer, group=self.group)]
+        for r in reqs:
+            r.wait()
+        for start, count, f, m in inbox:
+            fh = np.ascontiguousarray(f.cpu().numpy())
+            mh = np.ascontiguousarray(m.cpu().numpy()).astype(np.float64)
+            self._rows(start, count, fh, mh, put=True)
+        del keep, torch
+
+    def step(self, n: int = 1):
+        for _ in range(int(n)):
+            for seg in range(4):
+                words = np.zeros(4)
+                _check(self.lib.alebgk_rank_slab_segment(self.ctx, seg, _dp(words)), self.ctx)
+                self._combine(seg, words)
+            self._halo()
+            _check(self.lib.alebgk_rank_slab_finish(self.ctx), self.ctx)
+            self.steps += 1
+
+    def owned(self):
+        """This rank's owned rows of (g, macro) and their global row range."""
+        g, m = self.solver.cudaDownloadFull()
+        lo, hi = self.own
+        sl = self.plan["slabs"][self.rank]
+        st = self.plan["stride"]
+        return g[lo:hi], m[lo:hi], (sl["r0"] * st, sl["r1"] * st)
+
+    def close(self):
+        if getattr(self, "solver", None) is not None:
+            self.solver.close()
+            self.solver = None

@@ -433,6 +433,29 @@ int alebgk_slab_step(alebgk_slab *g, int nsteps);
 int alebgk_slab_sync(alebgk_slab *g);
 int alebgk_slab_destroy(alebgk_slab *g);
 
+/* Multi-process slab runs: one slab per process, the reference's decomposed
+ * mode with its MPI exchanges (Solver/MpiExchange.cpp:199-466,
+ * MomentCalculations/Conservation.cpp:33-36,76-84) left to the host's
+ * collectives.  Each rank uploads its slab (owned rows plus ghost rows, as
+ * for alebgk_slab_create) and then:
+ *   init(nranks, own range, words): the owned mass; all-gather the 4 words
+ *     in rank order and pass them to combine(phase 4);
+ *   per step, for seg = 0..3: segment(seg, words); all-gather; combine(seg);
+ *   then the ghost rows of the state being written: rows(get) of the owned
+ *     rows a neighbour needs, exchange, rows(put) into the ghost rows;
+ *   finish(): the step's state becomes current.
+ * words = the slab's owned-range partial sums (3) and its moodCheck flag;
+ * all = nranks x 4 words in rank order.  rows moves `count` rows of f (the
+ * storage type, ldf values each) and of the macros (6 doubles each) of the
+ * state the step in progress writes.  The arithmetic of the combine is the
+ * single-process slab group's, so both runs give the same state. */
+int alebgk_rank_slab_init(alebgk_ctx *ctx, int nranks, int own_lo, int own_hi, double *words);
+int alebgk_rank_slab_segment(alebgk_ctx *ctx, int seg, double *words);
+int alebgk_rank_slab_combine(alebgk_ctx *ctx, int phase, int nranks, const double *all);
+int alebgk_rank_slab_rows(alebgk_ctx *ctx, int start, int count, void *f_rows,
+                          double *macro_rows, int put);
+int alebgk_rank_slab_finish(alebgk_ctx *ctx);
+
 /* ---- restart files ------------------------------------------------------
  * The reference's checkpoint layout (Core/Checkpoint.hpp:37-236, magic
  * "ALEBGK01", version 1): header, one record per particle, N*gStride FP64
