@@ -51,3 +51,30 @@ def test_owned_particles_keep_their_whole_stencil(name, Nx, n):
             assert sc.nnb[i] == c.nnb[gi]
             assert np.array_equal(sc.nbr[i, :sc.nnb[i]] + base, c.nbr[gi, :c.nnb[gi]])
         assert np.array_equal(sc.xyz, c.xyz[base:base + sc.N])
+
+
+@pytest.mark.parametrize("name,kw,n", [("cavity2d", dict(Nx=33, Nv=4), 3),
+                                       ("cavity3d", dict(Nx=24, Nv=4), 2),
+                                       ("cavity2d", dict(Nx=48, Nv=4), 4)])
+def test_rank_halo_plan_pairs_every_send_with_a_receive(name, kw, n):
+    """Per rank, the ghost copies split into sends (own rows to a neighbour)
+    and receives (ghost rows from a neighbour); over all ranks every copy is
+    one send and one receive of the same size, sends read owned rows and
+    receives write ghost rows only."""
+    from alebgk4paper_b200.slab import rank_halo_plan
+    case = Case(name, **kw)
+    plan = plan_slabs(case, n)
+    sends, recvs = {}, {}
+    for r in range(n):
+        s, v = rank_halo_plan(plan, r)
+        lo, hi = plan["slabs"][r]["own"]
+        for peer, start, count in s:
+            assert lo <= start and start + count <= hi
+            sends.setdefault((r, peer), []).append(count)
+        for peer, start, count in v:
+            assert start + count <= lo or start >= hi
+            recvs.setdefault((peer, r), []).append(count)
+        # neighbours only
+        assert all(abs(peer - r) == 1 for peer, _, _ in s + v)
+    assert sends == recvs
+    assert sum(len(x) for x in sends.values()) == len(plan["copies"]) == 2 * (n - 1)
