@@ -307,16 +307,23 @@ int alebgk_rank_slab_rows(alebgk_ctx *c, int start, int count, void *f_rows,
     const size_t row = (size_t)c->sp.ldf * es;
     char *f = static_cast<char *>(c->d.f[buf]) + row * start;
     double *m = c->d.macro[buf] + 6 * (size_t)start;
+    // The copies run on the context's own (non-blocking) stream and are
+    // waited for before returning: a pageable host-to-device copy may return
+    // before its DMA has landed, and the next step's kernels on this stream
+    // must see the ghost rows.
     if (put)
     {
-        CKS(cudaMemcpy(f, f_rows, row * count, cudaMemcpyHostToDevice));
-        CKS(cudaMemcpy(m, macro_rows, 48 * (size_t)count, cudaMemcpyHostToDevice));
+        CKS(cudaMemcpyAsync(f, f_rows, row * count, cudaMemcpyHostToDevice, c->stream));
+        CKS(cudaMemcpyAsync(m, macro_rows, 48 * (size_t)count, cudaMemcpyHostToDevice,
+                            c->stream));
     }
     else
     {
-        CKS(cudaMemcpy(f_rows, f, row * count, cudaMemcpyDeviceToHost));
-        CKS(cudaMemcpy(macro_rows, m, 48 * (size_t)count, cudaMemcpyDeviceToHost));
+        CKS(cudaMemcpyAsync(f_rows, f, row * count, cudaMemcpyDeviceToHost, c->stream));
+        CKS(cudaMemcpyAsync(macro_rows, m, 48 * (size_t)count, cudaMemcpyDeviceToHost,
+                            c->stream));
     }
+    CKS(cudaStreamSynchronize(c->stream));
     return ALEBGK_OK;
 }
 

@@ -244,23 +244,29 @@ class RankSlab:
         return f, m
 
     def _halo(self):
-        """Ghost rows of the state being written, from their owners."""
+        """Ghost rows of the state being written, from their owners.
+
+        Every receive and send of the exchange is posted in one
+        batch_isend_irecv call.  Under NCCL that call groups the point-to-point
+        operations, so two ranks that each receive from and send to the other
+        cannot deadlock on the order in which their operations were queued on
+        the communicator's stream; under gloo it posts them one by one."""
         import torch
-        reqs, inbox = [], []
+        ops, inbox, keep = [], [], []
+        P2POp = self.dist.P2POp
         for peer, start, count in self.recvs:
             f = self._tensor(np.zeros(count * self.row_bytes, np.uint8))
             m = self._tensor(np.zeros(count * 6))
-            reqs += [self.dist.irecv(f, peer, group=self.group),
-                     self.dist.irecv(m, peer, group=self.group)]
+            ops += [P2POp(self.dist.irecv, f, peer, self.group),
+                    P2POp(self.dist.irecv, m, peer, self.group)]
             inbox.append((start, count, f, m))
-        keep = []
         for peer, start, count in self.sends:
             f, m = self._rows(start, count)
             tf, tm = self._tensor(f), self._tensor(m)
             keep.append((tf, tm))
-            reqs += [self.dist.isend(tf, peer, group=self.group),
-                     self.dist.isend(tm, peer, group=self.group)]
-        for r in reqs:
+            ops += [P2POp(self.dist.isend, tf, peer, self.group),
+                    P2POp(self.dist.isend, tm, peer, self.group)]
+        for r in (self.dist.batch_isend_irecv(ops) if ops else []):
             r.wait()
         for start, count, f, m in inbox:
             fh = np.ascontiguousarray(f.cpu().numpy())

@@ -62,6 +62,11 @@ def test_rank_slabs_equal_the_slab_group(gpu, name, kw, precision):
             p.start()
         for p in procs:
             p.join(300)
+        # a worker stuck in a collective would otherwise outlive the test
+        for p in procs:
+            if p.is_alive():
+                p.terminate()
+                p.join(30)
         assert all(p.exitcode == 0 for p in procs)
         res = dict(out)
     group = SlabGroup(Case(name, **kw), world, precision=precision)

@@ -132,6 +132,11 @@ def test_rank_slab_exchanges_on_two_gloo_ranks():
             p.start()
         for p in procs:
             p.join(120)
+        # a worker stuck in a collective would otherwise outlive the test
+        for p in procs:
+            if p.is_alive():
+                p.terminate()
+                p.join(30)
         assert all(p.exitcode == 0 for p in procs)
         res = dict(out)
     for rank in (0, 1):
@@ -156,3 +161,61 @@ def test_rank_slab_exchanges_on_two_gloo_ranks():
         for i in range(n):
             assert (r["f"][i] == (base + i + 7 * step) % 251).all(), (rank, i)
             assert (r["m"][i] == base + i + 1000.0 * step).all(), (rank, i)
+
+
+class _RecordingDist:
+    """Stands in for torch.distributed under an NCCL group: records how the
+    ghost-row exchange posts its point-to-point operations."""
+
+    class P2POp:
+        def __init__(self, op, tensor, peer, group=None):
+            self.op, self.tensor, self.peer, self.group = op, tensor, peer, group
+
+    class _Work:
+        def wait(self):
+            return True
+
+    def __init__(self):
+        self.batches, self.direct = [], 0
+
+    def get_backend(self, group=None):
+        return "nccl"
+
+    def irecv(self, *a, **k):
+        self.direct += 1
+        return self._Work()
+
+    def isend(self, *a, **k):
+        self.direct += 1
+        return self._Work()
+
+    def batch_isend_irecv(self, ops):
+        self.batches.append([(o.op.__name__, o.peer) for o in ops])
+        return [self._Work() for _ in ops]
+
+
+def test_nccl_ghost_exchange_is_one_batched_call():
+    """Under NCCL every receive and send of a step's ghost-row exchange goes
+    through a single batch_isend_irecv call (grouped point-to-point), never
+    as separately queued isend/irecv, which can deadlock two ranks that
+    exchange with each other."""
+    import torch
+    from alebgk4paper_b200.slab import RankSlab
+    rs = RankSlab.__new__(RankSlab)
+    rs.dist = _RecordingDist()
+    rs.group = None
+    rs.ctx = ctypes.c_void_p(1)
+    rs.row_bytes = ROW_BYTES
+    rs.device = 0
+    rs.recvs = [(0, 10, 3), (2, 40, 3)]
+    rs.sends = [(0, 13, 3), (2, 37, 3)]
+    lib = _FakeLib(1, 0, 50)
+    lib.own = (13, 40)
+    rs.lib = lib
+    rs._tensor = lambda a: torch.from_numpy(np.ascontiguousarray(a))
+    rs._halo()
+    assert rs.dist.direct == 0
+    assert len(rs.dist.batches) == 1
+    ops = rs.dist.batches[0]
+    assert sorted(ops) == sorted([("irecv", 0)] * 2 + [("irecv", 2)] * 2 +
+                                 [("isend", 0)] * 2 + [("isend", 2)] * 2)
