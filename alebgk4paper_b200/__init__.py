@@ -457,6 +457,10 @@ class Solver:
         _check(self.lib.alebgk_set_launch(self.ctx, int(transport_threads), int(particle_warps)),
                self.ctx)
 
+    def set_march_width(self, velocities_per_lane: int):
+        """Velocities per lane of the lattice march (2: packed FMAs, or 1)."""
+        _check(self.lib.alebgk_set_march_width(self.ctx, int(velocities_per_lane)), self.ctx)
+
     def get_launch(self):
         t = ctypes.c_int()
         w = ctypes.c_int()

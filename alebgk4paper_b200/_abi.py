@@ -99,6 +99,7 @@ SIGNATURES = {
     "alebgk_case_body_shapes": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p, c_double_p]),
     "alebgk_set_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "alebgk_get_launch": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p]),
+    "alebgk_set_march_width": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "alebgk_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_float)]),
     "alebgk_residual": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),

@@ -47,6 +47,7 @@ void freeBuffers(alebgk_ctx *c)
     void *ptrs[] = {d.f[0], d.f[1], d.coef, d.coefLin, d.pos, d.meshv, d.wall,
                     d.boundary, d.bodyId, d.cls, d.nslot, d.slots, d.macro[0],
                     d.macro[1], d.mood, d.flag, d.flagList, d.degList, d.massPos, d.massEnd, d.minG, d.nad, d.redPartial,
+                    d.rowSums, d.rowTab, d.rowKind,
                     d.dpx, d.bodyTmp, d.bodyOut, d.stage, d.surfList, d.bodyIO, d.rankAll, d.sc};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -57,6 +58,7 @@ void freeBuffers(alebgk_ctx *c)
     if (c->march.units) cudaFree(c->march.units);
     if (c->march.coefT) cudaFree(c->march.coefT);
     if (c->march.coefTy) cudaFree(c->march.coefTy);
+    if (c->march.gather) cudaFree(c->march.gather);
     c->march = MarchState();
     for (auto &g : c->graph)
         if (g) { cudaGraphExecDestroy(g); g = nullptr; }
@@ -82,8 +84,10 @@ int alebgk_create(const alebgk_config *cfg, alebgk_ctx **out)
         return fail(nullptr, ALEBGK_EINVAL, "mls_order must be 1 or 2");
     if (cfg->limiter != 0 && cfg->limiter != 2)
         return fail(nullptr, ALEBGK_EINVAL, "limiter must be 0 (none) or 2 (MOOD)");
-    if (cfg->transport < 0 || cfg->transport > 2 || cfg->particle < 0 || cfg->particle > 2)
-        return fail(nullptr, ALEBGK_EINVAL, "transport and particle selectors are 0, 1 or 2");
+    if (cfg->transport < 0 || cfg->transport > 2)
+        return fail(nullptr, ALEBGK_EINVAL, "the transport selector is 0, 1 or 2");
+    if (cfg->particle < 0 || cfg->particle > 3)
+        return fail(nullptr, ALEBGK_EINVAL, "the particle selector is 0, 1, 2 or 3");
     if (!(cfg->tau > 0) || !(cfg->R > 0) || !(cfg->dv > 0) || !(cfg->radius > 0))
         return fail(nullptr, ALEBGK_EINVAL, "tau, R, dv and radius must be > 0");
     const int gs = (cfg->dim == 3) ? cfg->Nv * cfg->Nv * cfg->Nv : 2 * cfg->Nv * cfg->Nv;
@@ -311,6 +315,10 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
     CK(dalloc(&d.massEnd, N));
     CK(dalloc(&d.minG, N));
     CK(dalloc(&d.nad, 2 * (size_t)N));
+    p.tabStride = (3 * p.Nv + 2 + 3) / 4 * 4;
+    CK(dalloc(&d.rowSums, 6 * (size_t)N));
+    CK(dalloc(&d.rowTab, (size_t)N * p.tabStride));
+    CK(dalloc(&d.rowKind, N));
     CK(dalloc(&d.redPartial, 256));
     CK(dalloc(&d.dpx, N));
     CK(dalloc(&d.bodyTmp, 6 * (size_t)N));
@@ -344,7 +352,7 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
     CK(cudaMemset(d.dpx, 0, 8 * (size_t)N));
     CK(cudaMemset(d.sc, 0, sizeof(StepScalars)));
     CK(prepareKernels(c));
-    if (c->cfg.particle == 2 && !c->pStream)
+    if ((c->cfg.particle == 2 || c->cfg.particle == 3) && !c->pStream)
         return fail(c, ALEBGK_EINVAL,
                     "the streamed particle kernel needs a 3-D cloud whose rows fit in "
                     "shared memory");
@@ -358,6 +366,7 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
         if (plan.ok)
         {
             MarchState &m = c->march;
+            m.vpl = c->tune.marchVpl;
             // one list, the long y-march units first
             std::vector<MarchUnit> all(plan.unitsY);
             all.insert(all.end(), plan.units.begin(), plan.units.end());
@@ -367,6 +376,13 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
             CK(cudaMalloc(&m.units, sizeof(MarchUnit) * m.nunits));
             CK(cudaMemcpy(m.units, all.data(), sizeof(MarchUnit) * m.nunits,
                           cudaMemcpyHostToDevice));
+            m.ngather = (int)plan.gatherList.size();
+            if (m.ngather > 0)
+            {
+                CK(cudaMalloc(&m.gather, 4 * (size_t)m.ngather));
+                CK(cudaMemcpy(m.gather, plan.gatherList.data(), 4 * (size_t)m.ngather,
+                              cudaMemcpyHostToDevice));
+            }
             CK(cudaMalloc(&m.coefT, plan.coefT.size() * 4));
             CK(cudaMemcpy(m.coefT, plan.coefT.data(), plan.coefT.size() * 4,
                           cudaMemcpyHostToDevice));
@@ -378,10 +394,12 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
             }
             for (int b = 0; b < 2; ++b)
             {
-                if (!encodeMarchMap(m.tmap[b], d.f[b], p.V, m.Nx, m.Ny, m.Nz, p.ldf, false, &err))
+                if (!encodeMarchMap(m.tmap[b], d.f[b], p.V, m.Nx, m.Ny, m.Nz, p.ldf, false,
+                                    m.vpl, &err))
                     return fail(c, ALEBGK_ECUDA, err);
                 if (m.nunitsY > 0 &&
-                    !encodeMarchMap(m.tmapY[b], d.f[b], p.V, m.Nx, m.Ny, m.Nz, p.ldf, true, &err))
+                    !encodeMarchMap(m.tmapY[b], d.f[b], p.V, m.Nx, m.Ny, m.Nz, p.ldf, true,
+                                    m.vpl, &err))
                     return fail(c, ALEBGK_ECUDA, err);
             }
             CK(prepareMarch());
@@ -392,6 +410,8 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
         return fail(c, ALEBGK_EINVAL,
                     "the lattice march needs FP32 and a complete 3-D lattice cloud");
     c->bodyIdHost.assign(cl->body_id, cl->body_id + N);
+    c->maxBodyId = -1;
+    for (int b : c->bodyIdHost) c->maxBodyId = std::max(c->maxBodyId, b);
     c->boundaryHost.assign(cl->boundary, cl->boundary + N);
     c->cur = 0;
     c->uploaded = true;
@@ -528,6 +548,8 @@ int refreshGeometryInPlace(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
     if (c->macSnap) { cudaFree(c->macSnap); c->macSnap = nullptr; }
     c->snapSteps = -1;
     c->bodyIdHost.assign(cl->body_id, cl->body_id + N);
+    c->maxBodyId = -1;
+    for (int b : c->bodyIdHost) c->maxBodyId = std::max(c->maxBodyId, b);
     c->boundaryHost.assign(cl->boundary, cl->boundary + N);
     c->geometryDirty = false;
     ++c->epoch;
@@ -816,7 +838,7 @@ int alebgk_get_counters(alebgk_ctx *c, alebgk_counters *out)
     out->mass_before = s.sigma * s.massNew;
     out->error_word = s.err;
     out->transport_kernel = c->march.enabled ? 2 : 1;
-    out->particle_kernel = c->pStream ? 2 : 1;
+    out->particle_kernel = c->pStream ? (c->pSplit ? 3 : 2) : 1;
     return ALEBGK_OK;
 }
 
@@ -858,9 +880,8 @@ int alebgk_body_loads(alebgk_ctx *c, int nbodies, const double *centre,
     if (!c || !centre || !area || !out) return fail(c, ALEBGK_EINVAL, "null argument");
     if (nbodies <= 0 || nbodies > 64) return fail(c, ALEBGK_EINVAL, "1..64 bodies");
     if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
-    for (int i = 0; i < c->sp.N; ++i)
-        if (c->bodyIdHost[i] >= nbodies)
-            return fail(c, ALEBGK_EINVAL, "a particle's body id exceeds nbodies");
+    if (c->maxBodyId >= nbodies)
+        return fail(c, ALEBGK_EINVAL, "a particle's body id exceeds nbodies");
     CK(cudaSetDevice(c->cfg.device));
     double *dc = nullptr;
     CK(cudaMalloc(&dc, 4 * 64 * sizeof(double)));
@@ -887,9 +908,8 @@ int alebgk_body_loads_noalloc(alebgk_ctx *c, int nbodies, const double *centre,
                         std::to_string(ALEBGK_NOALLOC_MAX_BODIES) + " bodies, got " +
                         std::to_string(nbodies));
     if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
-    for (int i = 0; i < c->sp.N; ++i)
-        if (c->bodyIdHost[i] >= nbodies)
-            return fail(c, ALEBGK_EINVAL, "a particle's body id exceeds nbodies");
+    if (c->maxBodyId >= nbodies)
+        return fail(c, ALEBGK_EINVAL, "a particle's body id exceeds nbodies");
     CK(cudaSetDevice(c->cfg.device));
     std::string err;
     if (alebgk::bodyLoadsNoAlloc(c, nbodies, centre, area, out, &err) != cudaSuccess)
@@ -903,9 +923,8 @@ int alebgk_body_set_surface_velocity(alebgk_ctx *c, int nbodies,
     if (!c || !centre || !state) return fail(c, ALEBGK_EINVAL, "null argument");
     if (nbodies <= 0 || nbodies > 64) return fail(c, ALEBGK_EINVAL, "1..64 bodies");
     if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
-    for (int i = 0; i < c->sp.N; ++i)
-        if (c->bodyIdHost[i] >= nbodies)
-            return fail(c, ALEBGK_EINVAL, "a particle's body id exceeds nbodies");
+    if (c->maxBodyId >= nbodies)
+        return fail(c, ALEBGK_EINVAL, "a particle's body id exceeds nbodies");
     CK(cudaSetDevice(c->cfg.device));
     double *dc = nullptr;
     CK(cudaMalloc(&dc, 9 * 64 * sizeof(double)));
@@ -935,9 +954,8 @@ int alebgk_body_step(alebgk_ctx *c, int nbodies, alebgk_body *bodies, const doub
         if (!(B.state[19] > 0) || !(B.state[20] > 0))
             return fail(c, ALEBGK_EINVAL, "body mass and moment of inertia must be > 0");
     }
-    for (int i = 0; i < c->sp.N; ++i)
-        if (c->bodyIdHost[i] >= nbodies)
-            return fail(c, ALEBGK_EINVAL, "a particle's body id exceeds nbodies");
+    if (c->maxBodyId >= nbodies)
+        return fail(c, ALEBGK_EINVAL, "a particle's body id exceeds nbodies");
     CK(cudaSetDevice(c->cfg.device));
     std::string err;
     const cudaError_t e = bodyStep(c, nbodies, bodies, box, dx, dt, &err);

@@ -138,6 +138,29 @@ int alebgk_set_launch(alebgk_ctx *c, int transport_threads, int particle_warps)
     return ALEBGK_OK;
 }
 
+int alebgk_set_march_width(alebgk_ctx *c, int velocities_per_lane)
+{
+    if (!c) return ALEBGK_EINVAL;
+    if (velocities_per_lane != 1 && velocities_per_lane != 2)
+        return failc(c, ALEBGK_EINVAL, "march width: 1 or 2 velocities per lane");
+    c->tune.marchVpl = velocities_per_lane;
+    MarchState &m = c->march;
+    if (!m.enabled || m.vpl == velocities_per_lane) return ALEBGK_OK;
+    m.vpl = velocities_per_lane;
+    const StepParams &p = c->sp;
+    std::string err;
+    for (int b = 0; b < 2; ++b)
+    {
+        if (!encodeMarchMap(m.tmap[b], c->d.f[b], p.V, m.Nx, m.Ny, m.Nz, p.ldf, false, m.vpl,
+                            &err) ||
+            (m.nunitsY > 0 && !encodeMarchMap(m.tmapY[b], c->d.f[b], p.V, m.Nx, m.Ny, m.Nz,
+                                              p.ldf, true, m.vpl, &err)))
+            return failc(c, ALEBGK_ECUDA, err);
+    }
+    dropGraphs(c);
+    return ALEBGK_OK;
+}
+
 int alebgk_get_launch(alebgk_ctx *c, int *transport_threads, int *particle_warps)
 {
     if (!c || !transport_threads || !particle_warps) return ALEBGK_EINVAL;

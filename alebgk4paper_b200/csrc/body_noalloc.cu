@@ -17,6 +17,7 @@
 // serialised by the caller.  Every call overwrites all of the scratch it reads
 // (each block writes all of its partial sums, zeros included), so nothing has
 // to start at zero.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -45,6 +46,38 @@ struct BodyGeom
 
 std::mutex g_setupMutex;
 double *g_scratchPtr[kNoAllocMaxDevices] = {};
+unsigned long long g_scratchCtx[kNoAllocMaxDevices] = {};   // context id of that address
+
+// Unique id of the device's current context (cuCtxGetId), or 0 where the
+// driver does not offer it.  A device reset destroys the context that an
+// address was looked up in; the next context has a new id.
+unsigned long long currentContextId()
+{
+    typedef CUresult (*GetCurrentFn)(CUcontext *);
+    typedef CUresult (*GetIdFn)(CUcontext, unsigned long long *);
+    static GetCurrentFn getCurrent = nullptr;
+    static GetIdFn getId = nullptr;
+    static bool looked = false;
+    if (!looked)
+    {
+        looked = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) ==
+                cudaSuccess && q == cudaDriverEntryPointSuccess)
+            getCurrent = reinterpret_cast<GetCurrentFn>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            getId = reinterpret_cast<GetIdFn>(p);
+    }
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (getCurrent && getId && getCurrent(&ctx) == CUDA_SUCCESS && ctx &&
+        getId(ctx, &id) == CUDA_SUCCESS)
+        return id;
+    return 0;
+}
 
 __device__ __forceinline__ double warpSum6(double v)
 {
@@ -152,18 +185,22 @@ __global__ void k_body_total(const double *__restrict__ partial, int nbodies,
     out[t] = s;
 }
 
-// Device address of this device's scratch, looked up once per device with
-// that device current.  Not to be first called inside a stream capture.
+// Device address of this device's scratch, looked up with that device
+// current the first time a context of the device calls (and again after a
+// device reset has replaced the context).  Not to be first called inside a
+// stream capture.
 cudaError_t scratchFor(int device, double **ptr)
 {
     if (device < 0 || device >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(g_setupMutex);
-    if (!g_scratchPtr[device])
+    const unsigned long long ctxId = currentContextId();
+    if (!g_scratchPtr[device] || g_scratchCtx[device] != ctxId)
     {
         double *p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress((void **)&p, g_bodyScratch);
         if (e != cudaSuccess) return e;
         g_scratchPtr[device] = p;
+        g_scratchCtx[device] = ctxId;
     }
     *ptr = g_scratchPtr[device];
     return cudaSuccess;

@@ -17,8 +17,11 @@ struct MarchState
 {
     bool enabled = false;
     int nunits = 0, nunitsY = 0, Vpad = 0, Nx = 0, Ny = 0, Nz = 0;
+    int vpl = 2;                              // velocities per lane (1 or 2)
     MarchUnit *units = nullptr;               // y-march units first, then z-march
     float *coefT = nullptr, *coefTy = nullptr;
+    int *gather = nullptr;                    // particles the gather transports
+    int ngather = 0;
     alignas(64) unsigned char tmap[2][128];   // CUtensorMap per source buffer
     alignas(64) unsigned char tmapY[2][128];  // the same with the y-march box
 };
@@ -64,6 +67,9 @@ struct DeviceBuffers
     double *massEnd = nullptr;         // per particle: mass of h at step end
     double *minG = nullptr;            // per particle: min of h over the mass layer
     double *nad = nullptr;             // per particle: NAD neighbour density range (lo, hi)
+    double *rowSums = nullptr;         // per particle: 6 row sums (three-kernel particle stage)
+    float *rowTab = nullptr;           // per particle: collision table (tabStride floats)
+    int *rowKind = nullptr;            // per particle: 1 collided by k_row_collide, else 0
     double *redPartial = nullptr;      // per-block partials of the grid sums
     double *dpx = nullptr;
     double *bodyTmp = nullptr;         // N x 6 per-particle load contributions
@@ -92,6 +98,7 @@ struct StepParams
     // ulp of FP32, far above the reference's 1e-9 absolute slack near a
     // uniform state, so the screen would flag rounding noise.
     double nadNoise = 0;
+    int tabStride = 0;    // floats per particle of the collision table (3 Nv + 2, padded)
 };
 
 }  // namespace alebgk
@@ -129,13 +136,19 @@ struct alebgk_ctx
     {
         int transportThreads = 0;     // coefficient-gather transport per block; 0 fused
         int particleWarps = 0;        // warp-per-particle kernel; 0 = as many as fit
+        int marchVpl = 2;             // lattice march: velocities per lane (1 or 2)
     } tune;
     // Streamed particle kernel: on, warps per block, blocks, dynamic smem.
     bool pStream = false;
     int pStreamWpb = 0, pStreamBlocks = 0;
     size_t pStreamSmem = 0;
+    // Three-kernel form of the streamed stages (FP32): on, launch sizes.
+    bool pSplit = false;
+    int pSumsBlocks = 0, pCollBlocks = 0;
+    size_t pSumsSmem = 0, pCollSmem = 0;
     std::string err;
     std::vector<int> bodyIdHost;
+    int maxBodyId = -1;          // largest entry of bodyIdHost (-1: no body particle)
     std::vector<int> boundaryHost;
     std::vector<int> surfHost;   // body-surface particle indices, ascending
     bool geometryDirty = false;  // a body step moved the surface since the upload
@@ -248,9 +261,17 @@ cudaError_t bodyLoadsNoAlloc(alebgk_ctx *c, int nbodies, const double *centre,
 cudaError_t launchResidual(alebgk_ctx *c, double *out, cudaStream_t st);
 cudaError_t launchConvertIn(alebgk_ctx *c, const double *src, int buf);
 cudaError_t launchConvertOut(alebgk_ctx *c, double *dst, int buf);
-cudaError_t launchMarch(alebgk_ctx *c, int from, float *outBuf, cudaStream_t st);
+// The lattice march of buffer `from` into outBuf on st; the gather of the
+// particles its units leave out goes on gatherStream (nullptr: launched by
+// the caller with launchTransportList).
+cudaError_t launchMarch(alebgk_ctx *c, int from, float *outBuf, cudaStream_t st,
+                        cudaStream_t gatherStream);
+// Coefficient-gather transport of the listed particles (step.cu): the
+// particles of a lattice that the march's units leave out.
+cudaError_t launchTransportList(alebgk_ctx *c, int from, float *outBuf, const int *list, int n,
+                                cudaStream_t st);
 cudaError_t prepareMarch();
 bool encodeMarchMap(void *tmapOut, void *f, int V, int Nx, int Ny, int Nz, int ldf,
-                    bool yMarch, std::string *err);
+                    bool yMarch, int vpl, std::string *err);
 
 }  // namespace alebgk

@@ -4,24 +4,27 @@
 // offsets |o|^2 <= 6, for a cloud that is a complete lattice (march.h).
 //
 // CTA = one work unit (an 8x4 tile of lattice columns, output planes
-// [za, zb)) x one chunk of 32 velocities, lane = velocity; the chunks of a
-// unit are consecutive CTAs.  The CTA marches
-// through z: every input plane of the tile plus a two-column halo (12x8
-// particles x 32 velocities, 12 KB) is brought into a six-slot shared-
-// memory ring by one TMA tensor load (cp.async.bulk.tensor.4d, completion on
-// an mbarrier; zero fill outside the lattice).  Each warp owns one
-// class-uniform 2x2 block of columns; its 81 coefficients for its lane's
-// velocity stay in registers for the whole march, and every staged value
-// feeds the FMAs of up to four columns and five output planes, held in a
-// 4 x 5 register queue.  An output plane is complete two input planes after
-// its own and is stored straight from the queue; planes outside the lattice
-// are zero and are skipped.  Long segments run every queue slot without
-// tests; short ones (the single-plane wall layers) only the slots of their
-// own output planes.  Thread 0 refills a ring
-// slot two planes after the warps released it, so the warps of a CTA may
-// drift apart by two planes without stalling the loads, which run four
-// planes ahead.  Every wait is bounded; a timeout sets the step's error
-// word instead of hanging.
+// [za, zb)) x one chunk of 32 VPL velocities; lane l holds the VPL adjacent
+// velocities k0 + VPL l .. k0 + VPL l + VPL - 1 (VPL = 2: a float2 per lane,
+// and every stencil FMA is one packed fma.rn.f32x2 on two velocities, which
+// halves the FMA and shared-memory load instructions per update).  The
+// chunks of a unit are consecutive CTAs.  The CTA marches through z: every
+// input plane of the tile plus a two-column halo (12x8 particles x 32 VPL
+// velocities) is brought into a six-slot shared-memory ring by one TMA
+// tensor load (cp.async.bulk.tensor.4d, completion on an mbarrier; zero fill
+// outside the lattice).  Each warp owns one class-uniform 2x2 block of
+// columns; its 81 coefficients for its lane's velocities stay in registers
+// for the whole march, and every staged value feeds the FMAs of up to four
+// columns and five output planes, held in a 4 x 5 register queue.  An output
+// plane is complete two input planes after its own and is stored straight
+// from the queue; planes outside the lattice are zero and are skipped.  Long
+// segments run every queue slot without tests; short ones (the single-plane
+// wall layers) only the slots of their own output planes.  Thread 0 refills
+// a ring slot two planes after the warps released it, so the warps of a CTA
+// may drift apart by two planes without stalling the loads, which run four
+// planes ahead.  Every wait is bounded; a timeout sets the step's error word
+// instead of hanging.  Packed and scalar FMAs round alike (each half of
+// fma.rn.f32x2 is one fmaf), so both widths give the same bits.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -41,7 +44,10 @@ constexpr int kPH = kMarchTileY + 4;
 constexpr int kRing = 6;                  // staged planes
 constexpr int kLag = 2;                   // refill lag behind the consumers
 static_assert(kLag < kRing, "ring");
-constexpr uint32_t kPlaneBytes = kPW * kPH * kMarchChunk * 4;
+// Bytes of one staged plane at VPL velocities per lane.
+template <int VPL>
+__host__ __device__ constexpr uint32_t planeBytes() { return kPW * kPH * kMarchChunk * VPL * 4; }
+
 
 __host__ __device__ constexpr int tidx(int dx, int dy, int dz)
 {
@@ -69,6 +75,27 @@ __device__ __forceinline__ void unroll(F &&f)
     unrollImpl(std::make_integer_sequence<int, N>{}, f);
 }
 
+// VPL velocities of one lane: a float, or a float2 updated by packed
+// fma.rn.f32x2 / mul.rn.f32x2 (sm_100a).
+template <int VPL> struct Lanes;
+template <> struct Lanes<1>
+{
+    typedef float T;
+    static __device__ __forceinline__ T zero() { return 0.0f; }
+    static __device__ __forceinline__ T fma(T a, T b, T c) { return fmaf(a, b, c); }
+    static __device__ __forceinline__ T mul(T a, float s) { return a * s; }
+};
+template <> struct Lanes<2>
+{
+    typedef float2 T;
+    static __device__ __forceinline__ T zero() { return make_float2(0.0f, 0.0f); }
+    static __device__ __forceinline__ T fma(T a, T b, T c) { return __ffma2_rn(a, b, c); }
+    static __device__ __forceinline__ T mul(T a, float s)
+    {
+        return __fmul2_rn(a, make_float2(s, s));
+    }
+};
+
 __device__ __forceinline__ void tmaLoadPlane(void *dst, const CUtensorMap *map, uint64_t *bar,
                                              int c0, int c1, int c2, int c3)
 {
@@ -82,14 +109,19 @@ __device__ __forceinline__ void tmaLoadPlane(void *dst, const CUtensorMap *map, 
 
 }  // namespace
 
-__global__ void __launch_bounds__(kMarchWarps * 32, 2)
+template <int VPL>
+__global__ void __launch_bounds__(kMarchWarps * 32, 3 - VPL)
 k_march(const __grid_constant__ CUtensorMap tmapZ, const __grid_constant__ CUtensorMap tmapY,
         const MarchUnit *__restrict__ units, const float *__restrict__ coefTz,
         const float *__restrict__ coefTy, float *__restrict__ out, int ldf, int Nx, int Ny,
         int Nz, int V, int Vpad, StepScalars *sc)
 {
+    typedef Lanes<VPL> LN;
+    typedef typename LN::T VT;
+    constexpr int CW = kMarchChunk * VPL;        // velocities per CTA
+    constexpr uint32_t kPlaneBytes = planeBytes<VPL>();
     extern __shared__ __align__(128) unsigned char marchSmem[];
-    typedef float Plane[kPH][kPW][kMarchChunk];
+    typedef VT Plane[kPH][kPW][kMarchChunk];
     Plane *ring = reinterpret_cast<Plane *>(marchSmem);
     __shared__ __align__(8) uint64_t full[kRing], empty[kRing];
     __shared__ int giveUp;
@@ -108,8 +140,8 @@ k_march(const __grid_constant__ CUtensorMap tmapZ, const __grid_constant__ CUten
     const int rowStride = yMarch ? ldf * Nx * Ny : ldf * Nx;
     const int planeStride = yMarch ? ldf * Nx : ldf * Nx * Ny;
     const int marchLen = yMarch ? Ny : Nz;
-    const int k0 = blockIdx.x * kMarchChunk;
-    const int k = k0 + lane;
+    const int k0 = blockIdx.x * CW;
+    const int k = k0 + VPL * lane;               // the lane's first velocity
     const int nin = zb - za + 4;                 // input planes za-2 .. zb+1
     // Planes outside the lattice hold zeros: they are not staged; the queue
     // only moves past them.  Staged plane m is lattice plane zlo + m.
@@ -149,21 +181,26 @@ k_march(const __grid_constant__ CUtensorMap tmapZ, const __grid_constant__ CUten
             loadPlane(&ring[m][0][0][0], &full[m], zlo + m);
         }
 
-    float coef[kTmplOffsets];
+    // The table is [class][81][Vpad] with Vpad a multiple of CW, so the
+    // lane's VPL coefficients of one offset are adjacent and aligned.
+    VT coef[kTmplOffsets];
     if (active)
     {
-        const float *cb = coefT + (size_t)cls * kTmplOffsets * Vpad + k;
+        const VT *cb = reinterpret_cast<const VT *>(coefT + (size_t)cls * kTmplOffsets * Vpad + k);
 #pragma unroll
-        for (int o = 0; o < kTmplOffsets; ++o) coef[o] = __ldg(cb + (size_t)o * Vpad);
+        for (int o = 0; o < kTmplOffsets; ++o) coef[o] = __ldg(cb + (size_t)o * (Vpad / VPL));
     }
-    float acc[4][5];
+    VT acc[4][5];
 #pragma unroll
     for (int c = 0; c < 4; ++c)
 #pragma unroll
-        for (int r = 0; r < 5; ++r) acc[c][r] = 0.0f;
+        for (int r = 0; r < 5; ++r) acc[c][r] = LN::zero();
     const float scale = (float)sc->scale;
     // Output column c of the warp's block at plane z:
     // outBase + z planeStride + (c & 1) colStride + (c >> 1) rowStride.
+    // With VPL = 2 and an odd V the last pair of a row may end one past V:
+    // that float lies in the row padding (ldf rounds V up to a multiple of
+    // four), which nothing reads.
     float *outBase = out + (long long)(ux0 + bx) * colStride + (long long)(uy0 + by) * rowStride + k;
     const int smask = (k < V) ? mask : 0;
     bool dead = false;
@@ -171,7 +208,7 @@ k_march(const __grid_constant__ CUtensorMap tmapZ, const __grid_constant__ CUten
     // The FMAs of one staged plane into the queue for a warp block of shape
     // SHAPE (column c at (CX(c), CY(c)) from the block origin); with
     // `gated`, only the slots holding the unit's own output planes.
-    auto fmaPlane = [&](auto SHAPE, const float *P, auto GATED, auto inSeg) {
+    auto fmaPlane = [&](auto SHAPE, const VT *P, auto GATED, auto inSeg) {
         constexpr int shp = decltype(SHAPE)::value;
         constexpr bool gated = decltype(GATED)::value;
         constexpr auto CX = [](int c) { return shp == kShapeBlock ? (c & 1)
@@ -185,7 +222,7 @@ k_march(const __grid_constant__ CUtensorMap tmapZ, const __grid_constant__ CUten
         constexpr bool xMajor = (shp == kShapeRow);
         constexpr int EA = xMajor ? EX : EY, EB = xMajor ? EY : EX;
         unroll<EA>([&](auto A) {
-            float v[EB];
+            VT v[EB];
             unroll<EB>([&](auto B) {
                 constexpr int dx = (xMajor ? decltype(A)::value : decltype(B)::value) - 2;
                 constexpr int dy = (xMajor ? decltype(B)::value : decltype(A)::value) - 2;
@@ -197,22 +234,25 @@ k_march(const __grid_constant__ CUtensorMap tmapZ, const __grid_constant__ CUten
                     v[decltype(B)::value] =
                         P[((by + dy + 2) * kPW + (bx + dx + 2)) * kMarchChunk + lane];
             });
-            unroll<5>([&](auto R) {
-                constexpr int r = decltype(R)::value;
-                constexpr int dz = 2 - r;
-                if (!gated || inSeg(r))
-                {
-                    unroll<EB>([&](auto B) {
-                        constexpr int dx = (xMajor ? decltype(A)::value : decltype(B)::value) - 2;
-                        constexpr int dy = (xMajor ? decltype(B)::value : decltype(A)::value) - 2;
+            // Value-major: each staged value feeds the queue slots and
+            // columns it reaches (up to 20 independent accumulators) before
+            // the next value, so FMAs into one accumulator are far apart.
+            unroll<EB>([&](auto B) {
+                constexpr int dx = (xMajor ? decltype(A)::value : decltype(B)::value) - 2;
+                constexpr int dy = (xMajor ? decltype(B)::value : decltype(A)::value) - 2;
+                unroll<5>([&](auto R) {
+                    constexpr int r = decltype(R)::value;
+                    constexpr int dz = 2 - r;
+                    if (!gated || inSeg(r))
+                    {
                         unroll<4>([&](auto C) {
                             constexpr int c = decltype(C)::value;
                             constexpr int o = tidx(dx - CX(c), dy - CY(c), dz);
                             if constexpr (o >= 0)
-                                acc[c][r] = fmaf(coef[o], v[decltype(B)::value], acc[c][r]);
+                                acc[c][r] = LN::fma(coef[o], v[decltype(B)::value], acc[c][r]);
                         });
-                    });
-                }
+                    }
+                });
             });
         });
     };
@@ -224,17 +264,17 @@ k_march(const __grid_constant__ CUtensorMap tmapZ, const __grid_constant__ CUten
             const int s1 = (shp == kShapeColumn) ? rowStride : colStride;
             const int s2 = (shp == kShapeBlock) ? rowStride : 2 * s1;
             const int s3 = (shp == kShapeBlock) ? rowStride + colStride : 3 * s1;
-            if (smask & 1) o[0] = acc[0][0] * scale;
-            if (smask & 2) o[s1] = acc[1][0] * scale;
-            if (smask & 4) o[s2] = acc[2][0] * scale;
-            if (smask & 8) o[s3] = acc[3][0] * scale;
+            if (smask & 1) *reinterpret_cast<VT *>(o) = LN::mul(acc[0][0], scale);
+            if (smask & 2) *reinterpret_cast<VT *>(o + s1) = LN::mul(acc[1][0], scale);
+            if (smask & 4) *reinterpret_cast<VT *>(o + s2) = LN::mul(acc[2][0], scale);
+            if (smask & 8) *reinterpret_cast<VT *>(o + s3) = LN::mul(acc[3][0], scale);
         }
 #pragma unroll
         for (int c = 0; c < 4; ++c)
         {
 #pragma unroll
             for (int r = 0; r < 4; ++r) acc[c][r] = acc[c][r + 1];
-            acc[c][4] = 0.0f;
+            acc[c][4] = LN::zero();
         }
     };
     // Consumer release of staged plane m, then the producer's lagged refill.
@@ -323,7 +363,7 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t
                                   CUtensorMapFloatOOBfill);
 
 bool encodeMarchMap(void *tmapOut, void *f, int V, int Nx, int Ny, int Nz, int ldf,
-                    bool yMarch, std::string *err)
+                    bool yMarch, int vpl, std::string *err)
 {
     static EncodeTiledFn fn = nullptr;
     if (!fn)
@@ -343,9 +383,10 @@ bool encodeMarchMap(void *tmapOut, void *f, int V, int Nx, int Ny, int Nz, int l
     const cuuint64_t strides[3] = {(cuuint64_t)ldf * 4, (cuuint64_t)ldf * 4 * Nx,
                                    (cuuint64_t)ldf * 4 * Nx * Ny};
     // z-march: a 12 x 8 (x, y) tile at one z; y-march: a 12 x 8 (x, z) tile
-    // at one y.  Both land in shared memory as [8][12][32 velocities].
-    const cuuint32_t boxZ[4] = {kMarchChunk, kPW, kPH, 1};
-    const cuuint32_t boxY[4] = {kMarchChunk, kPW, 1, kPH};
+    // at one y.  Both land in shared memory as [8][12][32 vpl velocities].
+    const cuuint32_t cw = (cuuint32_t)(kMarchChunk * vpl);
+    const cuuint32_t boxZ[4] = {cw, kPW, kPH, 1};
+    const cuuint32_t boxY[4] = {cw, kPW, 1, kPH};
     const cuuint32_t *box = yMarch ? boxY : boxZ;
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     CUresult r = fn(reinterpret_cast<CUtensorMap *>(tmapOut), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
@@ -362,21 +403,38 @@ bool encodeMarchMap(void *tmapOut, void *f, int V, int Nx, int Ny, int Nz, int l
 
 cudaError_t prepareMarch()
 {
-    return cudaFuncSetAttribute(k_march, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(kRing * kPlaneBytes));
+    cudaError_t e = cudaFuncSetAttribute(k_march<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(kRing * planeBytes<1>()));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_march<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(kRing * planeBytes<2>()));
+    return e;
 }
 
-cudaError_t launchMarch(alebgk_ctx *c, int from, float *outBuf, cudaStream_t st)
+cudaError_t launchMarch(alebgk_ctx *c, int from, float *outBuf, cudaStream_t st,
+                        cudaStream_t gatherStream)
 {
     const StepParams &p = c->sp;
     const MarchState &ms = c->march;
     const CUtensorMap *tz = reinterpret_cast<const CUtensorMap *>(ms.tmap[from]);
     const CUtensorMap *ty = reinterpret_cast<const CUtensorMap *>(ms.nunitsY ? ms.tmapY[from]
                                                                               : ms.tmap[from]);
-    k_march<<<dim3(ms.Vpad / kMarchChunk, ms.nunits), kMarchWarps * 32, kRing * kPlaneBytes,
-              st>>>(*tz, *ty, ms.units, ms.coefT, ms.coefTy ? ms.coefTy : ms.coefT, outBuf,
-                    p.ldf, ms.Nx, ms.Ny, ms.Nz, p.V, ms.Vpad, c->d.sc);
-    return cudaGetLastError();
+    const float *cy = ms.coefTy ? ms.coefTy : ms.coefT;
+    if (ms.vpl == 2)
+        k_march<2><<<dim3(ms.Vpad / (2 * kMarchChunk), ms.nunits), kMarchWarps * 32,
+                     kRing * planeBytes<2>(), st>>>(*tz, *ty, ms.units, ms.coefT, cy, outBuf,
+                                                    p.ldf, ms.Nx, ms.Ny, ms.Nz, p.V, ms.Vpad,
+                                                    c->d.sc);
+    else
+        k_march<1><<<dim3(ms.Vpad / kMarchChunk, ms.nunits), kMarchWarps * 32,
+                     kRing * planeBytes<1>(), st>>>(*tz, *ty, ms.units, ms.coefT, cy, outBuf,
+                                                    p.ldf, ms.Nx, ms.Ny, ms.Nz, p.V, ms.Vpad,
+                                                    c->d.sc);
+    cudaError_t e = cudaGetLastError();
+    // the particles no unit covers, on the given side stream (or st)
+    if (e == cudaSuccess && ms.ngather > 0 && gatherStream)
+        e = launchTransportList(c, from, outBuf, ms.gather, ms.ngather, gatherStream);
+    return e;
 }
 
 }  // namespace alebgk

@@ -115,7 +115,8 @@ void buildMarchPlan(const double *xyz, int N, int dim, const int *nnb, const int
 
     // Canonical tables [class][81][Vpad].
     const int V = tb.V, ncls = tb.ncls, S = tb.S;
-    const int Vpad = (V + kMarchChunk - 1) / kMarchChunk * kMarchChunk;
+    // Rows padded to whole chunks of the widest march (two velocities per lane).
+    const int Vpad = (V + 2 * kMarchChunk - 1) / (2 * kMarchChunk) * (2 * kMarchChunk);
     plan.Nx = nx; plan.Ny = ny; plan.Nz = nz; plan.ncls = ncls; plan.Vpad = Vpad;
     plan.coefT.assign((size_t)ncls * kTmplOffsets * Vpad, 0.0f);
     if (tl) plan.coefTLin.assign((size_t)ncls * kTmplOffsets * Vpad, 0.0f);
@@ -228,12 +229,21 @@ void buildMarchPlan(const double *xyz, int N, int dim, const int *nnb, const int
         }
     };
 
-    // z-march units: every long z-segment; in thin planes only the columns
-    // whose y is next to a y wall (the rest go to the y-march).
+    // z-march units: every long z-segment.  Thin planes go to the y-march,
+    // except the columns whose y is next to a y wall: those go to the gather.
     for (size_t sgi = 0; sgi + 1 < cuts.size(); ++sgi)
     {
         const int za = cuts[sgi], zb = cuts[sgi + 1];
         const bool isThin = zb - za < kThinSegment;
+        if (isThin)
+        {
+            for (int z = za; z < zb; ++z)
+                for (int y = 0; y < ny; ++y)
+                    if (!yLong[y])
+                        for (int x = 0; x < nx; ++x)
+                            plan.gatherList.push_back(x + nx * (y + ny * z));
+            continue;
+        }
         for (int y0 = 0; y0 < ny; y0 += kMarchTileY)
             for (int x0 = 0; x0 < nx; x0 += kMarchTileX)
             {
@@ -242,8 +252,7 @@ void buildMarchPlan(const double *xyz, int N, int dim, const int *nnb, const int
                     for (int bx = 0; bx < kMarchTileX; ++bx)
                     {
                         const int x = x0 + bx, y = y0 + by;
-                        tc[by][bx] = (x < nx && y < ny && !(isThin && yLong[y]))
-                                         ? cls(x, y, za) : -1;
+                        tc[by][bx] = (x < nx && y < ny) ? cls(x, y, za) : -1;
                     }
                 std::vector<int> subs;
                 coverTile(tc, subs);

@@ -22,6 +22,7 @@
 // reproducible.  No kernel waits on another block, so none can hang.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 
 #include "ctx.h"
@@ -251,6 +252,22 @@ k_transport(const T *__restrict__ f, T *__restrict__ g,
             int S, int N, int V, int L, int ldf, const StepScalars *__restrict__ sc)
 {
     k_transport_body(f, g, coef, cls, nslot, slots, S, N, V, L, ldf, sc, blockIdx.x, blockIdx.y);
+}
+
+// The same transport for a list of particles: block = list entries, one per
+// warp, at one velocity chunk.
+template <typename T>
+__global__ void __launch_bounds__(kNT)
+k_transport_list(const T *__restrict__ f, T *__restrict__ g, const T *__restrict__ coef,
+                 const int *__restrict__ cls, const int *__restrict__ nslot,
+                 const int *__restrict__ slots, const int *__restrict__ list, int n, int S,
+                 int V, int ldf, const StepScalars *__restrict__ sc)
+{
+    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int li = blockIdx.y * nw + warp;
+    if (li >= n) return;
+    transportRow<T, 1>(f, g, coef, cls, nslot, slots, S, V, ldf, T(sc->scale), list[li],
+                       blockIdx.x, transportChunks(V), threadIdx.x & 31);
 }
 
 // Walks the nodes k = lane, lane + 32, ... of a particle row and keeps the
@@ -1069,6 +1086,312 @@ k_particle_stream(ParticleArgs<T> a, StepParams p, int wpb)
 }
 
 // ---------------------------------------------------------------------------
+// The same stages for a 3-D single-layer FP32 cloud as three wide kernels,
+// so that no per-particle scalar chain holds up a streaming pass:
+//   k_row_sums      one warp per row.  Interior rows: the positivity sums
+//                   and the moments of the positive part (six FP32 lane sums,
+//                   combined over the warp in FP64) into rowSums.  Wall rows
+//                   are finished here whole: positivity, diffuse wall,
+//                   written back in place (finishWallStream).
+//   k_row_params    one thread per interior particle: positivity decision,
+//                   MOOD screen, moments of the repaired row, temperature,
+//                   the Maxwellian's per-axis factors (FP64, rounded into the
+//                   particle's FP32 table with c1 lam A folded into the x
+//                   axis), and the macros of the collided row by linearity
+//                   (c1 (moments of g + lam moments of M), the per-axis sums
+//                   of the factors giving the Maxwellian's moments).
+//   k_row_collide   one warp per row: h = a max(g, lo) + tx ty tz written
+//                   out (a = c1 s and lo = 0 when the repair fires, else
+//                   a = c1 and lo = -inf), and the row minimum.
+// The moments of the repaired row are those of the positive part (times the
+// repair scale when the repair fires); without a repair any negative values
+// sum to less than 1e-30 in magnitude (Positivity), below the rounding of
+// the FP64 moments, and rows of no positive mass are deferred to k_fixup as
+// before.  Per-particle table: 3 Nv factors, then a and lo (tabStride
+// floats, a multiple of four).
+// ---------------------------------------------------------------------------
+__host__ __device__ inline int rowTabStride(int Nv) { return (3 * Nv + 2 + 3) / 4 * 4; }
+constexpr int kRowBatch = 8;   // float4 loads in flight per lane in the row kernels
+
+__global__ void __launch_bounds__(kNT)
+k_row_sums(ParticleArgs<float> a, StepParams p, double *__restrict__ rowSums)
+{
+    __shared__ double tab[kNT / 32][3][kMaxNv];
+    __shared__ double velD[kMaxNv];
+    extern __shared__ __align__(16) unsigned char sumsSmem[];
+    VelNode<float> *velT = reinterpret_cast<VelNode<float> *>(sumsSmem);
+    int *idxT = reinterpret_cast<int *>(velT + p.V);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int V = p.V, Nv = p.Nv;
+    for (int k = threadIdx.x; k < V; k += blockDim.x)
+    {
+        const int iv = k % Nv, jv = (k / Nv) % Nv, kv = k / (Nv * Nv);
+        const double vx = fma((double)iv, p.dv, p.vmin);
+        const double vy = fma((double)jv, p.dv, p.vmin);
+        const double vz = fma((double)kv, p.dv, p.vmin);
+        velT[k] = VelNode<float>{float(vx), float(vy), float(vz),
+                                 float(vx * vx + vy * vy + vz * vz)};
+        idxT[k] = iv | jv << 8 | kv << 16;
+    }
+    for (int q = threadIdx.x; q < Nv; q += blockDim.x) velD[q] = fma((double)q, p.dv, p.vmin);
+    __syncthreads();
+    const int W = gridDim.x * (blockDim.x >> 5);
+    const int nq = (V + 3) >> 2;                 // float4 groups of a row
+    for (int i = blockIdx.x * (blockDim.x >> 5) + warp; i < p.N; i += W)
+    {
+        const float4 *row4 = reinterpret_cast<const float4 *>(a.g + (size_t)i * p.ldf);
+        if (a.boundary[i])
+        {
+            // positivity sums of the wall row, then the diffuse wall
+            float sp = 0.0f, sn = 0.0f;
+            for (int q = lane; q < nq; q += 32)
+            {
+                const float4 x = row4[q];
+                const float xs[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    if (4 * q + e < V) { sp += fmaxf(xs[e], 0.0f); sn += fminf(xs[e], 0.0f); }
+            }
+            double r2[2] = {(double)sp, (double)sn};
+            warpSumMany<2>(r2, lane);
+            const Positivity pv(r2[0], r2[1]);
+            if (lane == 0)
+            {
+                a.flag[i] = 0;
+                if (pv.fix) atomicAdd(&a.sc->nfix, 1);
+                a.massPos[i] = (r2[0] + r2[1]) * p.dvN;
+            }
+            finishWallStream(a, p, i, a.g + (size_t)i * p.ldf, idxT, velD, pv, tab[warp], lane);
+            __syncwarp();
+            continue;
+        }
+        float s0[2] = {0, 0}, sn[2] = {0, 0}, mx[2] = {0, 0}, my[2] = {0, 0}, mz[2] = {0, 0},
+              me[2] = {0, 0};
+        auto acc = [&](int u, float x, int k) {
+            const float xp = fmaxf(x, 0.0f);
+            const VelNode<float> v = velT[k];
+            s0[u] += xp;
+            sn[u] += fminf(x, 0.0f);
+            mx[u] = fmaf(v.vx, xp, mx[u]);
+            my[u] = fmaf(v.vy, xp, my[u]);
+            mz[u] = fmaf(v.vz, xp, mz[u]);
+            me[u] = fmaf(v.v2, xp, me[u]);
+        };
+        // The lane's float4 groups q = lane + 32 j, kRowBatch at a time: all
+        // of a batch's loads are issued before the first is used.
+        for (int q0 = 0; q0 < nq; q0 += 32 * kRowBatch)
+        {
+            float4 xv[kRowBatch];
+#pragma unroll
+            for (int j = 0; j < kRowBatch; ++j)
+            {
+                const int q = q0 + lane + 32 * j;
+                xv[j] = q < nq ? row4[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int j = 0; j < kRowBatch; ++j)
+            {
+                const int q = q0 + lane + 32 * j;
+                if (4 * q + 3 < V)
+                {
+                    acc(0, xv[j].x, 4 * q);
+                    acc(1, xv[j].y, 4 * q + 1);
+                    acc(0, xv[j].z, 4 * q + 2);
+                    acc(1, xv[j].w, 4 * q + 3);
+                }
+                else if (q < nq)
+                {
+                    acc(0, xv[j].x, 4 * q);
+                    if (4 * q + 1 < V) acc(1, xv[j].y, 4 * q + 1);
+                    if (4 * q + 2 < V) acc(0, xv[j].z, 4 * q + 2);
+                }
+            }
+        }
+        double r6[6] = {(double)s0[0] + (double)s0[1], (double)sn[0] + (double)sn[1],
+                        (double)mx[0] + (double)mx[1], (double)my[0] + (double)my[1],
+                        (double)mz[0] + (double)mz[1], (double)me[0] + (double)me[1]};
+        warpSumMany<6>(r6, lane);
+        if (lane < 6) rowSums[6 * (size_t)i + lane] = r6[lane];
+    }
+}
+
+__global__ void __launch_bounds__(kNT)
+k_row_params(ParticleArgs<float> a, StepParams p, const double *__restrict__ rowSums,
+             float *__restrict__ rowTab, int *__restrict__ rowKind)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.N) return;
+    if (a.boundary[i]) { rowKind[i] = 0; return; }
+    const double dvN = p.dvN;
+    const double *sm = rowSums + 6 * (size_t)i;
+    const double pos = sm[0], neg = sm[1];
+    const bool bad = !isfinite(pos) || !isfinite(neg) || !isfinite(sm[5]);
+    const double m = pos + neg;
+    const Positivity pv(pos, neg);
+    int flagged = 0;
+    if (p.limiter == 2)
+    {
+        const double2 nad = reinterpret_cast<const double2 *>(a.nad)[i];
+        if (bad || m <= 0.0) flagged = 1;
+        else if (isfinite(nad.x) && isfinite(nad.y))
+        {
+            const double rn = m * dvN;
+            const double slack = 0.1 * fmax(nad.y - nad.x, 1.0e-12) + 1.0e-9 +
+                                 p.nadNoise * fmax(fabs(nad.x), fabs(nad.y));
+            flagged = (rn < nad.x - slack || rn > nad.y + slack);
+        }
+    }
+    a.flag[i] = flagged;
+    if (pv.fix) atomicAdd(&a.sc->nfix, 1);
+    if (flagged)
+    {
+        a.flagList[atomicAdd(&a.sc->nflag, 1)] = i;
+        rowKind[i] = 0;
+        return;
+    }
+    a.massPos[i] = m * dvN;
+    // Moments of the repaired row (Moments.cpp:17-97): s times the
+    // positive part's when the repair fires.
+    const double f = (pv.fix ? pv.s : 1.0) * dvN;
+    const double M0 = pv.fix ? pos * f : m * dvN;
+    if (!(M0 > 1.0e-30) || p.tauVar)
+    {
+        a.degList[atomicAdd(&a.sc->ndeg, 1)] = i;
+        rowKind[i] = 0;
+        return;
+    }
+    const double iM0 = 1.0 / M0;
+    const double Mx = sm[2] * f, My = sm[3] * f, Mz = sm[4] * f, ME = sm[5] * f;
+    const double ux = Mx * iM0, uy = My * iM0, uz = Mz * iM0;
+    const double Tt = fmax((ME * iM0 - (ux * ux + uy * uy + uz * uz)) * p.inv3R, 1.0e-6);
+    const double c1 = p.c1, lam = p.lam;
+    const double twoRT = 2.0 * p.R * Tt;
+    const double piT = kPi * twoRT;
+    const double lamA = lam * M0 / (piT * sqrt(piT));
+    const double i2RT = 1.0 / twoRT;
+    const int Nv = p.Nv;
+    float *tb = rowTab + (size_t)i * p.tabStride;
+    double S[9];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+    {
+        const double u = d == 0 ? ux : (d == 1 ? uy : uz);
+        const double sc = d == 0 ? lamA : 1.0;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        for (int q = 0; q < Nv; ++q)
+        {
+            const double va = fma((double)q, p.dv, p.vmin);
+            const double e = sc * exp(-(va - u) * (va - u) * i2RT);
+            s0 += e;
+            s1 += va * e;
+            s2 += va * va * e;
+            tb[d * Nv + q] = (float)(d == 0 ? c1 * e : e);
+        }
+        S[3 * d] = s0; S[3 * d + 1] = s1; S[3 * d + 2] = s2;
+    }
+    tb[3 * Nv] = (float)(c1 * (pv.fix ? pv.s : 1.0));
+    tb[3 * Nv + 1] = pv.fix ? 0.0f : -INFINITY;
+    rowKind[i] = 1;
+    const double N0 = c1 * (M0 + dvN * S[0] * S[3] * S[6]);
+    const double Nx = c1 * (Mx + dvN * S[1] * S[3] * S[6]);
+    const double Ny = c1 * (My + dvN * S[0] * S[4] * S[6]);
+    const double Nz = c1 * (Mz + dvN * S[0] * S[3] * S[7]);
+    const double NE = c1 * (ME + dvN * (S[2] * S[3] * S[6] + S[0] * S[5] * S[6] +
+                                        S[0] * S[3] * S[8]));
+    double r2 = M0, x2 = ux, y2 = uy, z2 = uz, T2 = Tt;
+    if (N0 > 1.0e-30)
+    {
+        const double iN0 = 1.0 / N0;
+        r2 = N0; x2 = Nx * iN0; y2 = Ny * iN0; z2 = Nz * iN0;
+        T2 = fmax((NE * iN0 - (x2 * x2 + y2 * y2 + z2 * z2)) * p.inv3R, 1.0e-6);
+    }
+    double *mac = a.macNew + 6 * (size_t)i;
+    mac[0] = r2; mac[1] = x2; mac[2] = y2; mac[3] = z2; mac[4] = T2;
+    mac[5] = r2 * p.R * T2;
+    a.dpx[i] = 0.0;
+    a.massEnd[i] = N0;
+}
+
+__global__ void __launch_bounds__(kNT)
+k_row_collide(ParticleArgs<float> a, StepParams p, const float *__restrict__ rowTab,
+              const int *__restrict__ rowKind)
+{
+    __shared__ float wt[kNT / 32][3 * kMaxNv + 4];
+    extern __shared__ __align__(16) unsigned char collSmem[];
+    int *idxT = reinterpret_cast<int *>(collSmem);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int V = p.V, Nv = p.Nv;
+    // table offsets of each node's three factors, padded to whole float4s
+    for (int k = threadIdx.x; k < ((V + 3) & ~3); k += blockDim.x)
+    {
+        const int iv = k % Nv, jv = (k / Nv) % Nv, kv = k / (Nv * Nv);
+        idxT[k] = k < V ? (iv | (Nv + jv) << 8 | (2 * Nv + kv) << 16) : 0;
+    }
+    __syncthreads();
+    const int W = gridDim.x * (blockDim.x >> 5);
+    const int nq = (V + 3) >> 2;
+    float *t = wt[warp];
+    const int ntab = 3 * Nv + 2;
+    for (int i = blockIdx.x * (blockDim.x >> 5) + warp; i < p.N; i += W)
+    {
+        if (rowKind[i] != 1) continue;            // warp-uniform
+        float4 *row4 = reinterpret_cast<float4 *>(a.g + (size_t)i * p.ldf);
+        const float *tg = rowTab + (size_t)i * p.tabStride;
+        // the table and the first batch of the row in flight together
+        const float t0 = lane < ntab ? tg[lane] : 0.0f;
+        const float t1 = lane + 32 < ntab ? tg[lane + 32] : 0.0f;
+        const float t2 = lane + 64 < ntab ? tg[lane + 64] : 0.0f;
+        const float t3 = lane + 96 < ntab ? tg[lane + 96] : 0.0f;
+        const float t4 = lane + 128 < ntab ? tg[lane + 128] : 0.0f;
+        float mn = INFINITY;
+        for (int q0 = 0; q0 < nq; q0 += 32 * kRowBatch)
+        {
+            float4 xv[kRowBatch];
+            int4 iv[kRowBatch];
+#pragma unroll
+            for (int j = 0; j < kRowBatch; ++j)
+            {
+                const int q = q0 + lane + 32 * j;
+                xv[j] = q < nq ? row4[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+                iv[j] = q < nq ? reinterpret_cast<const int4 *>(idxT)[q] : make_int4(0, 0, 0, 0);
+            }
+            if (q0 == 0)
+            {
+                if (lane < ntab) t[lane] = t0;
+                if (lane + 32 < ntab) t[lane + 32] = t1;
+                if (lane + 64 < ntab) t[lane + 64] = t2;
+                if (lane + 96 < ntab) t[lane + 96] = t3;
+                if (lane + 128 < ntab) t[lane + 128] = t4;
+                __syncwarp();
+            }
+            const float am = t[3 * Nv], lo = t[3 * Nv + 1];
+            auto one = [&](float x, int id) {
+                return fmaf(am, fmaxf(x, lo), t[id & 255] * t[(id >> 8) & 255] * t[id >> 16]);
+            };
+#pragma unroll
+            for (int j = 0; j < kRowBatch; ++j)
+            {
+                const int q = q0 + lane + 32 * j;
+                if (q >= nq) continue;
+                float4 h;
+                h.x = one(xv[j].x, iv[j].x);
+                h.y = 4 * q + 1 < V ? one(xv[j].y, iv[j].y) : xv[j].y;
+                h.z = 4 * q + 2 < V ? one(xv[j].z, iv[j].z) : xv[j].z;
+                h.w = 4 * q + 3 < V ? one(xv[j].w, iv[j].w) : xv[j].w;
+                mn = fminf(mn, h.x);
+                if (4 * q + 1 < V) mn = fminf(mn, h.y);
+                if (4 * q + 2 < V) mn = fminf(mn, h.z);
+                if (4 * q + 3 < V) mn = fminf(mn, h.w);
+                row4[q] = h;
+            }
+        }
+        const double mnd = warpMin((double)mn);
+        if (lane == 0) a.minG[i] = mnd;
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Linear MLS redo of the flagged particles (Solver/Solver.cpp:641-646:
 // mlsTransportCompute(..., 1, onlyFlagged=true)) from the pre-transport
 // state, one block per particle, then positivity and finish on warp 0.
@@ -1792,6 +2115,28 @@ static int particleWarpsPerBlock(const StepParams &p, size_t es)
     return w < 1 ? 1 : (w > kNT / 32 ? kNT / 32 : w);
 }
 
+// The streamed particle stage of a 3-D single-layer cloud: batched (FP32)
+// or one warp per particle.
+template <typename T>
+static void launchParticleStream(alebgk_ctx *c, const ParticleArgs<T> &pa, const StepParams &p,
+                                 cudaStream_t st)
+{
+    if constexpr (sizeof(T) == 4)
+    {
+        if (c->pSplit)
+        {
+            DeviceBuffers &d = c->d;
+            k_row_sums<<<c->pSumsBlocks, kNT, c->pSumsSmem, st>>>(pa, p, d.rowSums);
+            k_row_params<<<(p.N + kNT - 1) / kNT, kNT, 0, st>>>(pa, p, d.rowSums, d.rowTab,
+                                                                d.rowKind);
+            k_row_collide<<<c->pCollBlocks, kNT, c->pCollSmem, st>>>(pa, p, d.rowTab,
+                                                                     d.rowKind);
+            return;
+        }
+    }
+    k_particle_stream<T><<<c->pStreamBlocks, kNT, c->pStreamSmem, st>>>(pa, p, c->pStreamWpb);
+}
+
 // Launches one step.  With ev != nullptr an event is recorded before each
 // launch and after the last one (ev[0..ALEBGK_NSTAGES]), in launch order:
 // step_begin, transport, particle, redo, sigma, fixup, mass_sum, scale_mood,
@@ -1832,6 +2177,13 @@ static cudaError_t stepT(alebgk_ctx *c, int from, cudaEvent_t *ev)
         cudaStreamWaitEvent(c->stream2, c->evFork, 0);
         k_step_begin<<<nadBlocks, kNT, 0, c->stream2>>>(d.sc, 0, macA, d.boundary, d.nslot,
                                                         d.slots, p.S, p.N, d.nad);
+        // the march's left-out particles ride on the side stream too
+        if (sizeof(T) == 4 && c->march.enabled && c->march.ngather > 0)
+        {
+            cudaError_t e = launchTransportList(c, from, reinterpret_cast<float *>(fb),
+                                                c->march.gather, c->march.ngather, c->stream2);
+            if (e != cudaSuccess) return e;
+        }
         cudaEventRecord(c->evJoin, c->stream2);
     }
     else
@@ -1845,7 +2197,8 @@ static cudaError_t stepT(alebgk_ctx *c, int from, cudaEvent_t *ev)
     const bool fused = !march && !c->pStream && c->tune.transportThreads == 0 && !ev;
     if (march)
     {
-        cudaError_t e = launchMarch(c, from, reinterpret_cast<float *>(fb), st);
+        cudaError_t e = launchMarch(c, from, reinterpret_cast<float *>(fb), st,
+                                    fork ? nullptr : st);
         if (e != cudaSuccess) return e;
     }
     else if (!fused)
@@ -1864,8 +2217,7 @@ static cudaError_t stepT(alebgk_ctx *c, int from, cudaEvent_t *ev)
                         ? c->tune.particleWarps : wmax;
     const int ppBlocks = (p.N + wpb - 1) / wpb;
     if (c->pStream)
-        k_particle_stream<T><<<c->pStreamBlocks, kNT, c->pStreamSmem, st>>>(pa, p,
-                                                                          c->pStreamWpb);
+        launchParticleStream<T>(c, pa, p, st);
     else if (fused)
     {
         if (p.L == 2) k_particle<T, 2, true><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
@@ -1950,13 +2302,54 @@ static cudaError_t prepareT(alebgk_ctx *c)
                 c->pStreamBlocks = need < sms * occ ? need : sms * occ;
             }
         }
+        // The three-kernel form of the same stages (FP32 only): the default,
+        // unless the warp-per-particle form is asked for.
+        c->pSplit = false;
+        if (e == cudaSuccess && c->pStream && sizeof(T) == 4 && c->cfg.particle != 3 &&
+            p.Nv <= kMaxNv)
+        {
+            const size_t s1 = streamRowsOffset<float>(p.V), s3 = (size_t)4 * ((p.V + 3) & ~3);
+            set((const void *)k_row_sums, s1);
+            set((const void *)k_row_collide, s3);
+            int o1 = 0, o3 = 0, sms = 0;
+            if (e == cudaSuccess)
+                e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (e == cudaSuccess)
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_row_sums, kNT, s1);
+            if (e == cudaSuccess)
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o3, k_row_collide, kNT, s3);
+            if (e == cudaSuccess && o1 > 0 && o3 > 0)
+            {
+                const int need = (p.N + kNT / 32 - 1) / (kNT / 32);
+                c->pSplit = true;
+                c->pSumsSmem = s1;
+                c->pCollSmem = s3;
+                c->pSumsBlocks = std::min(need, sms * o1);
+                c->pCollBlocks = std::min(need, sms * o3);
+            }
+        }
     }
     return e;
 }
 
+
+
 cudaError_t prepareKernels(alebgk_ctx *c)
 {
     return (c->cfg.precision == 64) ? prepareT<double>(c) : prepareT<float>(c);
+}
+
+cudaError_t launchTransportList(alebgk_ctx *c, int from, float *outBuf, const int *list, int n,
+                                cudaStream_t st)
+{
+    const StepParams &p = c->sp;
+    const DeviceBuffers &d = c->d;
+    dim3 grid(transportChunks(p.V), (n + kNT / 32 - 1) / (kNT / 32));
+    k_transport_list<float><<<grid, kNT, 0, st>>>(static_cast<const float *>(d.f[from]), outBuf,
+                                                  static_cast<const float *>(d.coef), d.cls,
+                                                  d.nslot, d.slots, list, n, p.S, p.V, p.ldf,
+                                                  d.sc);
+    return cudaGetLastError();
 }
 
 cudaError_t launchStep(alebgk_ctx *c, int from, cudaEvent_t *ev)
@@ -2338,7 +2731,7 @@ static cudaError_t slabSegT(alebgk_ctx *c, int from, int seg, cudaStream_t st)
         const bool fused = !march && !c->pStream && c->tune.transportThreads == 0;
         if (march)
         {
-            cudaError_t e = launchMarch(c, from, reinterpret_cast<float *>(fb), st);
+            cudaError_t e = launchMarch(c, from, reinterpret_cast<float *>(fb), st, st);
             if (e != cudaSuccess) return e;
         }
         else if (!fused)
@@ -2354,8 +2747,7 @@ static cudaError_t slabSegT(alebgk_ctx *c, int from, int seg, cudaStream_t st)
                             ? c->tune.particleWarps : wmax;
         const int ppBlocks = (p.N + wpb - 1) / wpb;
         if (c->pStream)
-            k_particle_stream<T><<<c->pStreamBlocks, kNT, c->pStreamSmem, st>>>(
-                pa, p, c->pStreamWpb);
+            launchParticleStream<T>(c, pa, p, st);
         else if (fused && p.L == 2)
             k_particle<T, 2, true><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);
         else if (fused) k_particle<T, 1, true><<<ppBlocks, kNT, wpb * rowBytes, st>>>(pa, p, wpb);

@@ -311,8 +311,8 @@ def run_ours(args):
     es = 4 if args.precision == 32 else 8
     cnt0 = s.counters()
     kernels = {"transport": "k_march" if cnt0["transport_kernel"] == 2 else "k_transport",
-               "particle": "k_particle_stream" if cnt0["particle_kernel"] == 2
-               else "k_particle"}
+               "particle": {1: "k_particle", 2: "k_particle_stream",
+                            3: "k_row_sums+k_row_params+k_row_collide"}[cnt0["particle_kernel"]]}
     # Algorithmic bytes per update: the transport and the particle stage each
     # read f once and write it once (FP32: 4 + 4 bytes).
     per_update = 2 * es
@@ -386,7 +386,10 @@ def run_ours(args):
                    "parallelism": f"{world} independent cavities, one per GPU",
                    "l2": "inputs larger than L2: two 256 MB distribution buffers "
                          "ping-pong, no flush needed"},
-        "gpu_launches": 10 * args.steps,
+        # 10 stage kernels; the row stage is three; the march adds the gather
+        # of its left-out particles
+        "gpu_launches": (10 + (2 if cnt0["particle_kernel"] == 3 else 0) +
+                         (1 if cnt0["transport_kernel"] == 2 else 0)) * args.steps,
         "kernels": kernels,
         "stage_ms": {k: round(v, 5) for k, v in stage_ms.items()},
         "roofline": {"bound": "hbm", "kernel": kern_name, "achieved": achieved,

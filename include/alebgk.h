@@ -9,7 +9,7 @@
  * replaces one of them with plain pointers, sizes and an int status, so that
  * a C, C++, Python (ctypes) or any other FFI caller can bind it; the
  * reference-side C++ shim that maps the original symbols onto these calls is
- * given in INTEGRATION.md.
+ * alebgk4paper_b200/shim/cuda_backend_shim.cpp.
  *
  * Conventions
  *   - Every call returns ALEBGK_OK (0) or a negative ALEBGK_E* code; the
@@ -67,8 +67,10 @@ typedef struct alebgk_config
                          lattice and precision is 32, else coefficient
                          gather), 1 always gather, 2 require the march       */
     int particle;     /* 0 auto (streamed rows for a 3-D cloud whose rows fit,
-                         else one warp per particle), 1 always the general
-                         kernel, 2 require the streamed kernel                */
+                         in FP32 as three row kernels; else one warp per
+                         particle), 1 always the general kernel, 2 require
+                         streamed rows (three row kernels in FP32), 3
+                         require streamed rows with one warp per particle     */
 } alebgk_config;
 
 /* The host cloud in SoA form.  Inputs for alebgk_upload; the download calls
@@ -104,7 +106,8 @@ typedef struct alebgk_counters
     int transport_kernel;     /* transport in use: 1 coefficient gather,
                                  2 lattice march                              */
     int particle_kernel;      /* particle stage in use: 1 warp per particle,
-                                 2 streamed rows                              */
+                                 2 streamed rows, one warp per particle,
+                                 3 streamed rows, three row kernels           */
 } alebgk_counters;
 
 /* ---- context --------------------------------------------------------- */
@@ -216,7 +219,8 @@ int alebgk_body_loads(alebgk_ctx *ctx, int nbodies, const double *body_centre,
  * ALEBGK_EINVAL.  Scratch: one fixed 114,432-byte device array per device,
  * shared by all contexts on it, so overlapping calls on one device race and
  * must be serialised by the caller.  The first call on a device looks the
- * array up and should come before any stream capture. */
+ * array up and should come before any stream capture; so should the first
+ * call after a device reset, which looks it up again in the new context. */
 #define ALEBGK_NOALLOC_MAX_BODIES 16
 int alebgk_body_loads_noalloc(alebgk_ctx *ctx, int nbodies, const double *body_centre,
                               const double *body_area, double *out);
@@ -273,6 +277,12 @@ int alebgk_body_set_surface_velocity(alebgk_ctx *ctx, int nbodies,
  * particle kernel have fixed shapes.  Drops the captured step graphs. */
 int alebgk_set_launch(alebgk_ctx *ctx, int transport_threads, int particle_warps);
 int alebgk_get_launch(alebgk_ctx *ctx, int *transport_threads, int *particle_warps);
+
+/* Velocities per lane of the lattice march: 2 (default; packed
+ * fma.rn.f32x2 on two adjacent velocities, 64 velocities per block) or 1
+ * (one velocity per lane, 32 per block).  Both widths give the same bits.
+ * Drops the captured step graphs. */
+int alebgk_set_march_width(alebgk_ctx *ctx, int velocities_per_lane);
 
 /* Times every candidate launch shape over `steps` steps, each on a device
  * snapshot of the state that is restored afterwards, and keeps the fastest;

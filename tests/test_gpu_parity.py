@@ -144,6 +144,26 @@ def test_lattice_march_matches_gather(gpu, case, Nx, Nv, order, steps):
     assert rel(mm[:, 0], mg[:, 0]) < 1e-6
 
 
+@pytest.mark.parametrize("case,Nx,Nv,order", [("cavity3d", 13, 10, 2), ("cavity3d", 9, 5, 2),
+                                              ("cavity3d", 8, 6, 1)])
+def test_packed_march_equals_scalar_march(gpu, case, Nx, Nv, order):
+    """Two velocities per lane (packed fma.rn.f32x2, 64 per block) and one
+    per lane give the same bits: each half of a packed FMA rounds as one
+    fmaf, in the same order.  Nv = 5 has an odd row length V = 125, whose
+    last lane pair straddles the end of the row."""
+    c = ab.Case(case, Nx, Nv, -1.0, order)
+    out = []
+    for width in (2, 1):
+        s = ab.Solver(c, config=c.config(32, 0, 2))
+        s.set_march_width(width)
+        s.cudaStep(3)
+        assert s.counters()["error_word"] == 0
+        out.append(s.cudaDownloadFull())
+        s.close()
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+
+
 def test_step_is_deterministic(gpu):
     c = ab.Case("cavity3d", 12, 6, -1.0, 2)
     out = []
@@ -225,7 +245,7 @@ def test_streamed_particle_kernel_matches_general(gpu, case, Nx, Nv, precision, 
     cfg_s.limiter = cfg_g.limiter = limiter
     s = ab.Solver(c, config=cfg_s)
     g = ab.Solver(c, config=cfg_g)
-    assert s.counters()["particle_kernel"] == 2
+    assert s.counters()["particle_kernel"] == (3 if precision == 32 else 2)
     assert g.counters()["particle_kernel"] == 1
     for _ in range(steps):
         s.cudaStep(1)
@@ -243,6 +263,58 @@ def test_streamed_particle_kernel_matches_general(gpu, case, Nx, Nv, precision, 
     assert np.abs(ms[:, 1:4] - mg[:, 1:4]).max() < (1e-8 if precision == 64 else 1e-2)
     s.close()
     g.close()
+
+
+@pytest.mark.parametrize("case,Nx,Nv,steps", [("cavity3d", 13, 10, 4), ("cavity3d", 9, 5, 3),
+                                              ("cavity3d-sphere", 12, 4, 2)])
+def test_row_kernels_match_streamed_particle_kernel(gpu, case, Nx, Nv, steps):
+    """FP32: the three row kernels (row sums; per-particle decisions and
+    tables on one thread; the collision written out) and the
+    warp-per-particle streamed stage take the same MOOD and repair branches
+    and agree to FP32 rounding."""
+    c = ab.Case(case, Nx, Nv, -1.0, 2, fixed_body=True)
+    b = ab.Solver(c, config=c.config(32, 0, 0, 2))
+    w = ab.Solver(c, config=c.config(32, 0, 0, 3))
+    assert b.counters()["particle_kernel"] == 3
+    assert w.counters()["particle_kernel"] == 2
+    for _ in range(steps):
+        b.cudaStep(1)
+        w.cudaStep(1)
+        cb, cw = b.counters(), w.counters()
+        assert cb["error_word"] == 0
+        for k in ("transport_flags", "positivity_fixes", "mood_fail"):
+            assert cb[k] == cw[k], k
+    gb, mb = b.cudaDownloadFull()
+    gw, mw = w.cudaDownloadFull()
+    assert rel(gb, gw) < 1e-5
+    for q in (0, 4, 5):
+        assert rel(mb[:, q], mw[:, q]) < 1e-5, q
+    b.close()
+    w.close()
+
+
+def test_row_kernels_positivity_repair(gpu):
+    """FP32, planted negative nodes: the row kernels repair the same rows as
+    the FP64 oracle and stay within the FP32 error of it."""
+    c = ab.Case("cavity3d", 10, 6, -1.0, 2)
+    inner = np.nonzero(c.boundary == 0)[0]
+    for i in inner[::5]:
+        c.g[i, ::4] *= -0.3
+    cfg = c.config(32, 0, 0, 2)
+    cfg.limiter = 0
+    s = ab.Solver(c, config=cfg)
+    assert s.counters()["particle_kernel"] == 3
+    o = Oracle.from_case(c, limiter=0)
+    for _ in range(2):
+        s.cudaStep(1)
+        st = o.step(1)
+        assert s.counters()["positivity_fixes"] == st["positivity_fixes"]
+    assert s.counters()["positivity_fixes"] > 0
+    g, m = s.cudaDownloadFull()
+    assert rel(g, o.g) < 3e-4
+    for q in (0, 4):
+        assert rel(m[:, q], o.macro[:, q]) < 5e-5, q
+    s.close()
 
 
 def test_streamed_particle_kernel_positivity_repair(gpu):
