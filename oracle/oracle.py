@@ -157,6 +157,12 @@ def ref_library() -> str | None:
     return None
 
 
+def ref_cuda_library() -> str | None:
+    """Path of the reference built with its own CUDA backend for sm_100a."""
+    p = os.path.join(REF_DIR, "libalebgk_refcuda.so")
+    return p if os.path.exists(p) else None
+
+
 class RefCase:
     """A case built and stepped by the reference's own CPU code."""
 
@@ -244,6 +250,21 @@ class RefCase:
 
     def set_threads(self, n):
         self.L.ref_set_threads(int(n))
+
+    def cuda_run(self, warmup: int, steps: int) -> float:
+        """Steps the case on the reference's own CUDA backend
+        (Solver/CudaBackend.cu; needs the library of :func:`ref_cuda_library`):
+        upload, ``warmup`` untimed and ``steps`` timed cudaStep calls, then the
+        moments come back into this case.  Returns ms per timed step."""
+        if not hasattr(self.L, "ref_cuda_run"):
+            raise RuntimeError("not the reference CUDA build (oracle/_ref/libalebgk_refcuda.so)")
+        ms = ctypes.c_double()
+        self.L.ref_cuda_run.argtypes = [_vp, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_double)]
+        rc = self.L.ref_cuda_run(self.h, int(warmup), int(steps), ctypes.byref(ms))
+        if rc != 0:
+            raise RuntimeError("the reference CUDA backend failed")
+        return ms.value
 
     def checkpoint_save(self, path: str) -> bool:
         """The reference's ckpt::save (Core/Checkpoint.hpp:84-155)."""

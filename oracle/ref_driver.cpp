@@ -25,6 +25,7 @@
 #include "TestCases.hpp"
 #include "Checkpoint.hpp"
 
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -419,5 +420,43 @@ void ref_checkpoint_sizes(int *out)
     out[1] = (int)sizeof(ckpt::PRec);
     out[2] = (int)sizeof(ckpt::BRec);
 }
+
+#ifdef ALEBGK_REF_CUDA
+// The reference's own CUDA backend (Solver/CudaBackend.cu, compiled
+// unmodified for sm_100a by oracle/Makefile's refcuda recipe), declared as
+// Solver/Solver.cpp:67-89 declares it.  Built only into
+// libalebgk_refcuda.so: the reference GPU path timed on the same case.
+}  // extern "C"
+void cudaUploadCloud(const std::vector<Particle> &P, const SimParameters &sp);
+void cudaStep(const SimParameters &sp, const CalcParameters &cp, double dt, double R);
+void cudaDownloadMoments(std::vector<Particle> &P);
+void cudaFreeCloud();
+extern "C" int cudaDeviceSynchronize(void);
+extern "C" {
+
+// Uploads the case's current state to the reference's device cloud, runs
+// `warmup` untimed steps and then `steps` timed steps of cudaStep (the
+// reference's GPU time loop body, Solver/Solver.cpp:301-303), with the
+// device synchronised on both sides of the timed region; the mean wall
+// time per step in *ms.  Downloads the moments (cudaDownloadMoments) into
+// the case afterwards, so that ref_get_macros reads the device result.
+int ref_cuda_run(void *h, int warmup, int steps, double *ms)
+{
+    auto *c = static_cast<RefCase *>(h);
+    cudaUploadCloud(c->P, c->sp);
+    for (int s = 0; s < warmup; ++s) cudaStep(c->sp, c->cp, c->dt, c->gc.R);
+    if (cudaDeviceSynchronize() != 0) return -1;
+    const auto t0 = std::chrono::high_resolution_clock::now();
+    for (int s = 0; s < steps; ++s) cudaStep(c->sp, c->cp, c->dt, c->gc.R);
+    if (cudaDeviceSynchronize() != 0) return -1;
+    const auto t1 = std::chrono::high_resolution_clock::now();
+    *ms = steps > 0 ? std::chrono::duration<double, std::milli>(t1 - t0).count() / steps : 0.0;
+    cudaDownloadMoments(c->P);
+    c->step += warmup + steps;
+    c->t += (warmup + steps) * c->dt;
+    cudaFreeCloud();
+    return 0;
+}
+#endif
 
 }  // extern "C"

@@ -1,8 +1,8 @@
-"""Checks the reference-side shim printed in INTEGRATION.md (test
-infrastructure, run where the reference sources are present).
+"""Checks the reference-side shim ``alebgk4paper_b200/shim/cuda_backend_shim.cpp``
+(test infrastructure, run where the reference sources are present).
 
-1. The shim's code block is extracted and compiled against the reference's
-   own headers and this project's ``include/alebgk.h``.
+1. The shim is compiled against the reference's own headers and this
+   project's ``include/alebgk.h``.
 2. The reference's ``Solver/Solver.cpp`` is compiled with ``ALEBGK_WITH_CUDA``
    (the build in which it calls the CUDA backend, ``Solver.cpp:67-89``).
 3. Every CUDA-backend symbol the solver object leaves undefined must be
@@ -24,11 +24,7 @@ ROOT = os.path.dirname(HERE)
 REF = os.environ.get("ALEBGK_REF", "/root/reference")
 
 
-def shim_source() -> str:
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    start = text.index("## The shim")
-    a = text.index("```cpp", start) + len("```cpp")
-    return text[a:text.index("```", a)]
+SHIM = os.path.join(ROOT, "alebgk4paper_b200", "shim", "cuda_backend_shim.cpp")
 
 
 def symbols(obj: str, defined: bool) -> set[str]:
@@ -51,8 +47,7 @@ def main() -> int:
     inc = [f"-I{os.path.join(REF, d)}" for d in sorted(os.listdir(REF))
            if os.path.isdir(os.path.join(REF, d))]
     with tempfile.TemporaryDirectory() as tmp:
-        shim = os.path.join(tmp, "alebgk_b200_shim.cpp")
-        open(shim, "w").write(shim_source())
+        shim = SHIM
         base = ["g++", "-std=c++17", "-O0", "-fopenmp", "-w"] + inc
         subprocess.run(base + ["-DALEBGK_WITH_CUDA", "-c", solver, "-o",
                                os.path.join(tmp, "solver.o")], check=True)

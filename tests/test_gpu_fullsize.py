@@ -1,0 +1,100 @@
+"""The headline configuration at full size against the reference itself.
+
+cavity3d, Nx = 40 (64 000 particles), Nv = 10 (1 000 velocities), quadratic
+MLS, the case's default dt, started from rest.  The fixture
+``step_c3d_n40_v10_q_s1_s10.npz`` holds the reference CPU build's own state
+after steps 1 and 10 (Solver/Solver.cpp:632-705 with mlsOrder = 2, written by
+``tests/golden/make_golden_c3d40.py``): every particle's moments and row sums,
+256 seeded full rows, and every step's transport-flag and moodCheck counts.
+
+FP64 mode is held to the FP64 contract with margin: 1e-10 relative on every
+moment field and sampled row, and the same MOOD decisions at every step.
+Velocity components are measured against the largest flow speed of the
+field (a component that is rounding noise at step 1, such as uy of a gas at
+rest under a lid moving in x, has no scale of its own).
+FP32 mode (FP32 f and reconstruction, FP64 sums) is held to its stated
+error against the same fixture: 5e-5 relative on rho and T and 2e-4 on the
+sampled rows, with flow velocities within 1e-3 of the lid speed.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+import alebgk4paper_b200 as ab
+
+pytestmark = pytest.mark.gpu
+
+FIXTURE = "step_c3d_n40_v10_q_s1_s10.npz"
+
+
+def relmax(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def field_errors(m, ref):
+    """Relative max error of rho, ux, uy, uz, T; velocities against the
+    largest flow speed of the reference field."""
+    uscale = max(np.abs(ref[:, 1:4]).max(), 1e-300)
+    return [relmax(m[:, 0], ref[:, 0])] + \
+        [float(np.abs(m[:, q] - ref[:, q]).max() / uscale) for q in (1, 2, 3)] + \
+        [relmax(m[:, 4], ref[:, 4])]
+
+
+@pytest.fixture(scope="module")
+def fx():
+    return golden(FIXTURE)
+
+
+def run(fx, precision):
+    """Steps the device run to 10 steps; the state at steps 1 and 10 and the
+    per-step decision counts."""
+    c = ab.Case("cavity3d", 40, 10, -1.0, 2)
+    s = ab.Solver(c, precision=precision)
+    rows = fx["rows"]
+    out, flags = {}, []
+    for step in range(1, 11):
+        s.cudaStep(1)
+        cnt = s.counters()
+        assert cnt["error_word"] == 0
+        flags.append([cnt["transport_flags"], cnt["mood_fail"]])
+        if step in (1, 10):
+            g, m = s.cudaDownloadFull()
+            out[step] = dict(macro=m[:, :5].copy(), gsum=g.sum(axis=1),
+                             gabs=np.abs(g).sum(axis=1), g=g[rows].copy())
+            del g
+    s.close()
+    return out, np.array(flags)
+
+
+def test_fp64_matches_reference_at_full_size(gpu, fx):
+    out, flags = run(fx, 64)
+    # The MOOD decisions of every step: step 1 flags every interior particle,
+    # steps 4-10 a few hundred to a thousand.
+    np.testing.assert_array_equal(flags, fx["flags"])
+    for step in (1, 10):
+        o = out[step]
+        err = field_errors(o["macro"], fx[f"macro_s{step}"])
+        print("FP64 vs reference at step", step, "rho ux uy uz T:", err)
+        assert max(err) < 1e-10, (step, err)
+        assert relmax(o["gsum"], fx[f"gsum_s{step}"]) < 1e-10
+        assert relmax(o["gabs"], fx[f"gabs_s{step}"]) < 1e-10
+        assert relmax(o["g"], fx[f"g_s{step}"]) < 1e-10
+
+
+def test_fp32_error_against_reference_at_full_size(gpu, fx):
+    out, flags = run(fx, 32)
+    # Step 1 flags every interior particle in both precisions.
+    assert flags[0, 0] == fx["flags"][0, 0]
+    assert (flags[:, 1] == 0).all()
+    errs = {}
+    for step in (1, 10):
+        o = out[step]
+        ref = fx[f"macro_s{step}"]
+        errs[step] = field_errors(o["macro"], ref)
+        assert errs[step][0] < 5e-5 and errs[step][4] < 5e-5, errs[step]
+        # flow velocities (up to the 1 m/s lid speed): absolute, in m/s
+        for q in (1, 2, 3):
+            assert np.abs(o["macro"][:, q] - ref[:, q]).max() < 1e-3, (step, q)
+        assert relmax(o["g"], fx[f"g_s{step}"]) < 2e-4
+    print("FP32 vs reference, relative max error of rho ux uy uz T:", errs)

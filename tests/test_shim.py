@@ -1,4 +1,4 @@
-"""The reference-side shim printed in INTEGRATION.md compiles against the
+"""The reference-side shim (alebgk4paper_b200/shim/cuda_backend_shim.cpp) compiles against the
 reference's own headers and this project's C-ABI header, and defines every
 CUDA-backend function the reference's Solver.cpp calls (Solver.cpp:67-89),
 with the reference's signatures (oracle/shim_check.py)."""
