@@ -461,6 +461,14 @@ class Solver:
         """Velocities per lane of the lattice march (2: packed FMAs, or 1)."""
         _check(self.lib.alebgk_set_march_width(self.ctx, int(velocities_per_lane)), self.ctx)
 
+    def set_residual_speed(self, speed: float):
+        """Speed scale of the residual's momentum terms (0: thermal speed)."""
+        _check(self.lib.alebgk_set_residual_speed(self.ctx, float(speed)), self.ctx)
+
+    def set_nad_floor(self, rel: float):
+        """Relative rounding floor of the FP32 NAD screen (default 64 * 2^-24)."""
+        _check(self.lib.alebgk_set_nad_floor(self.ctx, float(rel)), self.ctx)
+
     def get_launch(self):
         t = ctypes.c_int()
         w = ctypes.c_int()

@@ -100,6 +100,8 @@ SIGNATURES = {
     "alebgk_set_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "alebgk_get_launch": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p]),
     "alebgk_set_march_width": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "alebgk_set_nad_floor": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "alebgk_set_residual_speed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "alebgk_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_float)]),
     "alebgk_residual": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
@@ -110,6 +112,7 @@ SIGNATURES = {
     "alebgk_batch_set_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "alebgk_batch_get_mode": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p]),
     "alebgk_batch_set_groups": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "alebgk_batch_set_spin_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
     "alebgk_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_float)]),
     "alebgk_batch_residuals": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),

@@ -82,14 +82,27 @@ class BatchSolver:
     plain transport and particle kernels); ``launch="branches"`` puts every
     cavity's own step in the graph as a parallel branch.  Both compute each
     cavity exactly as it would step alone.
+
+    ``residual="lid"`` measures each cavity's steady residual's momentum
+    terms against its lid momentum rho U_lid (the spec's ``lid_speed``),
+    ``residual="flow"`` against the flow's own momentum rho |u|, and
+    ``residual="thermal"`` (the default) against the thermal momentum.
     """
 
+    # launch forms: one launch per step stage in groups of cavities, every
+    # cavity's own step as a graph branch, or the whole step in one
+    # persistent cooperative launch
+    _LAUNCH = {"stages": 0, "branches": 1, "persistent": 2}
+
     def __init__(self, specs, precision: int = 32, device: int = 0, autotune: bool = False,
-                 tune_steps: int = 3, setup: str = "host", launch: str = "stages"):
+                 tune_steps: int = 3, setup: str = "host", launch: str = "stages",
+                 residual: str = "thermal"):
+        if residual not in ("thermal", "lid", "flow"):
+            raise ValueError("residual must be 'thermal', 'lid' or 'flow'")
         if setup not in ("host", "device"):
             raise ValueError("setup must be 'host' or 'device'")
-        if launch not in ("stages", "branches"):
-            raise ValueError("launch must be 'stages' or 'branches'")
+        if launch not in self._LAUNCH:
+            raise ValueError("launch must be 'stages', 'branches' or 'persistent'")
         self.lib = _abi.load()
         self.specs = list(specs)
         self.cases = []
@@ -99,7 +112,12 @@ class BatchSolver:
             name = kw.pop("name")
             c = LatticeCase(name, **kw) if setup == "device" else Case(name, **kw)
             self.cases.append(c)
-            self.solvers.append(Solver(c, precision=precision, device=device))
+            s = Solver(c, precision=precision, device=device)
+            if residual == "lid":
+                s.set_residual_speed(float(sp.get("lid_speed", 0.0)))
+            elif residual == "flow":
+                s.set_residual_speed(-1.0)
+            self.solvers.append(s)
         self.tuned_ms = None
         if autotune:
             self.tuned_ms = [s.autotune(tune_steps) for s in self.solvers]
@@ -109,7 +127,7 @@ class BatchSolver:
         _check(self.lib.alebgk_batch_create(n, arr, ctypes.byref(h)), self.solvers[0].ctx)
         self.h = h
         self.steps = 0
-        _check(self.lib.alebgk_batch_set_mode(self.h, 0 if launch == "stages" else 1),
+        _check(self.lib.alebgk_batch_set_mode(self.h, self._LAUNCH[launch]),
                self.solvers[0].ctx)
         self.batch_tuned_ms = None
         if autotune:
@@ -117,12 +135,13 @@ class BatchSolver:
 
     def autotune(self, steps: int = 3) -> float:
         """Times the batch's launch forms (stage launches in 1, 2, 4, 8
-        groups; per-cavity branches) and keeps the fastest.  The timed steps
-        are real steps of the batch (every form computes the same states)."""
+        groups; one persistent launch; per-cavity branches) and keeps the
+        fastest.  The timed steps are real steps of the batch (every form
+        computes the same states)."""
         ms = ctypes.c_float()
         _check(self.lib.alebgk_batch_autotune(self.h, int(steps), ctypes.byref(ms)),
                self.solvers[0].ctx)
-        forms = 1 + sum(1 for g in (1, 2, 4, 8) if g <= len(self.solvers))
+        forms = 2 + sum(1 for g in (1, 2, 4, 8) if g <= len(self.solvers))
         self.steps += forms * (int(steps) + 2)
         return float(ms.value)
 
@@ -137,6 +156,24 @@ class BatchSolver:
 
     def set_groups(self, groups: int):
         _check(self.lib.alebgk_batch_set_groups(self.h, int(groups)), self.solvers[0].ctx)
+
+    def set_launch(self, launch: str):
+        """Switches the launch form ('stages', 'branches', 'persistent')."""
+        if launch not in self._LAUNCH:
+            raise ValueError("launch must be 'stages', 'branches' or 'persistent'")
+        _check(self.lib.alebgk_batch_set_mode(self.h, self._LAUNCH[launch]), self.solvers[0].ctx)
+
+    @property
+    def launch(self) -> str:
+        mode, staged = ctypes.c_int(), ctypes.c_int()
+        _check(self.lib.alebgk_batch_get_mode(self.h, ctypes.byref(mode), ctypes.byref(staged)),
+               self.solvers[0].ctx)
+        return {v: k for k, v in self._LAUNCH.items()}[int(mode.value)]
+
+    def set_spin_limit(self, polls: int):
+        """Polls of the persistent launch's grid barrier before it gives up
+        (sets bit 8 of the first cavity's error word and ends the step)."""
+        _check(self.lib.alebgk_batch_set_spin_limit(self.h, int(polls)), self.solvers[0].ctx)
 
     @property
     def updates_per_step(self) -> int:

@@ -47,7 +47,6 @@ void freeBuffers(alebgk_ctx *c)
     void *ptrs[] = {d.f[0], d.f[1], d.coef, d.coefLin, d.pos, d.meshv, d.wall,
                     d.boundary, d.bodyId, d.cls, d.nslot, d.slots, d.macro[0],
                     d.macro[1], d.mood, d.flag, d.flagList, d.degList, d.massPos, d.massEnd, d.minG, d.nad, d.redPartial,
-                    d.rowSums, d.rowTab, d.rowKind,
                     d.dpx, d.bodyTmp, d.bodyOut, d.stage, d.surfList, d.bodyIO, d.rankAll, d.sc};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -58,7 +57,6 @@ void freeBuffers(alebgk_ctx *c)
     if (c->march.units) cudaFree(c->march.units);
     if (c->march.coefT) cudaFree(c->march.coefT);
     if (c->march.coefTy) cudaFree(c->march.coefTy);
-    if (c->march.gather) cudaFree(c->march.gather);
     c->march = MarchState();
     for (auto &g : c->graph)
         if (g) { cudaGraphExecDestroy(g); g = nullptr; }
@@ -272,7 +270,9 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
         if (e != cudaSuccess || src.empty()) return e;
         if (f64) return cudaMemcpy(*dst, src.data(), ncoef * 8, cudaMemcpyHostToDevice);
         std::vector<float> cf(ncoef);
-        for (size_t q = 0; q < ncoef; ++q) cf[q] = (float)src[q];
+        const size_t per = (size_t)tb.S * tb.V;
+        for (int c = 0; c < tb.ncls; ++c)
+            roundCoefFP32(&src[c * per], &cf[c * per], tb.S, tb.V);
         return cudaMemcpy(*dst, cf.data(), ncoef * 4, cudaMemcpyHostToDevice);
     };
     c->coefCap = std::max<size_t>(ncoef, 1);
@@ -315,10 +315,6 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
     CK(dalloc(&d.massEnd, N));
     CK(dalloc(&d.minG, N));
     CK(dalloc(&d.nad, 2 * (size_t)N));
-    p.tabStride = (3 * p.Nv + 2 + 3) / 4 * 4;
-    CK(dalloc(&d.rowSums, 6 * (size_t)N));
-    CK(dalloc(&d.rowTab, (size_t)N * p.tabStride));
-    CK(dalloc(&d.rowKind, N));
     CK(dalloc(&d.redPartial, 256));
     CK(dalloc(&d.dpx, N));
     CK(dalloc(&d.bodyTmp, 6 * (size_t)N));
@@ -376,13 +372,6 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
             CK(cudaMalloc(&m.units, sizeof(MarchUnit) * m.nunits));
             CK(cudaMemcpy(m.units, all.data(), sizeof(MarchUnit) * m.nunits,
                           cudaMemcpyHostToDevice));
-            m.ngather = (int)plan.gatherList.size();
-            if (m.ngather > 0)
-            {
-                CK(cudaMalloc(&m.gather, 4 * (size_t)m.ngather));
-                CK(cudaMemcpy(m.gather, plan.gatherList.data(), 4 * (size_t)m.ngather,
-                              cudaMemcpyHostToDevice));
-            }
             CK(cudaMalloc(&m.coefT, plan.coefT.size() * 4));
             CK(cudaMemcpy(m.coefT, plan.coefT.data(), plan.coefT.size() * 4,
                           cudaMemcpyHostToDevice));
@@ -838,7 +827,7 @@ int alebgk_get_counters(alebgk_ctx *c, alebgk_counters *out)
     out->mass_before = s.sigma * s.massNew;
     out->error_word = s.err;
     out->transport_kernel = c->march.enabled ? 2 : 1;
-    out->particle_kernel = c->pStream ? (c->pSplit ? 3 : 2) : 1;
+    out->particle_kernel = c->pStream ? (c->pRows ? 3 : 2) : 1;
     return ALEBGK_OK;
 }
 

@@ -11,12 +11,16 @@
 // batch size, and the short stages of one group overlap the long ones of
 // another.  Otherwise one graph per ping-pong parity holds every context's
 // whole step (and its residual) as a parallel branch: a master stream forks
-// to each context's stream and joins them again.  Both forms compute each
-// context exactly as its own step does.
+// to each context's stream and joins them again.  A third form (mode 2)
+// puts the whole step of all contexts into one persistent cooperative
+// launch: every stage's blocks spread over the resident grid, a bounded
+// grid-wide barrier between stages.  All forms compute each context exactly
+// as its own step does.
 #include <algorithm>
 #include <cuda_runtime.h>
 
 #include <string>
+#include <cmath>
 #include <vector>
 
 #include "ctx.h"
@@ -32,12 +36,14 @@ struct alebgk_batch
     std::vector<cudaEvent_t> join;
     double *resid = nullptr;              // device, one per context
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    int mode = 0;                         // 0 stage launches when possible, 1 branches
+    int mode = 0;                         // 0 stage launches when possible, 1 branches,
+                                          // 2 one persistent launch when possible
     bool staged = false;                  // the graphs hold stage launches
     bool planned = false;                 // the stage groups were tried
     std::vector<BatchLaunch> groups;      // stage launches per group
     std::vector<int> groupStream;         // context whose stream runs the group
     int ngroups = 4;                      // stage groups wanted
+    long long spinCap = 1ll << 24;        // grid-barrier polls before giving up (mode 2)
     std::vector<unsigned long long> epochs;   // the contexts' epochs of the captured graphs
     std::string err;
 };
@@ -80,7 +86,9 @@ void freeGroups(alebgk_batch *b)
 cudaError_t planGroups(alebgk_batch *b)
 {
     const int n = (int)b->ctx.size();
-    const int G = std::max(1, std::min(b->ngroups, n));
+    // one persistent launch holds the whole batch: a second one beside it
+    // could not be resident at the same time
+    const int G = b->mode == 2 ? 1 : std::max(1, std::min(b->ngroups, n));
     std::vector<int> order(n);
     for (int i = 0; i < n; ++i) order[i] = i;
     auto cost = [&](int i) {
@@ -108,6 +116,8 @@ cudaError_t planGroups(alebgk_batch *b)
             rs.push_back(b->resid + i);
         }
         cudaError_t e = buildBatchLaunch(cs.data(), (int)cs.size(), rs.data(), b->groups[g]);
+        b->groups[g].persistent = b->mode == 2;
+        b->groups[g].spinCap = b->spinCap;
         if (e == cudaSuccess) e = prepareBatchLaunch(b->groups[g]);
         if (e != cudaSuccess) return e;
         b->groupStream.push_back(member[g][0]);
@@ -157,6 +167,25 @@ int alebgk_set_march_width(alebgk_ctx *c, int velocities_per_lane)
                                               p.ldf, true, m.vpl, &err)))
             return failc(c, ALEBGK_ECUDA, err);
     }
+    dropGraphs(c);
+    return ALEBGK_OK;
+}
+
+int alebgk_set_nad_floor(alebgk_ctx *c, double rel)
+{
+    if (!c) return ALEBGK_EINVAL;
+    if (!(rel >= 0.0) || rel > 1e-2)
+        return failc(c, ALEBGK_EINVAL, "the NAD rounding floor is a relative slack in [0, 1e-2]");
+    c->sp.nadNoise = rel;
+    dropGraphs(c);
+    return ALEBGK_OK;
+}
+
+int alebgk_set_residual_speed(alebgk_ctx *c, double speed)
+{
+    if (!c) return ALEBGK_EINVAL;
+    if (!std::isfinite(speed)) return failc(c, ALEBGK_EINVAL, "the residual speed is finite");
+    c->sp.resU = speed;
     dropGraphs(c);
     return ALEBGK_OK;
 }
@@ -336,7 +365,7 @@ int alebgk_batch_step(alebgk_batch *b, int nsteps)
     for (int n = 0; n < nsteps; ++n)
     {
         const int from = c->cur;
-        if (b->mode == 0 && !b->planned)
+        if (b->mode != 1 && !b->planned)
         {
             const cudaError_t be = planGroups(b);
             if (be != cudaSuccess)
@@ -401,7 +430,7 @@ int alebgk_batch_step(alebgk_batch *b, int nsteps)
 
 int alebgk_batch_set_mode(alebgk_batch *b, int mode)
 {
-    if (!b || mode < 0 || mode > 1) return ALEBGK_EINVAL;
+    if (!b || mode < 0 || mode > 2) return ALEBGK_EINVAL;
     if (mode != b->mode)
     {
         cudaSetDevice(b->device);
@@ -437,6 +466,21 @@ int alebgk_batch_set_groups(alebgk_batch *b, int groups)
     return ALEBGK_OK;
 }
 
+int alebgk_batch_set_spin_limit(alebgk_batch *b, long long polls)
+{
+    if (!b || polls < 0) return ALEBGK_EINVAL;
+    if (polls != b->spinCap)
+    {
+        cudaSetDevice(b->device);
+        cudaStreamSynchronize(b->master);
+        for (auto &g : b->graph)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        freeGroups(b);
+        b->spinCap = polls;
+    }
+    return ALEBGK_OK;
+}
+
 int alebgk_batch_autotune(alebgk_batch *b, int steps, float *best_ms)
 {
     if (!b || steps < 1) return ALEBGK_EINVAL;
@@ -445,11 +489,13 @@ int alebgk_batch_autotune(alebgk_batch *b, int steps, float *best_ms)
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     CKC(cudaEventCreate(&t0));
     CKC(cudaEventCreate(&t1));
-    // candidates: stage launches in 1, 2, 4, 8 groups, then branches
+    // candidates: stage launches in 1, 2, 4, 8 groups, one persistent
+    // launch, then branches
     struct Cand { int mode, groups; };
     std::vector<Cand> cands;
     for (int g : {1, 2, 4, 8})
         if (g <= (int)b->ctx.size()) cands.push_back({0, g});
+    cands.push_back({2, 1});
     cands.push_back({1, b->ngroups});
     float best = -1.0f;
     Cand pick = {b->mode, b->ngroups};

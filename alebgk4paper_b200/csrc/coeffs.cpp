@@ -312,4 +312,24 @@ bool buildCoefficients(const CoeffInput &in, CoeffTables &out, std::string *err)
     return true;
 }
 
+void roundCoefFP32(const double *src, float *dst, int S, int V)
+{
+    for (int k = 0; k < V; ++k)
+    {
+        double s64 = 0.0, s32 = 0.0, big = -1.0;
+        int smax = 0;
+        for (int s = 0; s < S; ++s)
+        {
+            const double c = src[(size_t)s * V + k];
+            const float c32 = (float)c;
+            dst[(size_t)s * V + k] = c32;
+            s64 += c;
+            s32 += (double)c32;
+            if (std::fabs(c) > big) { big = std::fabs(c); smax = s; }
+        }
+        const size_t q = (size_t)smax * V + k;
+        dst[q] = (float)((double)dst[q] + (s64 - s32));
+    }
+}
+
 }  // namespace alebgk

@@ -54,6 +54,17 @@ struct CoeffTables
 // Builds classes and coefficients.  Returns false with *err on bad input.
 bool buildCoefficients(const CoeffInput &in, CoeffTables &out, std::string *err);
 
+// FP32 image of the FP64 coefficients of one class, [S slots][V nodes]: each
+// node's coefficients are rounded to nearest, then the largest of them (in
+// magnitude, the first in slot order on a tie) takes the FP64 difference
+// between the FP64 sum and the sum of the rounded values.  The FP32
+// stencil then reproduces a constant field to within half an FP32 ulp of
+// its largest coefficient, instead of to the accumulated rounding of all of
+// them; a uniform state transports without a systematic density bias of
+// order 1e-7, which would otherwise swamp the 1e-9 slack of the MOOD NAD
+// screen (MLSTransport.cpp:370).  The device table builder does the same.
+void roundCoefFP32(const double *src, float *dst, int S, int V);
+
 // The class part alone (cls, nslot, slots, rep, members, order; no coef).
 bool buildClasses(const CoeffInput &in, CoeffTables &out, std::string *err);
 

@@ -178,6 +178,10 @@ __global__ void k_class_tables(ClassArgs a, int order0, const int *__restrict__ 
     for (int q = 0; q < 100; ++q) B[q] = 0.0;
     for (int m = 0; m < P; ++m) B[m * P + m] = 1.0;
     if (solveSkipGED(A, B, P, P) > 0) atomicAdd(degen + c, 1);
+    // FP32 tables: the largest coefficient takes the rounding of the node's
+    // sum, as roundCoefFP32 does on the host (same order, same operations).
+    double s64 = 0.0, s32 = 0.0, big = -1.0;
+    int smax = 0;
     for (int s = 1; s < n; ++s)
     {
         double dx, dy, dz;
@@ -188,7 +192,19 @@ __global__ void k_class_tables(ClassArgs a, int order0, const int *__restrict__ 
         basisD(dx, dy, dz, ndim, a.h, b, order);
         double acc = 0.0;
         for (int m = 0; m < P; ++m) acc += B[m] * b[m];
-        cc[(size_t)s * V + k] = (T)(ws * acc);
+        const double c = ws * acc;
+        cc[(size_t)s * V + k] = (T)c;
+        if (sizeof(T) == 4)
+        {
+            s64 += c;
+            s32 += (double)(T)c;
+            if (fabs(c) > big) { big = fabs(c); smax = s; }
+        }
+    }
+    if (sizeof(T) == 4 && big > 0.0)
+    {
+        const size_t q = (size_t)smax * V + k;
+        cc[q] = (T)((double)cc[q] + (s64 - s32));
     }
 }
 

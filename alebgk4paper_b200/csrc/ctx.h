@@ -20,8 +20,6 @@ struct MarchState
     int vpl = 2;                              // velocities per lane (1 or 2)
     MarchUnit *units = nullptr;               // y-march units first, then z-march
     float *coefT = nullptr, *coefTy = nullptr;
-    int *gather = nullptr;                    // particles the gather transports
-    int ngather = 0;
     alignas(64) unsigned char tmap[2][128];   // CUtensorMap per source buffer
     alignas(64) unsigned char tmapY[2][128];  // the same with the y-march box
 };
@@ -67,9 +65,6 @@ struct DeviceBuffers
     double *massEnd = nullptr;         // per particle: mass of h at step end
     double *minG = nullptr;            // per particle: min of h over the mass layer
     double *nad = nullptr;             // per particle: NAD neighbour density range (lo, hi)
-    double *rowSums = nullptr;         // per particle: 6 row sums (three-kernel particle stage)
-    float *rowTab = nullptr;           // per particle: collision table (tabStride floats)
-    int *rowKind = nullptr;            // per particle: 1 collided by k_row_collide, else 0
     double *redPartial = nullptr;      // per-block partials of the grid sums
     double *dpx = nullptr;
     double *bodyTmp = nullptr;         // N x 6 per-particle load contributions
@@ -98,7 +93,7 @@ struct StepParams
     // ulp of FP32, far above the reference's 1e-9 absolute slack near a
     // uniform state, so the screen would flag rounding noise.
     double nadNoise = 0;
-    int tabStride = 0;    // floats per particle of the collision table (3 Nv + 2, padded)
+    double resU = 0;      // momentum speed scale of the steady residual (0: thermal)
 };
 
 }  // namespace alebgk
@@ -142,10 +137,9 @@ struct alebgk_ctx
     bool pStream = false;
     int pStreamWpb = 0, pStreamBlocks = 0;
     size_t pStreamSmem = 0;
-    // Three-kernel form of the streamed stages (FP32): on, launch sizes.
-    bool pSplit = false;
-    int pSumsBlocks = 0, pCollBlocks = 0;
-    size_t pSumsSmem = 0, pCollSmem = 0;
+    // Register-row form of the streamed stages (FP32, Nv <= 10): on, blocks.
+    bool pRows = false;
+    int pRowsBlocks = 0;
     std::string err;
     std::vector<int> bodyIdHost;
     int maxBodyId = -1;          // largest entry of bodyIdHost (-1: no body particle)
@@ -183,6 +177,12 @@ struct BatchLaunch
     bool f64 = false;
     size_t smemParticle = 0, smemRedo = 0;
     int blocks[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    // One persistent launch per step instead of one launch per stage: its
+    // grid (co-resident blocks), the grid barrier's words and poll limit.
+    bool persistent = false;
+    int pGrid = 0;
+    unsigned *bar = nullptr;
+    long long spinCap = 1ll << 24;
 };
 // cudaErrorNotSupported when the clouds cannot share launches (mixed
 // precision or layers, the streamed particle kernel or the lattice march).
@@ -261,15 +261,7 @@ cudaError_t bodyLoadsNoAlloc(alebgk_ctx *c, int nbodies, const double *centre,
 cudaError_t launchResidual(alebgk_ctx *c, double *out, cudaStream_t st);
 cudaError_t launchConvertIn(alebgk_ctx *c, const double *src, int buf);
 cudaError_t launchConvertOut(alebgk_ctx *c, double *dst, int buf);
-// The lattice march of buffer `from` into outBuf on st; the gather of the
-// particles its units leave out goes on gatherStream (nullptr: launched by
-// the caller with launchTransportList).
-cudaError_t launchMarch(alebgk_ctx *c, int from, float *outBuf, cudaStream_t st,
-                        cudaStream_t gatherStream);
-// Coefficient-gather transport of the listed particles (step.cu): the
-// particles of a lattice that the march's units leave out.
-cudaError_t launchTransportList(alebgk_ctx *c, int from, float *outBuf, const int *list, int n,
-                                cudaStream_t st);
+cudaError_t launchMarch(alebgk_ctx *c, int from, float *outBuf, cudaStream_t st);
 cudaError_t prepareMarch();
 bool encodeMarchMap(void *tmapOut, void *f, int V, int Nx, int Ny, int Nz, int ldf,
                     bool yMarch, int vpl, std::string *err);

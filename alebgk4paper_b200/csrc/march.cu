@@ -19,11 +19,11 @@
 // plane is complete two input planes after its own and is stored straight
 // from the queue; planes outside the lattice are zero and are skipped.  Long
 // segments run every queue slot without tests; short ones (the single-plane
-// wall layers) only the slots of their own output planes.  Thread 0 refills
-// a ring slot two planes after the warps released it, so the warps of a CTA
-// may drift apart by two planes without stalling the loads, which run four
-// planes ahead.  Every wait is bounded; a timeout sets the step's error word
-// instead of hanging.  Packed and scalar FMAs round alike (each half of
+// wall layers) only the slots of their own output planes.  The last warp to
+// release a ring slot refills it at once (a shared-memory count per slot),
+// so no warp ever waits for the others to free a slot and the loads run as
+// far ahead as the ring allows.  Every wait is bounded; a timeout sets the
+// step's error word instead of hanging.  Packed and scalar FMAs round alike (each half of
 // fma.rn.f32x2 is one fmaf), so both widths give the same bits.
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -42,8 +42,6 @@ namespace {
 constexpr int kPW = kMarchTileX + 4;      // staged plane: 12 x 8 particles
 constexpr int kPH = kMarchTileY + 4;
 constexpr int kRing = 6;                  // staged planes
-constexpr int kLag = 2;                   // refill lag behind the consumers
-static_assert(kLag < kRing, "ring");
 // Bytes of one staged plane at VPL velocities per lane.
 template <int VPL>
 __host__ __device__ constexpr uint32_t planeBytes() { return kPW * kPH * kMarchChunk * VPL * 4; }
@@ -123,7 +121,8 @@ k_march(const __grid_constant__ CUtensorMap tmapZ, const __grid_constant__ CUten
     extern __shared__ __align__(128) unsigned char marchSmem[];
     typedef VT Plane[kPH][kPW][kMarchChunk];
     Plane *ring = reinterpret_cast<Plane *>(marchSmem);
-    __shared__ __align__(8) uint64_t full[kRing], empty[kRing];
+    __shared__ __align__(8) uint64_t full[kRing];
+    __shared__ int relCnt[kRing];
     __shared__ int giveUp;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -160,7 +159,7 @@ k_march(const __grid_constant__ CUtensorMap tmapZ, const __grid_constant__ CUten
         for (int s = 0; s < kRing; ++s)
         {
             mbarInit(&full[s], 1);
-            mbarInit(&empty[s], kMarchWarps);
+            relCnt[s] = 0;
         }
         mbarInitFence();
     }
@@ -277,20 +276,27 @@ k_march(const __grid_constant__ CUtensorMap tmapZ, const __grid_constant__ CUten
             acc[c][4] = LN::zero();
         }
     };
-    // Consumer release of staged plane m, then the producer's lagged refill.
-    // Staged plane m sits in ring slot s with phase parity par.
+    // Consumer release of staged plane m in ring slot s: the last warp to
+    // release the slot refills it at once with plane m + kRing.
     auto release = [&](int m, int s, uint32_t par) {
         __syncwarp();
-        if (lane == 0) mbarArrive(&empty[s]);
-        const int mr = m - kLag;
-        if (threadIdx.x == 0 && mr >= 0 && mr + kRing < nv)
+        if (lane == 0)
         {
-            const int sr = (s >= kLag) ? s - kLag : s - kLag + kRing;
-            const uint32_t pr = (s >= kLag) ? par : par ^ 1u;
-            mbarWait(&empty[sr], pr, dead);
-            mbarExpectTx(&full[sr], kPlaneBytes);
-            loadPlane(&ring[sr][0][0][0], &full[sr], zlo + mr + kRing);
+            __threadfence_block();
+            const int prev = atomicAdd(&relCnt[s], 1);
+            if (prev == kMarchWarps - 1)
+            {
+                __threadfence_block();
+                relCnt[s] = 0;
+                if (m + kRing < nv)
+                {
+                    fenceProxyAsync();
+                    mbarExpectTx(&full[s], kPlaneBytes);
+                    loadPlane(&ring[s][0][0][0], &full[s], zlo + m + kRing);
+                }
+            }
         }
+        (void)par;
     };
 
     // Long segment: every input plane is staged (the TMA zero-fills any
@@ -411,8 +417,7 @@ cudaError_t prepareMarch()
     return e;
 }
 
-cudaError_t launchMarch(alebgk_ctx *c, int from, float *outBuf, cudaStream_t st,
-                        cudaStream_t gatherStream)
+cudaError_t launchMarch(alebgk_ctx *c, int from, float *outBuf, cudaStream_t st)
 {
     const StepParams &p = c->sp;
     const MarchState &ms = c->march;
@@ -430,11 +435,7 @@ cudaError_t launchMarch(alebgk_ctx *c, int from, float *outBuf, cudaStream_t st,
                      kRing * planeBytes<1>(), st>>>(*tz, *ty, ms.units, ms.coefT, cy, outBuf,
                                                     p.ldf, ms.Nx, ms.Ny, ms.Nz, p.V, ms.Vpad,
                                                     c->d.sc);
-    cudaError_t e = cudaGetLastError();
-    // the particles no unit covers, on the given side stream (or st)
-    if (e == cudaSuccess && ms.ngather > 0 && gatherStream)
-        e = launchTransportList(c, from, outBuf, ms.gather, ms.ngather, gatherStream);
-    return e;
+    return cudaGetLastError();
 }
 
 }  // namespace alebgk

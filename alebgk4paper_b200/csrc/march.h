@@ -47,11 +47,6 @@ struct MarchPlan
     int ncls = 0, Vpad = 0;
     std::vector<MarchUnit> units;    // marching through z
     std::vector<MarchUnit> unitsY;   // thin z-planes, marching through y
-    // Particles no unit covers: those of thin z-planes whose y is next to a
-    // y wall (the lines along x where a z wall meets a y wall).  Marching
-    // them would take one-plane units, each paying a whole pipeline fill for
-    // one output plane; the coefficient gather transports them instead.
-    std::vector<int> gatherList;
     std::vector<float> coefT;        // [class][81][Vpad]
     std::vector<float> coefTy;       // the same in the y-march frame
     std::vector<float> coefTLin;     // same, linear MLS

@@ -120,25 +120,29 @@ void buildMarchPlan(const double *xyz, int N, int dim, const int *nnb, const int
     plan.Nx = nx; plan.Ny = ny; plan.Nz = nz; plan.ncls = ncls; plan.Vpad = Vpad;
     plan.coefT.assign((size_t)ncls * kTmplOffsets * Vpad, 0.0f);
     if (tl) plan.coefTLin.assign((size_t)ncls * kTmplOffsets * Vpad, 0.0f);
+    // FP32 images of the class tables (roundCoefFP32), re-laid by offset.
+    std::vector<float> img((size_t)S * V), imgLin(tl ? (size_t)S * V : 0);
     for (int c = 0; c < ncls; ++c)
     {
         const int r = tb.rep[c];
         int xr, yr, zr;
         coord(r, xr, yr, zr);
         const int *sl = &tb.slots[(size_t)r * S];
+        roundCoefFP32(&tb.coef[(size_t)c * S * V], img.data(), S, V);
+        if (tl) roundCoefFP32(&tl->coef[(size_t)c * S * V], imgLin.data(), S, V);
         for (int s = 0; s < tb.nslot[r]; ++s)
         {
             int xj, yj, zj;
             coord(sl[s], xj, yj, zj);
             const int o = templateIndex(xj - xr, yj - yr, zj - zr);
-            const double *src = &tb.coef[((size_t)c * S + s) * V];
+            const float *src = &img[(size_t)s * V];
             float *dst = &plan.coefT[((size_t)c * kTmplOffsets + o) * Vpad];
-            for (int k = 0; k < V; ++k) dst[k] = (float)src[k];
+            for (int k = 0; k < V; ++k) dst[k] = src[k];
             if (tl)
             {
-                const double *sl2 = &tl->coef[((size_t)c * S + s) * V];
+                const float *sl2 = &imgLin[(size_t)s * V];
                 float *d2 = &plan.coefTLin[((size_t)c * kTmplOffsets + o) * Vpad];
-                for (int k = 0; k < V; ++k) d2[k] = (float)sl2[k];
+                for (int k = 0; k < V; ++k) d2[k] = sl2[k];
             }
         }
     }
@@ -229,21 +233,12 @@ void buildMarchPlan(const double *xyz, int N, int dim, const int *nnb, const int
         }
     };
 
-    // z-march units: every long z-segment.  Thin planes go to the y-march,
-    // except the columns whose y is next to a y wall: those go to the gather.
+    // z-march units: every long z-segment; in thin planes only the columns
+    // whose y is next to a y wall (the rest go to the y-march).
     for (size_t sgi = 0; sgi + 1 < cuts.size(); ++sgi)
     {
         const int za = cuts[sgi], zb = cuts[sgi + 1];
         const bool isThin = zb - za < kThinSegment;
-        if (isThin)
-        {
-            for (int z = za; z < zb; ++z)
-                for (int y = 0; y < ny; ++y)
-                    if (!yLong[y])
-                        for (int x = 0; x < nx; ++x)
-                            plan.gatherList.push_back(x + nx * (y + ny * z));
-            continue;
-        }
         for (int y0 = 0; y0 < ny; y0 += kMarchTileY)
             for (int x0 = 0; x0 < nx; x0 += kMarchTileX)
             {
@@ -252,7 +247,8 @@ void buildMarchPlan(const double *xyz, int N, int dim, const int *nnb, const int
                     for (int bx = 0; bx < kMarchTileX; ++bx)
                     {
                         const int x = x0 + bx, y = y0 + by;
-                        tc[by][bx] = (x < nx && y < ny) ? cls(x, y, za) : -1;
+                        tc[by][bx] = (x < nx && y < ny && !(isThin && yLong[y]))
+                                         ? cls(x, y, za) : -1;
                     }
                 std::vector<int> subs;
                 coverTile(tc, subs);

@@ -254,22 +254,6 @@ k_transport(const T *__restrict__ f, T *__restrict__ g,
     k_transport_body(f, g, coef, cls, nslot, slots, S, N, V, L, ldf, sc, blockIdx.x, blockIdx.y);
 }
 
-// The same transport for a list of particles: block = list entries, one per
-// warp, at one velocity chunk.
-template <typename T>
-__global__ void __launch_bounds__(kNT)
-k_transport_list(const T *__restrict__ f, T *__restrict__ g, const T *__restrict__ coef,
-                 const int *__restrict__ cls, const int *__restrict__ nslot,
-                 const int *__restrict__ slots, const int *__restrict__ list, int n, int S,
-                 int V, int ldf, const StepScalars *__restrict__ sc)
-{
-    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int li = blockIdx.y * nw + warp;
-    if (li >= n) return;
-    transportRow<T, 1>(f, g, coef, cls, nslot, slots, S, V, ldf, T(sc->scale), list[li],
-                       blockIdx.x, transportChunks(V), threadIdx.x & 31);
-}
-
 // Walks the nodes k = lane, lane + 32, ... of a particle row and keeps the
 // node's grid indices (iv fastest, MLSTransport.cpp:142) without divisions.
 struct NodeWalk
@@ -1086,308 +1070,281 @@ k_particle_stream(ParticleArgs<T> a, StepParams p, int wpb)
 }
 
 // ---------------------------------------------------------------------------
-// The same stages for a 3-D single-layer FP32 cloud as three wide kernels,
-// so that no per-particle scalar chain holds up a streaming pass:
-//   k_row_sums      one warp per row.  Interior rows: the positivity sums
-//                   and the moments of the positive part (six FP32 lane sums,
-//                   combined over the warp in FP64) into rowSums.  Wall rows
-//                   are finished here whole: positivity, diffuse wall,
-//                   written back in place (finishWallStream).
-//   k_row_params    one thread per interior particle: positivity decision,
-//                   MOOD screen, moments of the repaired row, temperature,
-//                   the Maxwellian's per-axis factors (FP64, rounded into the
-//                   particle's FP32 table with c1 lam A folded into the x
-//                   axis), and the macros of the collided row by linearity
-//                   (c1 (moments of g + lam moments of M), the per-axis sums
-//                   of the factors giving the Maxwellian's moments).
-//   k_row_collide   one warp per row: h = a max(g, lo) + tx ty tz written
-//                   out (a = c1 s and lo = 0 when the repair fires, else
-//                   a = c1 and lo = -inf), and the row minimum.
-// The moments of the repaired row are those of the positive part (times the
-// repair scale when the repair fires); without a repair any negative values
-// sum to less than 1e-30 in magnitude (Positivity), below the rounding of
-// the FP64 moments, and rows of no positive mass are deferred to k_fixup as
-// before.  Per-particle table: 3 Nv factors, then a and lo (tabStride
-// floats, a multiple of four).
+// The same stages for a 3-D single-layer FP32 cloud with Nv = NV <= 10, the
+// row held in registers: one warp per row (a persistent grid walks the
+// rows).  A row of NV^3 velocities is NV^2 lines of NV contiguous values
+// (fixed ky, kz; kx = 0..NV-1); lane l holds lines l, l + 32, ... .  One
+// load of the row serves the whole stage:
+//   - positivity sums and the moments of the positive part, in FP32 per lane
+//     (the kx loop runs over compile-time velocity registers, the line's vy,
+//     vz apply once per line), combined over the warp in FP64;
+//   - the decisions and the Maxwellian's parameters, on every lane alike;
+//   - the per-axis Maxwellian factors, one (axis, node) per lane in FP64,
+//     and their per-axis moment sums by one warp reduction;
+//   - the collision h = a max(g, lo) + c1 lam A ex ey ez written back, with
+//     a = c1 s and lo = 0 when the repair fires, else a = c1 and lo = -inf;
+//   - the macros of the collided row by linearity, as in k_particle_stream.
+// Wall rows take the diffuse wall (finishWallStream) after their positivity
+// sums.  The moments of the repaired row are those of the positive part
+// (times the repair scale when the repair fires); without a repair any
+// negative values sum to less than 1e-30 in magnitude (Positivity), below the
+// rounding of the FP64 moments, and rows of no positive mass are deferred to
+// k_fixup as before.
 // ---------------------------------------------------------------------------
-__host__ __device__ inline int rowTabStride(int Nv) { return (3 * Nv + 2 + 3) / 4 * 4; }
-constexpr int kRowBatch = 8;   // float4 loads in flight per lane in the row kernels
+constexpr int kRowsThreads = 128;   // four warps per block of the register-row stage
 
-__global__ void __launch_bounds__(kNT)
-k_row_sums(ParticleArgs<float> a, StepParams p, double *__restrict__ rowSums)
+// Lane l's lines l, l + 32, ... of a row of NV^3 values (zeros past the
+// row's NV^2 lines).
+template <int NV>
+__device__ __forceinline__ void loadRowLines(const float *row, int lane,
+                                             float (&x)[(NV * NV + 31) / 32][NV])
 {
-    __shared__ double tab[kNT / 32][3][kMaxNv];
+    constexpr int LINES = NV * NV, LPL = (LINES + 31) / 32;
+#pragma unroll
+    for (int j = 0; j < LPL; ++j)
+    {
+        const int L = lane + 32 * j;
+        if (L < LINES)
+        {
+            const float *ln = row + L * NV;
+            if constexpr (NV % 2 == 0)
+            {
+#pragma unroll
+                for (int q = 0; q < NV; q += 2)
+                {
+                    const float2 v2 = *reinterpret_cast<const float2 *>(ln + q);
+                    x[j][q] = v2.x;
+                    x[j][q + 1] = v2.y;
+                }
+            }
+            else
+            {
+#pragma unroll
+                for (int q = 0; q < NV; ++q) x[j][q] = ln[q];
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int q = 0; q < NV; ++q) x[j][q] = 0.0f;
+        }
+    }
+}
+
+template <int NV>
+__global__ void __launch_bounds__(kRowsThreads, 4)
+k_particle_rows(ParticleArgs<float> a, StepParams p)
+{
+    constexpr int LINES = NV * NV;
+    constexpr int LPL = (LINES + 31) / 32;       // lines per lane
+    constexpr int V = NV * NV * NV;
+    static_assert(NV <= 10 && 3 * NV <= 32, "rows of at most 10^3 velocities");
+    __shared__ double wtab[kRowsThreads / 32][3][kMaxNv];  // diffuse-wall tables
     __shared__ double velD[kMaxNv];
-    extern __shared__ __align__(16) unsigned char sumsSmem[];
-    VelNode<float> *velT = reinterpret_cast<VelNode<float> *>(sumsSmem);
-    int *idxT = reinterpret_cast<int *>(velT + p.V);
+    __shared__ float velF[kMaxNv];
+    __shared__ int idxT[V];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int V = p.V, Nv = p.Nv;
     for (int k = threadIdx.x; k < V; k += blockDim.x)
     {
-        const int iv = k % Nv, jv = (k / Nv) % Nv, kv = k / (Nv * Nv);
-        const double vx = fma((double)iv, p.dv, p.vmin);
-        const double vy = fma((double)jv, p.dv, p.vmin);
-        const double vz = fma((double)kv, p.dv, p.vmin);
-        velT[k] = VelNode<float>{float(vx), float(vy), float(vz),
-                                 float(vx * vx + vy * vy + vz * vz)};
+        const int iv = k % NV, jv = (k / NV) % NV, kv = k / (NV * NV);
         idxT[k] = iv | jv << 8 | kv << 16;
     }
-    for (int q = threadIdx.x; q < Nv; q += blockDim.x) velD[q] = fma((double)q, p.dv, p.vmin);
+    for (int q = threadIdx.x; q < NV; q += blockDim.x)
+    {
+        velD[q] = fma((double)q, p.dv, p.vmin);
+        velF[q] = (float)velD[q];
+    }
     __syncthreads();
+    float vx[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) vx[q] = velF[q];
+    // this lane's axis node of the per-axis factors
+    const int myAxis = lane / NV, myNode = lane - (lane / NV) * NV;
+    const double myV = lane < 3 * NV ? velD[myNode] : 0.0;
+    const double dvN = p.dvN, c1 = p.c1;
     const int W = gridDim.x * (blockDim.x >> 5);
-    const int nq = (V + 3) >> 2;                 // float4 groups of a row
     for (int i = blockIdx.x * (blockDim.x >> 5) + warp; i < p.N; i += W)
     {
-        const float4 *row4 = reinterpret_cast<const float4 *>(a.g + (size_t)i * p.ldf);
-        if (a.boundary[i])
-        {
-            // positivity sums of the wall row, then the diffuse wall
-            float sp = 0.0f, sn = 0.0f;
-            for (int q = lane; q < nq; q += 32)
-            {
-                const float4 x = row4[q];
-                const float xs[4] = {x.x, x.y, x.z, x.w};
+        float *row = a.g + (size_t)i * p.ldf;
+        float x[LPL][NV];
+        loadRowLines<NV>(row, lane, x);
+        const int wallI = a.boundary[i];
+        float s0 = 0.f, sn = 0.f, sx = 0.f, sy = 0.f, sz = 0.f, se = 0.f;
 #pragma unroll
-                for (int e = 0; e < 4; ++e)
-                    if (4 * q + e < V) { sp += fmaxf(xs[e], 0.0f); sn += fminf(xs[e], 0.0f); }
+        for (int j = 0; j < LPL; ++j)
+        {
+            const int L = lane + 32 * j;
+            float ls = 0.f, lx = 0.f, le = 0.f;
+#pragma unroll
+            for (int q = 0; q < NV; ++q)
+            {
+                const float xp = fmaxf(x[j][q], 0.0f);
+                ls += xp;
+                sn += fminf(x[j][q], 0.0f);
+                lx = fmaf(vx[q], xp, lx);
+                le = fmaf(vx[q] * vx[q], xp, le);
             }
-            double r2[2] = {(double)sp, (double)sn};
-            warpSumMany<2>(r2, lane);
-            const Positivity pv(r2[0], r2[1]);
+            if (L < LINES)
+            {
+                const float vy = velF[L % NV], vz = velF[L / NV];
+                s0 += ls;
+                sx += lx;
+                sy = fmaf(vy, ls, sy);
+                sz = fmaf(vz, ls, sz);
+                se += le + (vy * vy + vz * vz) * ls;
+            }
+        }
+        double r6[6] = {(double)s0, (double)sn, (double)sx, (double)sy, (double)sz, (double)se};
+        warpSumMany<6>(r6, lane);
+        const double pos = r6[0], neg = r6[1];
+        const bool bad = !isfinite(pos) || !isfinite(neg) || !isfinite(r6[5]);
+        const double m = pos + neg;
+        const Positivity pv(pos, neg);
+        if (wallI)
+        {
             if (lane == 0)
             {
                 a.flag[i] = 0;
                 if (pv.fix) atomicAdd(&a.sc->nfix, 1);
-                a.massPos[i] = (r2[0] + r2[1]) * p.dvN;
+                a.massPos[i] = m * dvN;
             }
-            finishWallStream(a, p, i, a.g + (size_t)i * p.ldf, idxT, velD, pv, tab[warp], lane);
+            finishWallStream(a, p, i, row, idxT, velD, pv, wtab[warp], lane);
             __syncwarp();
             continue;
         }
-        float s0[2] = {0, 0}, sn[2] = {0, 0}, mx[2] = {0, 0}, my[2] = {0, 0}, mz[2] = {0, 0},
-              me[2] = {0, 0};
-        auto acc = [&](int u, float x, int k) {
-            const float xp = fmaxf(x, 0.0f);
-            const VelNode<float> v = velT[k];
-            s0[u] += xp;
-            sn[u] += fminf(x, 0.0f);
-            mx[u] = fmaf(v.vx, xp, mx[u]);
-            my[u] = fmaf(v.vy, xp, my[u]);
-            mz[u] = fmaf(v.vz, xp, mz[u]);
-            me[u] = fmaf(v.v2, xp, me[u]);
-        };
-        // The lane's float4 groups q = lane + 32 j, kRowBatch at a time: all
-        // of a batch's loads are issued before the first is used.
-        for (int q0 = 0; q0 < nq; q0 += 32 * kRowBatch)
+        int flagged = 0;
+        if (p.limiter == 2)
         {
-            float4 xv[kRowBatch];
-#pragma unroll
-            for (int j = 0; j < kRowBatch; ++j)
+            const double2 nad = reinterpret_cast<const double2 *>(a.nad)[i];
+            if (bad || m <= 0.0) flagged = 1;
+            else if (isfinite(nad.x) && isfinite(nad.y))
             {
-                const int q = q0 + lane + 32 * j;
-                xv[j] = q < nq ? row4[q] : make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-#pragma unroll
-            for (int j = 0; j < kRowBatch; ++j)
-            {
-                const int q = q0 + lane + 32 * j;
-                if (4 * q + 3 < V)
-                {
-                    acc(0, xv[j].x, 4 * q);
-                    acc(1, xv[j].y, 4 * q + 1);
-                    acc(0, xv[j].z, 4 * q + 2);
-                    acc(1, xv[j].w, 4 * q + 3);
-                }
-                else if (q < nq)
-                {
-                    acc(0, xv[j].x, 4 * q);
-                    if (4 * q + 1 < V) acc(1, xv[j].y, 4 * q + 1);
-                    if (4 * q + 2 < V) acc(0, xv[j].z, 4 * q + 2);
-                }
+                const double rn = m * dvN;
+                const double slack = 0.1 * fmax(nad.y - nad.x, 1.0e-12) + 1.0e-9 +
+                                     p.nadNoise * fmax(fabs(nad.x), fabs(nad.y));
+                flagged = (rn < nad.x - slack || rn > nad.y + slack);
             }
         }
-        double r6[6] = {(double)s0[0] + (double)s0[1], (double)sn[0] + (double)sn[1],
-                        (double)mx[0] + (double)mx[1], (double)my[0] + (double)my[1],
-                        (double)mz[0] + (double)mz[1], (double)me[0] + (double)me[1]};
-        warpSumMany<6>(r6, lane);
-        if (lane < 6) rowSums[6 * (size_t)i + lane] = r6[lane];
-    }
-}
-
-__global__ void __launch_bounds__(kNT)
-k_row_params(ParticleArgs<float> a, StepParams p, const double *__restrict__ rowSums,
-             float *__restrict__ rowTab, int *__restrict__ rowKind)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.N) return;
-    if (a.boundary[i]) { rowKind[i] = 0; return; }
-    const double dvN = p.dvN;
-    const double *sm = rowSums + 6 * (size_t)i;
-    const double pos = sm[0], neg = sm[1];
-    const bool bad = !isfinite(pos) || !isfinite(neg) || !isfinite(sm[5]);
-    const double m = pos + neg;
-    const Positivity pv(pos, neg);
-    int flagged = 0;
-    if (p.limiter == 2)
-    {
-        const double2 nad = reinterpret_cast<const double2 *>(a.nad)[i];
-        if (bad || m <= 0.0) flagged = 1;
-        else if (isfinite(nad.x) && isfinite(nad.y))
+        if (lane == 0)
         {
-            const double rn = m * dvN;
-            const double slack = 0.1 * fmax(nad.y - nad.x, 1.0e-12) + 1.0e-9 +
-                                 p.nadNoise * fmax(fabs(nad.x), fabs(nad.y));
-            flagged = (rn < nad.x - slack || rn > nad.y + slack);
+            a.flag[i] = flagged;
+            if (pv.fix) atomicAdd(&a.sc->nfix, 1);
+            if (flagged) a.flagList[atomicAdd(&a.sc->nflag, 1)] = i;
+            else a.massPos[i] = m * dvN;
         }
-    }
-    a.flag[i] = flagged;
-    if (pv.fix) atomicAdd(&a.sc->nfix, 1);
-    if (flagged)
-    {
-        a.flagList[atomicAdd(&a.sc->nflag, 1)] = i;
-        rowKind[i] = 0;
-        return;
-    }
-    a.massPos[i] = m * dvN;
-    // Moments of the repaired row (Moments.cpp:17-97): s times the
-    // positive part's when the repair fires.
-    const double f = (pv.fix ? pv.s : 1.0) * dvN;
-    const double M0 = pv.fix ? pos * f : m * dvN;
-    if (!(M0 > 1.0e-30) || p.tauVar)
-    {
-        a.degList[atomicAdd(&a.sc->ndeg, 1)] = i;
-        rowKind[i] = 0;
-        return;
-    }
-    const double iM0 = 1.0 / M0;
-    const double Mx = sm[2] * f, My = sm[3] * f, Mz = sm[4] * f, ME = sm[5] * f;
-    const double ux = Mx * iM0, uy = My * iM0, uz = Mz * iM0;
-    const double Tt = fmax((ME * iM0 - (ux * ux + uy * uy + uz * uz)) * p.inv3R, 1.0e-6);
-    const double c1 = p.c1, lam = p.lam;
-    const double twoRT = 2.0 * p.R * Tt;
-    const double piT = kPi * twoRT;
-    const double lamA = lam * M0 / (piT * sqrt(piT));
-    const double i2RT = 1.0 / twoRT;
-    const int Nv = p.Nv;
-    float *tb = rowTab + (size_t)i * p.tabStride;
-    double S[9];
+        if (flagged) continue;
+        // Moments of the repaired row (Moments.cpp:17-97): s times the
+        // positive part's when the repair fires.
+        const double f = (pv.fix ? pv.s : 1.0) * dvN;
+        const double M0 = pv.fix ? pos * f : m * dvN;
+        if (!(M0 > 1.0e-30) || p.tauVar)
+        {
+            if (lane == 0) a.degList[atomicAdd(&a.sc->ndeg, 1)] = i;
+            continue;
+        }
+        const double iM0 = 1.0 / M0;
+        const double Mx = r6[2] * f, My = r6[3] * f, Mz = r6[4] * f, ME = r6[5] * f;
+        const double ux = Mx * iM0, uy = My * iM0, uz = Mz * iM0;
+        const double Tt = fmax((ME * iM0 - (ux * ux + uy * uy + uz * uz)) * p.inv3R, 1.0e-6);
+        const double twoRT = 2.0 * p.R * Tt;
+        const double piT = kPi * twoRT;
+        const double lamA = p.lam * M0 / (piT * sqrt(piT));
+        // Per-axis factors: lane d NV + q holds axis d, node q; their
+        // per-axis sums of velocity^0,1,2 by one reduction (eight values,
+        // then the ninth).
+        double e = 0.0;
+        if (lane < 3 * NV)
+        {
+            const double u = myAxis == 0 ? ux : (myAxis == 1 ? uy : uz);
+            e = (myAxis == 0 ? lamA : 1.0) * exp(-(myV - u) * (myV - u) / twoRT);
+        }
+        double S8[8];
 #pragma unroll
-    for (int d = 0; d < 3; ++d)
-    {
-        const double u = d == 0 ? ux : (d == 1 ? uy : uz);
-        const double sc = d == 0 ? lamA : 1.0;
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-        for (int q = 0; q < Nv; ++q)
+        for (int j = 0; j < 8; ++j)
         {
-            const double va = fma((double)q, p.dv, p.vmin);
-            const double e = sc * exp(-(va - u) * (va - u) * i2RT);
-            s0 += e;
-            s1 += va * e;
-            s2 += va * va * e;
-            tb[d * Nv + q] = (float)(d == 0 ? c1 * e : e);
+            const int d = j / 3, pw = j - 3 * d;
+            S8[j] = (lane < 3 * NV && myAxis == d)
+                        ? (pw == 0 ? e : (pw == 1 ? myV * e : myV * myV * e)) : 0.0;
         }
-        S[3 * d] = s0; S[3 * d + 1] = s1; S[3 * d + 2] = s2;
-    }
-    tb[3 * Nv] = (float)(c1 * (pv.fix ? pv.s : 1.0));
-    tb[3 * Nv + 1] = pv.fix ? 0.0f : -INFINITY;
-    rowKind[i] = 1;
-    const double N0 = c1 * (M0 + dvN * S[0] * S[3] * S[6]);
-    const double Nx = c1 * (Mx + dvN * S[1] * S[3] * S[6]);
-    const double Ny = c1 * (My + dvN * S[0] * S[4] * S[6]);
-    const double Nz = c1 * (Mz + dvN * S[0] * S[3] * S[7]);
-    const double NE = c1 * (ME + dvN * (S[2] * S[3] * S[6] + S[0] * S[5] * S[6] +
-                                        S[0] * S[3] * S[8]));
-    double r2 = M0, x2 = ux, y2 = uy, z2 = uz, T2 = Tt;
-    if (N0 > 1.0e-30)
-    {
-        const double iN0 = 1.0 / N0;
-        r2 = N0; x2 = Nx * iN0; y2 = Ny * iN0; z2 = Nz * iN0;
-        T2 = fmax((NE * iN0 - (x2 * x2 + y2 * y2 + z2 * z2)) * p.inv3R, 1.0e-6);
-    }
-    double *mac = a.macNew + 6 * (size_t)i;
-    mac[0] = r2; mac[1] = x2; mac[2] = y2; mac[3] = z2; mac[4] = T2;
-    mac[5] = r2 * p.R * T2;
-    a.dpx[i] = 0.0;
-    a.massEnd[i] = N0;
-}
-
-__global__ void __launch_bounds__(kNT)
-k_row_collide(ParticleArgs<float> a, StepParams p, const float *__restrict__ rowTab,
-              const int *__restrict__ rowKind)
-{
-    __shared__ float wt[kNT / 32][3 * kMaxNv + 4];
-    extern __shared__ __align__(16) unsigned char collSmem[];
-    int *idxT = reinterpret_cast<int *>(collSmem);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int V = p.V, Nv = p.Nv;
-    // table offsets of each node's three factors, padded to whole float4s
-    for (int k = threadIdx.x; k < ((V + 3) & ~3); k += blockDim.x)
-    {
-        const int iv = k % Nv, jv = (k / Nv) % Nv, kv = k / (Nv * Nv);
-        idxT[k] = k < V ? (iv | (Nv + jv) << 8 | (2 * Nv + kv) << 16) : 0;
-    }
-    __syncthreads();
-    const int W = gridDim.x * (blockDim.x >> 5);
-    const int nq = (V + 3) >> 2;
-    float *t = wt[warp];
-    const int ntab = 3 * Nv + 2;
-    for (int i = blockIdx.x * (blockDim.x >> 5) + warp; i < p.N; i += W)
-    {
-        if (rowKind[i] != 1) continue;            // warp-uniform
-        float4 *row4 = reinterpret_cast<float4 *>(a.g + (size_t)i * p.ldf);
-        const float *tg = rowTab + (size_t)i * p.tabStride;
-        // the table and the first batch of the row in flight together
-        const float t0 = lane < ntab ? tg[lane] : 0.0f;
-        const float t1 = lane + 32 < ntab ? tg[lane + 32] : 0.0f;
-        const float t2 = lane + 64 < ntab ? tg[lane + 64] : 0.0f;
-        const float t3 = lane + 96 < ntab ? tg[lane + 96] : 0.0f;
-        const float t4 = lane + 128 < ntab ? tg[lane + 128] : 0.0f;
+        warpSumMany<8>(S8, lane);
+        const double S22 = warpSum(lane < 3 * NV && myAxis == 2 ? myV * myV * e : 0.0);
+        const float ef = (float)(lane < NV ? c1 * e : e);
+        float ex[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) ex[q] = __shfl_sync(0xffffffffu, ef, q);
+        const float am = (float)(c1 * (pv.fix ? pv.s : 1.0));
+        const float lo = pv.fix ? 0.0f : -INFINITY;
         float mn = INFINITY;
-        for (int q0 = 0; q0 < nq; q0 += 32 * kRowBatch)
+#pragma unroll
+        for (int j = 0; j < LPL; ++j)
         {
-            float4 xv[kRowBatch];
-            int4 iv[kRowBatch];
+            const int L = lane + 32 * j;
+            const int Lc = L < LINES ? L : 0;
+            const float eyz = __shfl_sync(0xffffffffu, ef, NV + Lc % NV) *
+                              __shfl_sync(0xffffffffu, ef, 2 * NV + Lc / NV);
+            if (L < LINES)
+            {
+                float h[NV];
 #pragma unroll
-            for (int j = 0; j < kRowBatch; ++j)
-            {
-                const int q = q0 + lane + 32 * j;
-                xv[j] = q < nq ? row4[q] : make_float4(0.f, 0.f, 0.f, 0.f);
-                iv[j] = q < nq ? reinterpret_cast<const int4 *>(idxT)[q] : make_int4(0, 0, 0, 0);
-            }
-            if (q0 == 0)
-            {
-                if (lane < ntab) t[lane] = t0;
-                if (lane + 32 < ntab) t[lane + 32] = t1;
-                if (lane + 64 < ntab) t[lane + 64] = t2;
-                if (lane + 96 < ntab) t[lane + 96] = t3;
-                if (lane + 128 < ntab) t[lane + 128] = t4;
-                __syncwarp();
-            }
-            const float am = t[3 * Nv], lo = t[3 * Nv + 1];
-            auto one = [&](float x, int id) {
-                return fmaf(am, fmaxf(x, lo), t[id & 255] * t[(id >> 8) & 255] * t[id >> 16]);
-            };
+                for (int q = 0; q < NV; ++q)
+                {
+                    h[q] = fmaf(am, fmaxf(x[j][q], lo), ex[q] * eyz);
+                    mn = fminf(mn, h[q]);
+                }
+                float *ln = row + L * NV;
+                if constexpr (NV % 2 == 0)
+                {
 #pragma unroll
-            for (int j = 0; j < kRowBatch; ++j)
-            {
-                const int q = q0 + lane + 32 * j;
-                if (q >= nq) continue;
-                float4 h;
-                h.x = one(xv[j].x, iv[j].x);
-                h.y = 4 * q + 1 < V ? one(xv[j].y, iv[j].y) : xv[j].y;
-                h.z = 4 * q + 2 < V ? one(xv[j].z, iv[j].z) : xv[j].z;
-                h.w = 4 * q + 3 < V ? one(xv[j].w, iv[j].w) : xv[j].w;
-                mn = fminf(mn, h.x);
-                if (4 * q + 1 < V) mn = fminf(mn, h.y);
-                if (4 * q + 2 < V) mn = fminf(mn, h.z);
-                if (4 * q + 3 < V) mn = fminf(mn, h.w);
-                row4[q] = h;
+                    for (int q = 0; q < NV; q += 2)
+                        *reinterpret_cast<float2 *>(ln + q) = make_float2(h[q], h[q + 1]);
+                }
+                else
+                {
+#pragma unroll
+                    for (int q = 0; q < NV; ++q) ln[q] = h[q];
+                }
             }
         }
         const double mnd = warpMin((double)mn);
-        if (lane == 0) a.minG[i] = mnd;
-        __syncwarp();
+        if (lane == 0)
+        {
+            const double *S = S8;
+            const double N0 = c1 * (M0 + dvN * S[0] * S[3] * S[6]);
+            const double Nx = c1 * (Mx + dvN * S[1] * S[3] * S[6]);
+            const double Ny = c1 * (My + dvN * S[0] * S[4] * S[6]);
+            const double Nz = c1 * (Mz + dvN * S[0] * S[3] * S[7]);
+            const double NE = c1 * (ME + dvN * (S[2] * S[3] * S[6] + S[0] * S[5] * S[6] +
+                                                S[0] * S[3] * S22));
+            double r2 = M0, x2 = ux, y2 = uy, z2 = uz, T2 = Tt;
+            if (N0 > 1.0e-30)
+            {
+                const double iN0 = 1.0 / N0;
+                r2 = N0; x2 = Nx * iN0; y2 = Ny * iN0; z2 = Nz * iN0;
+                T2 = fmax((NE * iN0 - (x2 * x2 + y2 * y2 + z2 * z2)) * p.inv3R, 1.0e-6);
+            }
+            double *mac = a.macNew + 6 * (size_t)i;
+            mac[0] = r2; mac[1] = x2; mac[2] = y2; mac[3] = z2; mac[4] = T2;
+            mac[5] = r2 * p.R * T2;
+            a.dpx[i] = 0.0;
+            a.massEnd[i] = N0;
+            a.minG[i] = mnd;
+        }
+    }
+}
+
+// Launch of the register-row stage for the cloud's Nv (nullptr when no
+// instance covers it).
+typedef void (*RowsKernel)(ParticleArgs<float>, StepParams);
+static RowsKernel rowsKernel(int Nv)
+{
+    switch (Nv)
+    {
+    case 4: return k_particle_rows<4>;
+    case 5: return k_particle_rows<5>;
+    case 6: return k_particle_rows<6>;
+    case 8: return k_particle_rows<8>;
+    case 10: return k_particle_rows<10>;
+    default: return nullptr;
     }
 }
 
@@ -2055,16 +2012,16 @@ __global__ void k_convert_out(const T *src, double *dst, int N, int gs, int ldf,
 // Steady residual of the last step, over the interior particles:
 //   max( |d rho| / |rho|, |d(rho ux)| / |rho c|, |d(rho uy)| / |rho c|,
 //        |d(rho E)| / |rho E| ),  |.| the 2-norm over particles,
-// E = |u|^2 / 2 + 3 R T / 2 (monatomic gas), c = sqrt(R T) the thermal
-// speed.  Momentum changes are measured against the thermal momentum: that
-// scale does not vanish for a gas at rest, and FP32 storage resolves the
-// flow velocity only to about 1e-7 of c, far above 1e-6 of a slow flow's
-// own momentum.  The reference defines no residual; this is the
-// convergence measure of a run to steady state.  One block, fixed order:
-// deterministic.
+// E = |u|^2 / 2 + 3 R T / 2 (monatomic gas) and c the momentum speed scale:
+// uRef when it is positive (the lid speed of a driven cavity), the flow
+// speed |u| itself when it is negative (momentum changes against the flow's
+// own momentum), else sqrt(R T), the thermal speed, which does not vanish
+// for a gas at rest.  The reference defines no
+// residual; this is the convergence measure of a run to steady state.  One
+// block, fixed order: deterministic.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void k_residual_body(const double *__restrict__ macNew, const double *__restrict__ macOld,
-           const int *__restrict__ boundary, int N, double R, double *out, int unused)
+           const int *__restrict__ boundary, int N, double R, double *out, double uRef)
 {
     __shared__ double sh[8 * 32];
     double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -2076,7 +2033,10 @@ __device__ __forceinline__ void k_residual_body(const double *__restrict__ macNe
         const double eb = 0.5 * (b[1] * b[1] + b[2] * b[2] + b[3] * b[3]) + 1.5 * R * b[4];
         const double mn[4] = {a[0], a[0] * a[1], a[0] * a[2], a[0] * ea};
         const double mo[4] = {b[0], b[0] * b[1], b[0] * b[2], b[0] * eb};
-        const double thermal2 = b[0] * b[0] * R * b[4];      // (rho c)^2
+        const double thermal2 =                                  // (rho c)^2
+            uRef > 0.0 ? b[0] * b[0] * uRef * uRef
+                       : (uRef < 0.0 ? b[0] * b[0] * (b[1] * b[1] + b[2] * b[2] + b[3] * b[3])
+                                     : b[0] * b[0] * R * b[4]);
         const double ref[4] = {b[0] * b[0], thermal2, thermal2, mo[3] * mo[3]};
 #pragma unroll
         for (int q = 0; q < 4; ++q)
@@ -2098,9 +2058,9 @@ __device__ __forceinline__ void k_residual_body(const double *__restrict__ macNe
 
 __global__ void __launch_bounds__(1024)
 k_residual(const double *__restrict__ macNew, const double *__restrict__ macOld,
-           const int *__restrict__ boundary, int N, double R, double *out)
+           const int *__restrict__ boundary, int N, double R, double *out, double uRef)
 {
-    k_residual_body(macNew, macOld, boundary, N, R, out, 0);
+    k_residual_body(macNew, macOld, boundary, N, R, out, uRef);
 }
 
 // ---------------------------------------------------------------------------
@@ -2123,14 +2083,9 @@ static void launchParticleStream(alebgk_ctx *c, const ParticleArgs<T> &pa, const
 {
     if constexpr (sizeof(T) == 4)
     {
-        if (c->pSplit)
+        if (c->pRows)
         {
-            DeviceBuffers &d = c->d;
-            k_row_sums<<<c->pSumsBlocks, kNT, c->pSumsSmem, st>>>(pa, p, d.rowSums);
-            k_row_params<<<(p.N + kNT - 1) / kNT, kNT, 0, st>>>(pa, p, d.rowSums, d.rowTab,
-                                                                d.rowKind);
-            k_row_collide<<<c->pCollBlocks, kNT, c->pCollSmem, st>>>(pa, p, d.rowTab,
-                                                                     d.rowKind);
+            rowsKernel(p.Nv)<<<c->pRowsBlocks, kRowsThreads, 0, st>>>(pa, p);
             return;
         }
     }
@@ -2177,13 +2132,6 @@ static cudaError_t stepT(alebgk_ctx *c, int from, cudaEvent_t *ev)
         cudaStreamWaitEvent(c->stream2, c->evFork, 0);
         k_step_begin<<<nadBlocks, kNT, 0, c->stream2>>>(d.sc, 0, macA, d.boundary, d.nslot,
                                                         d.slots, p.S, p.N, d.nad);
-        // the march's left-out particles ride on the side stream too
-        if (sizeof(T) == 4 && c->march.enabled && c->march.ngather > 0)
-        {
-            cudaError_t e = launchTransportList(c, from, reinterpret_cast<float *>(fb),
-                                                c->march.gather, c->march.ngather, c->stream2);
-            if (e != cudaSuccess) return e;
-        }
         cudaEventRecord(c->evJoin, c->stream2);
     }
     else
@@ -2197,8 +2145,7 @@ static cudaError_t stepT(alebgk_ctx *c, int from, cudaEvent_t *ev)
     const bool fused = !march && !c->pStream && c->tune.transportThreads == 0 && !ev;
     if (march)
     {
-        cudaError_t e = launchMarch(c, from, reinterpret_cast<float *>(fb), st,
-                                    fork ? nullptr : st);
+        cudaError_t e = launchMarch(c, from, reinterpret_cast<float *>(fb), st);
         if (e != cudaSuccess) return e;
     }
     else if (!fused)
@@ -2302,30 +2249,21 @@ static cudaError_t prepareT(alebgk_ctx *c)
                 c->pStreamBlocks = need < sms * occ ? need : sms * occ;
             }
         }
-        // The three-kernel form of the same stages (FP32 only): the default,
-        // unless the warp-per-particle form is asked for.
-        c->pSplit = false;
-        if (e == cudaSuccess && c->pStream && sizeof(T) == 4 && c->cfg.particle != 3 &&
-            p.Nv <= kMaxNv)
+        // The register-row form of the same stages (FP32, Nv of an
+        // instance): the default, unless the shared-memory form is asked for.
+        c->pRows = false;
+        const RowsKernel rk = rowsKernel(p.Nv);
+        if (e == cudaSuccess && c->pStream && sizeof(T) == 4 && c->cfg.particle != 3 && rk)
         {
-            const size_t s1 = streamRowsOffset<float>(p.V), s3 = (size_t)4 * ((p.V + 3) & ~3);
-            set((const void *)k_row_sums, s1);
-            set((const void *)k_row_collide, s3);
-            int o1 = 0, o3 = 0, sms = 0;
+            int occ = 0, sms = 0;
+            e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
             if (e == cudaSuccess)
-                e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            if (e == cudaSuccess)
-                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_row_sums, kNT, s1);
-            if (e == cudaSuccess)
-                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o3, k_row_collide, kNT, s3);
-            if (e == cudaSuccess && o1 > 0 && o3 > 0)
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, rk, kRowsThreads, 0);
+            if (e == cudaSuccess && occ > 0)
             {
-                const int need = (p.N + kNT / 32 - 1) / (kNT / 32);
-                c->pSplit = true;
-                c->pSumsSmem = s1;
-                c->pCollSmem = s3;
-                c->pSumsBlocks = std::min(need, sms * o1);
-                c->pCollBlocks = std::min(need, sms * o3);
+                const int need = (p.N + kRowsThreads / 32 - 1) / (kRowsThreads / 32);
+                c->pRows = true;
+                c->pRowsBlocks = std::min(need, sms * occ);
             }
         }
     }
@@ -2337,19 +2275,6 @@ static cudaError_t prepareT(alebgk_ctx *c)
 cudaError_t prepareKernels(alebgk_ctx *c)
 {
     return (c->cfg.precision == 64) ? prepareT<double>(c) : prepareT<float>(c);
-}
-
-cudaError_t launchTransportList(alebgk_ctx *c, int from, float *outBuf, const int *list, int n,
-                                cudaStream_t st)
-{
-    const StepParams &p = c->sp;
-    const DeviceBuffers &d = c->d;
-    dim3 grid(transportChunks(p.V), (n + kNT / 32 - 1) / (kNT / 32));
-    k_transport_list<float><<<grid, kNT, 0, st>>>(static_cast<const float *>(d.f[from]), outBuf,
-                                                  static_cast<const float *>(d.coef), d.cls,
-                                                  d.nslot, d.slots, list, n, p.S, p.V, p.ldf,
-                                                  d.sc);
-    return cudaGetLastError();
 }
 
 cudaError_t launchStep(alebgk_ctx *c, int from, cudaEvent_t *ev)
@@ -2401,13 +2326,15 @@ __device__ __forceinline__ int batchCtxOf(const int *__restrict__ off, int n, in
 template <typename T>
 __device__ __forceinline__ const BatchCtx<T> &batchStage(const BatchCtx<T> *__restrict__ ctx,
                                                          const int *__restrict__ off, int n,
-                                                         int stage, int &vb, int &vg)
+                                                         int stage, int &vb, int &vg,
+                                                         int gb = -1)
 {
     __shared__ __align__(16) unsigned char raw[sizeof(BatchCtx<T>)];
     static_assert(sizeof(BatchCtx<T>) % 8 == 0, "descriptor words");
+    if (gb < 0) gb = blockIdx.x;
     const int *o = off + stage * (n + 1);
-    const int c = batchCtxOf(o, n, blockIdx.x);
-    vb = blockIdx.x - o[c];
+    const int c = batchCtxOf(o, n, gb);
+    vb = gb - o[c];
     vg = o[c + 1] - o[c];
     const unsigned long long *src = reinterpret_cast<const unsigned long long *>(ctx + c);
     unsigned long long *dst = reinterpret_cast<unsigned long long *>(raw);
@@ -2528,7 +2455,237 @@ __global__ void __launch_bounds__(1024)
 k_batch_residual(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ off, int n)
 {
     BATCH_CTX(10);
-    k_residual_body(B.pa.macNew, B.pa.macPrev, B.pa.boundary, B.p.N, B.p.R, B.resid, 0);
+    k_residual_body(B.pa.macNew, B.pa.macPrev, B.pa.boundary, B.p.N, B.p.R, B.resid, B.p.resU);
+}
+
+// The residual's 1024-thread block (k_residual_body) on a 256-thread block:
+// each thread runs four virtual threads t + 256 j with their own strided
+// sums, a warp reduces virtual warp wid + 8 j, and the 32 virtual warps'
+// sums are added in virtual-warp order -- the operations and order of the
+// 1024-thread block, so the same bits.
+__device__ void residualBody1024(const double *__restrict__ macNew,
+                                 const double *__restrict__ macOld,
+                                 const int *__restrict__ boundary, int N, double R, double *out,
+                                 double uRef)
+{
+    __shared__ double sh[8 * 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll 1
+    for (int j = 0; j < 4; ++j)
+    {
+        double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int i = threadIdx.x + 256 * j; i < N; i += 1024)
+        {
+            if (boundary[i]) continue;
+            const double *a = macNew + 6 * (size_t)i, *b = macOld + 6 * (size_t)i;
+            const double ea = 0.5 * (a[1] * a[1] + a[2] * a[2] + a[3] * a[3]) + 1.5 * R * a[4];
+            const double eb = 0.5 * (b[1] * b[1] + b[2] * b[2] + b[3] * b[3]) + 1.5 * R * b[4];
+            const double mn[4] = {a[0], a[0] * a[1], a[0] * a[2], a[0] * ea};
+            const double mo[4] = {b[0], b[0] * b[1], b[0] * b[2], b[0] * eb};
+            const double thermal2 =
+                uRef > 0.0 ? b[0] * b[0] * uRef * uRef
+                           : (uRef < 0.0 ? b[0] * b[0] * (b[1] * b[1] + b[2] * b[2] + b[3] * b[3])
+                                         : b[0] * b[0] * R * b[4]);
+            const double ref[4] = {b[0] * b[0], thermal2, thermal2, mo[3] * mo[3]};
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+            {
+                const double d = mn[q] - mo[q];
+                v[q] += d * d;
+                v[4 + q] += ref[q];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = warpSum(v[q]);
+        if (lane == 0)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) sh[q * 32 + wid + 8 * j] = v[q];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+        {
+            double sum = 0.0;
+            for (int w = 0; w < 32; ++w) sum += sh[q * 32 + w];
+            v[q] = sum;
+        }
+        double r = 0.0;
+        for (int q = 0; q < 4; ++q)
+            if (v[4 + q] > 0.0) r = fmax(r, sqrt(v[q] / v[4 + q]));
+        *out = r;
+    }
+    __syncthreads();
+}
+
+// Grid-wide barrier of the persistent batch step: bar[0] counts the blocks
+// in, bar[1] is the generation, bar[2] an abort flag.  Every wait gives up
+// after `cap` polls (or when another block has given up), raises the abort
+// flag and returns false; the caller then leaves the kernel.  The host
+// clears bar before every launch.
+__device__ __forceinline__ bool gridBarrier(unsigned *bar, long long cap)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        volatile unsigned *vb = bar;
+        ok = 1;
+        const unsigned gen = vb[1];
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1)
+        {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        }
+        else
+        {
+            long long it = 0;
+            while (vb[1] == gen)
+            {
+                if (it >= cap || vb[2] != 0u)
+                {
+                    ok = 0;
+                    atomicExch(bar + 2, 1u);
+                    break;
+                }
+                ++it;
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// The whole batch step in one launch: every stage of every cloud as
+// virtual blocks (the bodies, virtual block indices and grid sizes of the
+// stage launches, so every cloud computes what its own launches compute),
+// the blocks of a stage spread over a persistent grid, and a bounded
+// grid-wide barrier between stages.  A barrier that gives up sets bit 8 of
+// the first cloud's error word and ends the launch.
+template <typename T, int L>
+__global__ void __launch_bounds__(kNT)
+k_batch_persistent(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ off, int n,
+                   unsigned *bar, long long cap)
+{
+    auto blocksOf = [&](int stage) { return off[stage * (n + 1) + n]; };
+    auto barrier = [&]() {
+        if (gridBarrier(bar, cap)) return true;
+        if (threadIdx.x == 0) atomicOr(&ctx[0].pa.sc->err, 8);
+        return false;
+    };
+    int vb, vg;
+    // 0: counters
+    for (int b = blockIdx.x; b < blocksOf(0); b += gridDim.x)
+    {
+        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 0, vb, vg, b);
+        if (vb == 0 && threadIdx.x == 0)
+        {
+            StepScalars *sc = B.pa.sc;
+            sc->nflag = 0; sc->ndeg = 0; sc->nfix = 0; sc->moodfail = 0;
+        }
+        __syncthreads();
+    }
+    if (!barrier()) return;
+    // 2: transport + particle stage (fused)
+    for (int b = blockIdx.x; b < blocksOf(2); b += gridDim.x)
+    {
+        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 2, vb, vg, b);
+        k_particle_body<T, L, true>(B.pa, B.p, B.wpb, vb);
+        __syncthreads();
+    }
+    if (!barrier()) return;
+    // 3: linear redo of the flagged particles
+    for (int b = blockIdx.x; b < blocksOf(3); b += gridDim.x)
+    {
+        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 3, vb, vg, b);
+        k_redo_body<T, L>(B.pa, B.p, vb, vg);
+        __syncthreads();
+    }
+    if (!barrier()) return;
+    // 4: sigma
+    for (int b = blockIdx.x; b < blocksOf(4); b += gridDim.x)
+    {
+        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 4, vb, vg, b);
+        StepScalars *sc = B.pa.sc;
+        double m;
+        if (gridSumLast(B.pa.massPos, B.p.N, B.redPartial, sc, &m, vb, vg))
+        {
+            sc->massNew = m;
+            sc->sigma = (m > 1.0e-30) ? sc->massOld / m : 1.0;
+        }
+        __syncthreads();
+    }
+    if (!barrier()) return;
+    // 5: fixup
+    for (int b = blockIdx.x; b < blocksOf(5); b += gridDim.x)
+    {
+        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 5, vb, vg, b);
+        k_fixup_body<T>(B.pa, B.p, vb, vg);
+        __syncthreads();
+    }
+    if (!barrier()) return;
+    // 6: end-of-step mass
+    for (int b = blockIdx.x; b < blocksOf(6); b += gridDim.x)
+    {
+        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 6, vb, vg, b);
+        StepScalars *sc = B.pa.sc;
+        double m;
+        if (gridSumLast(B.pa.massEnd, B.p.N, B.redPartial, sc, &m, vb, vg))
+        {
+            const double sigma = sc->sigma;
+            sc->massEnd = sigma * m;
+            sc->massOld = sc->massEnd;
+            sc->scale = sigma;
+            sc->steps += 1;
+        }
+        __syncthreads();
+    }
+    if (!barrier()) return;
+    // 7: sigma on the macros, moodCheck
+    for (int b = blockIdx.x; b < blocksOf(7); b += gridDim.x)
+    {
+        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 7, vb, vg, b);
+        k_scale_mood_body(B.p, B.pa.boundary, B.pa.macNew, B.pa.minG, B.mood, B.pa.sc, vb);
+        __syncthreads();
+    }
+    if (!barrier()) return;
+    // 8: second collision where moodCheck failed
+    for (int b = blockIdx.x; b < blocksOf(8); b += gridDim.x)
+    {
+        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 8, vb, vg, b);
+        k_recollide_body<T>(B.pa.g, B.p, B.pa.boundary, B.pa.macNew, B.pa.massEnd, B.pa.sc, vb,
+                            vg);
+        __syncthreads();
+    }
+    if (!barrier()) return;
+    // 9: end mass after a second collision
+    for (int b = blockIdx.x; b < blocksOf(9); b += gridDim.x)
+    {
+        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 9, vb, vg, b);
+        StepScalars *sc = B.pa.sc;
+        double m;
+        if (sc->moodfail != 0 &&
+            gridSumLast(B.pa.massEnd, B.p.N, B.redPartial, sc, &m, vb, vg))
+        {
+            sc->massEnd = sc->sigma * m;
+            sc->massOld = sc->massEnd;
+        }
+        __syncthreads();
+    }
+    if (!barrier()) return;
+    // 10: steady residual (1024-thread virtual blocks)
+    for (int b = blockIdx.x; b < blocksOf(10); b += gridDim.x)
+    {
+        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 10, vb, vg, b);
+        residualBody1024(B.pa.macNew, B.pa.macPrev, B.pa.boundary, B.p.N, B.p.R, B.resid,
+                         B.p.resU);
+        __syncthreads();
+    }
 }
 
 #undef BATCH_CTX
@@ -2600,6 +2757,8 @@ static cudaError_t buildBatchT(alebgk_ctx *const *cs, int n, double *const *resi
             e = cudaMemcpy(bl.desc[from], h[from].data(), sizeof(BatchCtx<T>) * n,
                            cudaMemcpyHostToDevice);
     }
+    if (e == cudaSuccess) e = cudaMalloc(&bl.bar, 4 * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(bl.bar, 0, 4 * sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMalloc(&bl.off, sizeof(int) * off.size());
     if (e == cudaSuccess)
         e = cudaMemcpy(bl.off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice);
@@ -2664,7 +2823,42 @@ static cudaError_t batchPrepareT(const BatchLaunch &bl)
     };
     set((const void *)k_batch_particle<T, L>, bl.smemParticle);
     set((const void *)k_batch_redo<T, L>, bl.smemRedo);
+    // the persistent form: as many blocks as are resident at once
+    const size_t smemPersist = std::max(bl.smemParticle, bl.smemRedo);
+    set((const void *)k_batch_persistent<T, L>, smemPersist);
+    int occ = 0, sms = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_persistent<T, L>, kNT,
+                                                          smemPersist);
+    const_cast<BatchLaunch &>(bl).pGrid = occ * sms;
     return e;
+}
+
+template <typename T, int L>
+static cudaError_t batchPersistentT(const BatchLaunch &bl, int from, cudaStream_t st)
+{
+    int most = 0;
+    for (int s = 0; s < kBatchStages; ++s) most = std::max(most, bl.blocks[s]);
+    const int grid = std::min(bl.pGrid, most);
+    if (grid < 1) return cudaErrorLaunchOutOfResources;
+    const BatchCtx<T> *ctx = static_cast<const BatchCtx<T> *>(bl.desc[from]);
+    cudaError_t e = cudaMemsetAsync(bl.bar, 0, 4 * sizeof(unsigned), st);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kNT);
+    cfg.dynamicSmemBytes = std::max(bl.smemParticle, bl.smemRedo);
+    cfg.stream = st;
+    // co-resident blocks (a cooperative launch); the barrier's poll limit
+    // still ends the launch with an error if they ever were not
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_batch_persistent<T, L>, ctx, (const int *)bl.off, bl.n,
+                              bl.bar, bl.spinCap);
 }
 
 cudaError_t prepareBatchLaunch(const BatchLaunch &bl)
@@ -2675,6 +2869,14 @@ cudaError_t prepareBatchLaunch(const BatchLaunch &bl)
 
 cudaError_t launchBatchStep(const BatchLaunch &bl, int from, cudaStream_t st)
 {
+    if (bl.persistent)
+    {
+        if (bl.f64)
+            return bl.L == 2 ? batchPersistentT<double, 2>(bl, from, st)
+                             : batchPersistentT<double, 1>(bl, from, st);
+        return bl.L == 2 ? batchPersistentT<float, 2>(bl, from, st)
+                         : batchPersistentT<float, 1>(bl, from, st);
+    }
     if (bl.f64) return bl.L == 2 ? batchStepT<double, 2>(bl, from, st)
                                  : batchStepT<double, 1>(bl, from, st);
     return bl.L == 2 ? batchStepT<float, 2>(bl, from, st) : batchStepT<float, 1>(bl, from, st);
@@ -2682,7 +2884,7 @@ cudaError_t launchBatchStep(const BatchLaunch &bl, int from, cudaStream_t st)
 
 void freeBatchLaunch(BatchLaunch &bl)
 {
-    for (void *p : {bl.desc[0], bl.desc[1], (void *)bl.off})
+    for (void *p : {bl.desc[0], bl.desc[1], (void *)bl.off, (void *)bl.bar})
         if (p) cudaFree(p);
     bl = BatchLaunch();
 }
@@ -2731,7 +2933,7 @@ static cudaError_t slabSegT(alebgk_ctx *c, int from, int seg, cudaStream_t st)
         const bool fused = !march && !c->pStream && c->tune.transportThreads == 0;
         if (march)
         {
-            cudaError_t e = launchMarch(c, from, reinterpret_cast<float *>(fb), st, st);
+            cudaError_t e = launchMarch(c, from, reinterpret_cast<float *>(fb), st);
             if (e != cudaSuccess) return e;
         }
         else if (!fused)
@@ -2854,7 +3056,7 @@ cudaError_t launchSetSurfaceVelocity(alebgk_ctx *c, int nbodies,
 cudaError_t launchResidual(alebgk_ctx *c, double *out, cudaStream_t st)
 {
     k_residual<<<1, 1024, 0, st>>>(c->d.macro[c->cur], c->d.macro[1 - c->cur], c->d.boundary,
-                                   c->sp.N, c->sp.R, out);
+                                   c->sp.N, c->sp.R, out, c->sp.resU);
     return cudaGetLastError();
 }
 

@@ -70,10 +70,13 @@ def train(X, T, steps: int = 20000, batch: int = 16384, lr: float = 2e-3,
     return net
 
 
-def _run(specs, net=None, tol: float = 1e-6, check_every: int = 10, max_steps: int = 20000):
+def _run(specs, net=None, tol: float = 1e-6, check_every: int = 100, max_steps: int = 60000,
+         residual: str = "lid"):
     """Runs the cases to steady, cold or seeded; returns (steps per case,
-    seconds until all are steady incl. seeding, 13-moment rows per case)."""
-    b = BatchSolver(specs)
+    seconds until all are steady incl. seeding, 13-moment rows per case).
+    Steady: the mean change per step over a check interval, momentum against
+    the lid momentum (residual="lid"), below tol."""
+    b = BatchSolver(specs, residual=residual)
     b.sync()
     t0 = time.perf_counter()
     if net is not None:
@@ -110,12 +113,12 @@ def _reference(specs, steps: int):
     return moms
 
 
-def evaluate(net, specs, tol: float = 1e-6, check_every: int = 10, max_steps: int = 20000,
-             reference_steps: int = 8000):
+def evaluate(net, specs, tol: float = 1e-6, check_every: int = 100, max_steps: int = 60000,
+             reference_steps: int = 8000, residual: str = "lid"):
     """Cold start against warm start on the same cases; both steady states
     are also compared with the fields after a long cold run."""
-    cold, t_cold, m_cold, _ = _run(specs, None, tol, check_every, max_steps)
-    warm, t_warm, m_warm, pred = _run(specs, net, tol, check_every, max_steps)
+    cold, t_cold, m_cold, _ = _run(specs, None, tol, check_every, max_steps, residual)
+    warm, t_warm, m_warm, pred = _run(specs, net, tol, check_every, max_steps, residual)
     m_ref = _reference(specs, reference_steps) if reference_steps else None
     names = ("rho", "ux", "uy", "T")
     field = {k: [] for k in names}
@@ -140,7 +143,7 @@ def evaluate(net, specs, tol: float = 1e-6, check_every: int = 10, max_steps: in
         vs_ref["reference_steps"] = reference_steps
     ok = (cold > 0) & (warm > 0)
     return {
-        "cases": len(specs), "tol": tol, "check_every": check_every,
+        "cases": len(specs), "tol": tol, "check_every": check_every, "residual": residual,
         "cold_steps": cold.tolist(), "warm_steps": warm.tolist(),
         "cold_steps_mean": float(cold[ok].mean()) if ok.any() else None,
         "warm_steps_mean": float(warm[ok].mean()) if ok.any() else None,

@@ -33,6 +33,10 @@ sys.path.insert(0, ROOT)
 WORKLOAD = dict(case="cavity3d", Nx=40, Nv=10, mls_order=2)
 METRIC = "cavity3d Nx40 Nv10 updates/s"
 BYTES_PER_UPDATE_FP32 = 8.0     # read f once + write f once, FP32
+# The reference's Solver/CudaBackend.cu, compiled unmodified for sm_100a, on
+# this workload (cavity3d Nx40 Nv10, quadratic MLS, FP64): recorded.
+REFERENCE_GPU = {"ms_per_step": 99.50, "updates_per_s": 6.432e8, "kind": "recorded",
+                 "sample": "10 timed cudaStep calls after 3, one B200, SM 1965 MHz"}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -52,9 +56,10 @@ def parse():
                          "(96 seeded cavities advanced by one graph launch per step), or the "
                          "learned warm start on 32 held-out cavity2d cases")
     ap.add_argument("--batch", type=int, default=96)
-    ap.add_argument("--batch-form", default="auto", choices=["auto", "stages", "branches"],
-                    help="batched-cavity2d graph form: autotuned, stage groups (4), or "
-                         "per-cavity branches")
+    ap.add_argument("--batch-form", default="auto",
+                    choices=["auto", "stages", "branches", "persistent"],
+                    help="batched-cavity2d graph form: autotuned, stage groups (4), one "
+                         "persistent launch per step, or per-cavity branches")
     ap.add_argument("--no-steady", action="store_true",
                     help="batched-cavity2d: skip the run to the steady residual")
     ap.add_argument("--ncu", action="store_true",
@@ -306,18 +311,18 @@ def run_ours(args):
     if rc != 0:
         raise RuntimeError("alebgk_profile_steps failed")
     stage_ms = {name: prof[i] / nprof for i, name in enumerate(_abi.STAGES)}
-    dominant = max(stage_ms, key=stage_ms.get)
     peak, peak_src = measured_peak()
     es = 4 if args.precision == 32 else 8
     cnt0 = s.counters()
     kernels = {"transport": "k_march" if cnt0["transport_kernel"] == 2 else "k_transport",
                "particle": {1: "k_particle", 2: "k_particle_stream",
-                            3: "k_row_sums+k_row_params+k_row_collide"}[cnt0["particle_kernel"]]}
-    # Algorithmic bytes per update: the transport and the particle stage each
-    # read f once and write it once (FP32: 4 + 4 bytes).
+                            3: "k_particle_rows"}[cnt0["particle_kernel"]]}
+    # Algorithmic bytes per update: the transport reads f once and writes it
+    # once (FP32: 4 + 4 bytes); so does the particle stage.  The roofline is
+    # the transport's, the step's single largest kernel.
     per_update = 2 * es
-    achieved = per_update * updates / (stage_ms[dominant] / 1e3) / 1e9
-    kern_name = kernels.get(dominant, dominant)
+    kern_name = kernels["transport"]
+    achieved = per_update * updates / (stage_ms["transport"] / 1e3) / 1e9
     traffic, traffic_src = recorded_traffic(kern_name)
     # The transport's own bound is the FP32 FMA pipe: one FMA per stencil
     # slot and velocity (slots = neighbours + self), against the nominal
@@ -386,10 +391,9 @@ def run_ours(args):
                    "parallelism": f"{world} independent cavities, one per GPU",
                    "l2": "inputs larger than L2: two 256 MB distribution buffers "
                          "ping-pong, no flush needed"},
-        # 10 stage kernels; the row stage is three; the march adds the gather
-        # of its left-out particles
-        "gpu_launches": (10 + (2 if cnt0["particle_kernel"] == 3 else 0) +
-                         (1 if cnt0["transport_kernel"] == 2 else 0)) * args.steps,
+        # one launch per stage: step_begin, transport, particle, redo, sigma,
+        # fixup, mass_sum, scale_mood, recollide, mass_end
+        "gpu_launches": 10 * args.steps,
         "kernels": kernels,
         "stage_ms": {k: round(v, 5) for k, v in stage_ms.items()},
         "roofline": {"bound": "hbm", "kernel": kern_name, "achieved": achieved,
@@ -397,6 +401,11 @@ def run_ours(args):
                      "peak_source": peak_src, "traffic": traffic,
                      "traffic_source": traffic_src,
                      "algorithmic_bytes_per_launch": per_update * updates},
+        # the reference's own GPU path (Solver/CudaBackend.cu for sm_100a,
+        # FP64, quadratic MLS) on the same workload, timed by
+        # oracle/time_reference_gpu.py on a B200 of this pool
+        "reference_gpu": REFERENCE_GPU,
+        "vs_reference_gpu": value / REFERENCE_GPU["updates_per_s"],
         "transport_fma_roofline": {
             "bound": "fp32-fma", "kernel": kernels["transport"],
             "achieved": fmas / (stage_ms["transport"] / 1e3) / 1e12,
@@ -428,6 +437,15 @@ def run_ours(args):
     print(json.dumps(out))
 
 
+def batched_roofline(updates, steps, seconds, precision):
+    es = 4 if precision == 32 else 8
+    achieved = 2 * es * updates * steps / seconds / 1e9
+    peak, src = measured_peak()
+    return {"bound": "hbm", "kernel": "whole batch step", "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": achieved / peak, "peak_source": src, "traffic": None,
+            "bytes_per_update": 2 * es}
+
+
 def run_batched(args):
     """Batched cavity2d on one GPU (ranks > 0 of a torchrun take their LPT
     share of the instances): step throughput of the whole batch, then the
@@ -439,7 +457,7 @@ def run_batched(args):
     specs = batched_cavity2d(args.batch, seed=0)
     mine = partition_lpt([s["Nx"] ** 2 * s["Nv"] ** 2 for s in specs], world)[rank]
     b = BatchSolver([specs[i] for i in mine], precision=args.precision, device=local,
-                    launch="branches" if args.batch_form == "branches" else "stages")
+                    launch="stages" if args.batch_form == "auto" else args.batch_form)
     if args.batch_form == "auto":
         b.autotune(3)
     with ClockSampler(local) as clk:
@@ -450,14 +468,14 @@ def run_batched(args):
         b.sync()
         t = time.perf_counter() - t0
     updates = b.updates_per_step
-    form = b.staged
+    form, launch = b.staged, b.launch
     b.close()
     # Steps and wall time to steady from the Maxwellian at rest: a fresh
     # batch, timed from before its autotuning (the host set-up excluded).
     done, t_steady = np.zeros(1, np.int64), None
     if not args.no_steady:
         b = BatchSolver([specs[i] for i in mine], precision=args.precision, device=local,
-                        launch="branches" if args.batch_form == "branches" else "stages")
+                        launch="stages" if args.batch_form == "auto" else args.batch_form)
         b.sync()
         t1 = time.perf_counter()
         if args.batch_form == "auto":
@@ -477,9 +495,14 @@ def run_batched(args):
         "config": {"workload": f"batched cavity2d, {len(mine)} of {args.batch} instances on "
                                f"rank 0, one CUDA graph launch per step, launch form "
                                f"{args.batch_form}", "instances": len(mine),
-                   "launch_form": (f"stage launches in {form} groups" if form
+                   "launch_form": ("one persistent launch per step" if launch == "persistent"
+                                   and form else f"stage launches in {form} groups" if form
                                    else "per-cavity graph branches")},
         "timing": "wall clock around synchronised graph launches",
+        # the whole step's algorithmic traffic: every update reads f and
+        # writes it once in the transport+particle stage (4 + 4 bytes FP32)
+        # and the macros' traffic is small beside it
+        "roofline": batched_roofline(updates, args.steps, t, args.precision),
         "steady": None if args.no_steady else {
             "tol": 1e-6, "max_steps_to_steady": int(done.max()),
             "all_steady": bool((done > 0).all()), "seconds": t_steady,
@@ -602,9 +625,10 @@ def run_fp32_error(args):
 def run_free_body(args):
     """The free-body cube (cavity3d-cube Nx40 Nv10, density 4.4, parabolic lid
     10 m/s, dt 1.5e-11): --warmup untimed then --steps timed steps of fluid
-    step, Heun body step and cloud management, in FP32 and in FP64; per-step
-    wall time, the cube's path (all steps) and
-    accumulated rotation, and the FP32 run's deviation from the FP64 run."""
+    step, Heun body step and cloud management, in FP32, in FP64, and in FP64
+    from the FP32-rounded initial state; per-step wall time, the cube's path
+    (all steps) and accumulated rotation, and the deviations of the FP32 run
+    and of the rounded-start FP64 run from the FP64 run."""
     rank, world, local = dist_env()
     if rank != 0:
         return
@@ -612,8 +636,14 @@ def run_free_body(args):
     torch.cuda.set_device(local)
     import alebgk4paper_b200 as ab
     runs = {}
-    for prec in (32, 64):
+    # FP32, FP64, and FP64 started from the FP32-rounded initial state: the
+    # third run measures how far the body's path moves under a perturbation
+    # of the size of FP32 rounding alone, against which the FP32 run's
+    # deviation from FP64 is read.
+    for tag, prec, rounded in ((32, 32, False), (64, 64, False), ("64r", 64, True)):
         c = ab.Case("cavity3d-cube", 40, 10, -1.0, 2, fixed_body=False)
+        if rounded:
+            c.g[:] = c.g.astype(np.float32).astype(np.float64)
         s = ab.Solver(c, precision=prec, device=local)
         st = c.bodies.copy()
         path, t_step, t_body, t_refresh, changes = [st.copy()], 0.0, 0.0, 0.0, 0
@@ -640,14 +670,18 @@ def run_free_body(args):
         R0T = R[0].T
         ang = [float(np.degrees(np.arccos(np.clip((np.trace(Ri @ R0T) - 1) / 2, -1, 1))))
                for Ri in R]
-        runs[prec] = dict(path=path, angle=np.array(ang),
+        runs[tag] = dict(path=path, angle=np.array(ang),
                           s_per_step=(t_step + t_body + t_refresh) / args.steps,
                           fluid_ms=1e3 * t_step / args.steps, body_ms=1e3 * t_body / args.steps,
                           refresh_ms=1e3 * t_refresh / args.steps, cloud_changes=changes,
                           clocks=clk.summary())
-    a, b = runs[32], runs[64]
+    a, b, br = runs[32], runs[64], runs["64r"]
     disp64 = b["path"][-1, 0:3] - b["path"][0, 0:3]
     dev_centre = float(np.abs(a["path"][:, 0:3] - b["path"][:, 0:3]).max())
+    dev_centre_r = float(np.abs(br["path"][:, 0:3] - b["path"][:, 0:3]).max())
+
+    def rot_rel(x, y):
+        return float(abs(x["angle"][-1] - y["angle"][-1]) / max(abs(y["angle"][-1]), 1e-300))
     print(json.dumps({
         "metric": "free-body cube steps/s", "value": 1.0 / a["s_per_step"], "unit": "steps/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
@@ -660,10 +694,18 @@ def run_free_body(args):
         "f64": {k: b[k] for k in ("s_per_step", "fluid_ms", "body_ms", "refresh_ms",
                                   "cloud_changes")},
         "rotation_deg": {"f32": float(a["angle"][-1]), "f64": float(b["angle"][-1]),
-                         "rel_diff": float(abs(a["angle"][-1] - b["angle"][-1]) /
-                                           max(abs(b["angle"][-1]), 1e-300))},
+                         "f64_rounded_start": float(br["angle"][-1]),
+                         "rel_diff": rot_rel(a, b),
+                         "rel_diff_f64_rounded_start": rot_rel(br, b)},
+        "rotation_rel_diff_by_step": {
+            str(k): {"f32": rot_rel({"angle": a["angle"][:k + 1]}, {"angle": b["angle"][:k + 1]}),
+                     "f64_rounded_start": rot_rel({"angle": br["angle"][:k + 1]},
+                                                  {"angle": b["angle"][:k + 1]})}
+            for k in sorted({min(len(b["angle"]) - 1, m) for m in (500, 1000, 2000, 3000,
+                                                                   4000, 5000)})},
         "displacement_m": {"f64": disp64.tolist(),
                            "max_centre_diff_m": dev_centre,
+                           "max_centre_diff_f64_rounded_start_m": dev_centre_r,
                            "rel_to_displacement": dev_centre / max(np.linalg.norm(disp64),
                                                                    1e-300)},
         "clocks": a["clocks"],

@@ -102,7 +102,10 @@ typedef struct alebgk_counters
     double mass_after_transport; /* sumMass after transport (before rescale) */
     double mass_scale;        /* global rescale factor applied               */
     double mass_end;          /* sumMass at the end of the step               */
-    int error_word;           /* device-side error bits (0 = none)            */
+    int error_word;           /* device-side error bits (0 = none): 2 a lattice
+                                 march plane never arrived, 4 a streamed
+                                 particle row never arrived, 8 a batch's
+                                 persistent grid barrier gave up           */
     int transport_kernel;     /* transport in use: 1 coefficient gather,
                                  2 lattice march                              */
     int particle_kernel;      /* particle stage in use: 1 warp per particle,
@@ -278,6 +281,14 @@ int alebgk_body_set_surface_velocity(alebgk_ctx *ctx, int nbodies,
 int alebgk_set_launch(alebgk_ctx *ctx, int transport_threads, int particle_warps);
 int alebgk_get_launch(alebgk_ctx *ctx, int *transport_threads, int *particle_warps);
 
+/* Rounding floor of the MOOD NAD screen in FP32 mode: a slack of
+ * rel * max(|lo|, |hi|) added to the reference's (MLSTransport.cpp:370),
+ * where lo, hi is the neighbours' density range.  The default is 64 * 2^-24
+ * in FP32 mode and 0 in FP64 mode: the FP32 transported density carries
+ * rounding far above the reference's 1e-9 absolute slack near a uniform
+ * state.  Drops the captured step graphs. */
+int alebgk_set_nad_floor(alebgk_ctx *ctx, double rel);
+
 /* Velocities per lane of the lattice march: 2 (default; packed
  * fma.rn.f32x2 on two adjacent velocities, 64 velocities per block) or 1
  * (one velocity per lane, 32 per block).  Both widths give the same bits.
@@ -291,10 +302,18 @@ int alebgk_autotune(alebgk_ctx *ctx, int steps, float *best_ms);
 
 /* Steady residual of the last step over the interior particles: the largest
  * of ||d rho|| / ||rho||, ||d(rho ux)|| / ||rho c||, ||d(rho uy)|| / ||rho c||
- * and ||d(rho E)|| / ||rho E|| (2-norms over particles, E = |u|^2/2 + 3RT/2,
- * c = sqrt(RT) the thermal speed, so that momentum changes are measured
- * against the thermal momentum).  The reference defines no residual. */
+ * and ||d(rho E)|| / ||rho E|| (2-norms over particles, E = |u|^2/2 + 3RT/2).
+ * c is the speed set by alebgk_set_residual_speed (a lid speed, or the flow
+ * speed |u| so that momentum changes are measured against the flow's own
+ * momentum), else sqrt(RT), the thermal speed.  The reference defines no
+ * residual. */
 int alebgk_residual(alebgk_ctx *ctx, double *res);
+
+/* Speed scale c of the residual's momentum terms: a positive speed (a
+ * cavity's lid speed), a negative value for the flow speed |u| itself (the
+ * momentum field's own norm), or 0 (the default) for the thermal speed.  A
+ * batch copies it when the batch is created. */
+int alebgk_set_residual_speed(alebgk_ctx *ctx, double speed);
 
 /* The same measure between the macros of the previous call and now,
  * divided by the steps in between: the mean change per step over the
@@ -312,19 +331,27 @@ int alebgk_batch_step(alebgk_batch *b, int nsteps);
  * each group stepped by one launch per step stage over its contexts (the
  * groups are parallel branches of the graph), when the contexts share
  * precision and Chu layers and run the plain kernels; else mode 1.
- * mode 1: every context's own step as a branch of one graph.  staged
- * reports the form the captured graphs hold (the number of stage groups,
- * 0 for per-context branches).  set_groups sets the stage groups wanted
- * (default 4).  All forms give every context exactly the state of its own
- * steps. */
+ * mode 1: every context's own step as a branch of one graph.
+ * mode 2: under the conditions of mode 0, the whole step of every context
+ * in one persistent cooperative launch per step (the stages' blocks spread
+ * over the resident grid, a grid-wide barrier between stages); else mode 1.
+ * staged reports the form the captured graphs hold (the number of stage
+ * groups -- 1 for the persistent launch -- or 0 for per-context branches).
+ * set_groups sets the stage groups wanted in mode 0 (default 4).  All
+ * forms give every context exactly the state of its own steps. */
 int alebgk_batch_set_mode(alebgk_batch *b, int mode);
 int alebgk_batch_get_mode(alebgk_batch *b, int *mode, int *staged);
 int alebgk_batch_set_groups(alebgk_batch *b, int groups);
+/* Polls of the persistent launch's grid barrier before it gives up
+ * (default 2^24, polls >= 0).  A barrier that gives up ends the launch and
+ * sets bit 8 of the first context's error word (alebgk_sync then returns
+ * ALEBGK_EDEVICE); the step's state is then undefined. */
+int alebgk_batch_set_spin_limit(alebgk_batch *b, long long polls);
 /* Times `steps` steps of each form (stage launches in 1, 2, 4 and 8
- * groups, per-context branches) and keeps the fastest; *best_ms = its time
- * per step.  The timed steps are real steps: the batch advances by
- * (steps + 2) per form tried, (forms = 1 + the group counts in 1, 2, 4, 8
- * not above the number of contexts). */
+ * groups, the persistent launch, per-context branches) and keeps the
+ * fastest; *best_ms = its time per step.  The timed steps are real steps:
+ * the batch advances by (steps + 2) per form tried (forms = 2 + the group
+ * counts in 1, 2, 4, 8 not above the number of contexts). */
 int alebgk_batch_autotune(alebgk_batch *b, int steps, float *best_ms);
 int alebgk_batch_residuals(alebgk_batch *b, double *out);   /* n residuals */
 int alebgk_batch_sync(alebgk_batch *b);

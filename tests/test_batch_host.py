@@ -41,7 +41,7 @@ def test_batch_solver_rejects_unknown_forms_before_any_device_work():
     import pytest
     from alebgk4paper_b200.batch import BatchSolver
     with pytest.raises(ValueError, match="launch"):
-        BatchSolver([], launch="persistent")
+        BatchSolver([], launch="cooperative")
     with pytest.raises(ValueError, match="setup"):
         BatchSolver([], setup="gpu")
 
@@ -55,10 +55,14 @@ def test_batch_and_launch_entry_points_are_exported():
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     header = open(os.path.join(root, "include", "alebgk.h")).read()
     for name in ("alebgk_batch_set_mode", "alebgk_batch_get_mode", "alebgk_batch_set_groups",
-                 "alebgk_batch_autotune", "alebgk_set_launch", "alebgk_get_launch",
+                 "alebgk_batch_autotune", "alebgk_batch_set_spin_limit", "alebgk_set_launch",
+                 "alebgk_get_launch",
                  "alebgk_upload_geometry", "alebgk_set_coeff_builder"):
         assert f"{name}(" in header, name
         assert hasattr(lib, name), name
+    # the batch forms are 0, 1, 2; a negative poll limit is refused
+    assert lib.alebgk_batch_set_mode(None, 2) != 0
+    assert lib.alebgk_batch_set_spin_limit(None, 5) != 0
     # only 0, 1, 2 are builder modes; the setting is restored
     assert lib.alebgk_set_coeff_builder(3) != 0
     assert lib.alebgk_set_coeff_builder(-1) != 0

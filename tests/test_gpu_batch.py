@@ -150,14 +150,14 @@ def test_mixed_batch_falls_back_to_branches(gpu):
 
 
 def test_batch_autotune_keeps_states_exact(gpu):
-    """The batch autotuner's timed steps (stage groups 1, 2, 4 and per-cavity
-    branches) are real steps: afterwards every cavity holds exactly the state
-    of as many steps on its own."""
+    """The batch autotuner's timed steps (stage groups 1, 2, 4, the
+    persistent launch and per-cavity branches) are real steps: afterwards
+    every cavity holds exactly the state of as many steps on its own."""
     specs = batched_cavity2d(5, seed=11)
     b = BatchSolver(specs, precision=32)
     ms = b.autotune(2)
     assert ms > 0
-    assert b.steps == 4 * (2 + 2)
+    assert b.steps == 5 * (2 + 2)
     b.step(1)
     for i, sp in enumerate(specs):
         g0, m0, _ = _alone(sp, 32, b.steps)
@@ -167,7 +167,7 @@ def test_batch_autotune_keeps_states_exact(gpu):
     b.close()
 
 
-@pytest.mark.parametrize("launch", ["stages", "branches"])
+@pytest.mark.parametrize("launch", ["stages", "branches", "persistent"])
 def test_batch_recaptures_after_a_context_is_uploaded_again(gpu, launch):
     """A context uploaded again between batch steps has new buffers: the
     batch notices (upload epoch) and rebuilds its graphs, so the cavity
@@ -183,4 +183,53 @@ def test_batch_recaptures_after_a_context_is_uploaded_again(gpu, launch):
     for i in (1, 2):
         gi, mi, _ = _alone(specs[i], 32, 4)
         np.testing.assert_array_equal(b.solvers[i].cudaDownloadFull()[0], gi)
+    b.close()
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+def test_persistent_launch_equals_each_cavity_alone(gpu, precision):
+    """The whole step of the batch in one persistent cooperative launch
+    (every stage's blocks over the resident grid, a grid barrier between
+    stages): every cavity's distribution, macros and residual are bitwise
+    those of its own step."""
+    specs = batched_cavity2d(6, seed=13)
+    b = BatchSolver(specs, precision=precision, launch="persistent")
+    b.step(5)
+    assert b.staged == 1 and b.launch == "persistent"
+    res = b.residuals()
+    for i, sp in enumerate(specs):
+        g0, m0, r0 = _alone(sp, precision, 5)
+        g1, m1 = b.solvers[i].cudaDownloadFull()
+        np.testing.assert_array_equal(g1, g0)
+        np.testing.assert_array_equal(m1, m0)
+        assert res[i] == r0
+        assert b.solvers[i].counters()["error_word"] == 0
+    b.close()
+
+
+def test_persistent_request_falls_back_to_branches(gpu):
+    """Cavities that cannot share stage launches (2-D and 3-D, the lattice
+    march) run as per-cavity branches when the persistent launch is asked
+    for, each exactly as alone."""
+    b = BatchSolver(SPECS, precision=32, launch="persistent")
+    b.step(2)
+    assert b.staged == 0
+    for i, sp in enumerate(SPECS):
+        g0, _, _ = _alone(sp, 32, 2)
+        np.testing.assert_array_equal(b.solvers[i].cudaDownloadFull()[0], g0)
+    b.close()
+
+
+def test_persistent_barrier_gives_up_with_an_error(gpu):
+    """A grid barrier allowed no polls gives up at once: the launch ends,
+    bit 8 of the first cavity's error word is set and the host sees
+    ALEBGK_EDEVICE -- no wait without end on the device."""
+    specs = batched_cavity2d(3, seed=3)
+    b = BatchSolver(specs, precision=32, launch="persistent")
+    b.set_spin_limit(0)
+    b.step(1)
+    b.sync()
+    assert b.solvers[0].counters()["error_word"] & 8
+    with pytest.raises(ab.AlebgkError):
+        b.solvers[0].sync()
     b.close()

@@ -14,7 +14,14 @@ field (a component that is rounding noise at step 1, such as uy of a gas at
 rest under a lid moving in x, has no scale of its own).
 FP32 mode (FP32 f and reconstruction, FP64 sums) is held to its stated
 error against the same fixture: 5e-5 relative on rho and T and 2e-4 on the
-sampled rows, with flow velocities within 1e-3 of the lid speed.
+sampled rows.  Its flow velocities differ from the reference's by up to
+about 0.04 m/s (4 % of the 1 m/s lid speed) at step 10, next to the lid; the
+bound is 0.06 m/s.  That difference is the MOOD screen's, not FP32's: the
+FP32 screen carries a rounding floor (64 FP32 ulps of the neighbour density)
+and so takes none of the 665-1324 linear redos per step that the reference
+takes from step 4 on, and an FP64 run with the screen off differs from the
+reference by the same 0.04 m/s.  With the screen off in both, FP32 tracks
+FP64 to 1e-4 m/s (test_fp32_tracks_fp64_without_the_screen).
 """
 import numpy as np
 import pytest
@@ -94,7 +101,30 @@ def test_fp32_error_against_reference_at_full_size(gpu, fx):
         errs[step] = field_errors(o["macro"], ref)
         assert errs[step][0] < 5e-5 and errs[step][4] < 5e-5, errs[step]
         # flow velocities (up to the 1 m/s lid speed): absolute, in m/s
-        for q in (1, 2, 3):
-            assert np.abs(o["macro"][:, q] - ref[:, q]).max() < 1e-3, (step, q)
+        du = np.abs(o["macro"][:, 1:4] - ref[:, 1:4]).max()
+        print(f"FP32 vs reference at step {step}: max |du| {du:.3e} m/s")
+        assert du < (1e-3 if step == 1 else 0.06), (step, du)
         assert relmax(o["g"], fx[f"g_s{step}"]) < 2e-4
     print("FP32 vs reference, relative max error of rho ux uy uz T:", errs)
+
+
+def test_fp32_tracks_fp64_without_the_screen(gpu):
+    """The FP32 path's own error at full size, with the MOOD screen off in
+    both precisions so that both take the same scheme at every particle:
+    10 steps of FP32 against FP64 on the device."""
+    c = ab.Case("cavity3d", 40, 10, -1.0, 2)
+    out = {}
+    for prec in (32, 64):
+        cfg = c.config(prec, 0, 0, 0)
+        cfg.limiter = 0
+        s = ab.Solver(c, config=cfg)
+        s.cudaStep(10)
+        assert s.counters()["error_word"] == 0
+        out[prec] = s.cudaDownloadMoments()
+        s.close()
+    du = np.abs(out[32][:, 1:4] - out[64][:, 1:4]).max()
+    print(f"FP32 vs FP64, screen off, step 10: max |du| {du:.3e} m/s, rho "
+          f"{relmax(out[32][:, 0], out[64][:, 0]):.3e}, T {relmax(out[32][:, 4], out[64][:, 4]):.3e}")
+    assert du < 1e-3
+    assert relmax(out[32][:, 0], out[64][:, 0]) < 1e-5
+    assert relmax(out[32][:, 4], out[64][:, 4]) < 1e-5

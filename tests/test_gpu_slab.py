@@ -38,6 +38,13 @@ def test_slabs_step_like_the_whole_cavity(name, kw, n, precision, tol):
         assert np.abs(ms[:, :6] - mw[:, :6]).max(0).max() <= \
             tol * np.abs(mw[:, :6]).max()
         m_whole, m_slab = whole.cudaTotalMass(), group.total_mass()
-        assert abs(m_slab - m_whole) <= 1e-12 * m_whole
+        # The step's mass change is the collision's: the discrete
+        # Maxwellian's mass differs from rho by a function of (u, T) (its
+        # discretisation error), weighted by dt/tau.  In FP64 the two runs
+        # agree up to summation order; in FP32 their macros differ by the
+        # FP32 transport's rounding (~1e-6 relative, of random sign), so the
+        # masses part by ~1e-11 over the 12 steps.
+        mtol = 1e-12 if precision == 64 else 1e-9
+        assert abs(m_slab - m_whole) <= mtol * m_whole
     group.close()
     whole.cudaFreeCloud()
