@@ -18,7 +18,8 @@ import numpy as np
 from . import _abi
 
 __all__ = ["Case", "LatticeCase", "Solver", "AlebgkError", "load_library", "read_checkpoint",
-           "CASE_NAMES"]
+           "CASE_NAMES", "diagnostics", "write_vtk_host", "write_timeseries", "format_step",
+           "read_fields"]
 
 CASE_NAMES = ("cavity2d", "cavity3d", "cavity2d-square", "cavity2d-circle",
               "cavity3d-sphere", "cavity3d-cube")
@@ -77,6 +78,68 @@ def read_checkpoint(path: str, N: int | None = None, gstride: int | None = None,
                                       _ip(out["voxel"]), bodies))
     out["bodies"] = np.array([[bodies[b].state[k] for k in range(32)] for b in range(nb)])
     out["body_rotates"] = np.array([bodies[b].rotates for b in range(nb)], np.int32)
+    return out
+
+
+def _diag_dict(d) -> dict:
+    return {k: getattr(d, k) for k, _ in _abi.Diag._fields_}
+
+
+def _diag_struct(d: dict):
+    return _abi.Diag(**{k: d[k] for k, _ in _abi.Diag._fields_})
+
+
+def diagnostics(macro: np.ndarray, boundary: np.ndarray) -> dict:
+    """Interior averages of rho, kinetic energy, T, p, the moodFlag count and
+    the interior count from host arrays (macro N x 7, boundary N), in
+    particle order as computeDiagnostics (Core/Output.hpp:66-85)."""
+    lib = _abi.load()
+    m = np.ascontiguousarray(macro, np.float64)
+    b = np.ascontiguousarray(boundary, np.int32)
+    d = _abi.Diag()
+    _check(lib.alebgk_diagnostics_host(int(m.shape[0]), _dp(m), _ip(b), ctypes.byref(d)))
+    return _diag_dict(d)
+
+
+def write_vtk_host(path: str, xyz: np.ndarray, macro: np.ndarray, boundary: np.ndarray,
+                   Nv: int, time: float = 0.0):
+    """The reference's ASCII VTK frame (Core/Output.hpp:17-51) of host arrays."""
+    lib = _abi.load()
+    x = np.ascontiguousarray(xyz, np.float64)
+    m = np.ascontiguousarray(macro, np.float64)
+    b = np.ascontiguousarray(boundary, np.int32)
+    _check(lib.alebgk_vtk_write_host(str(path).encode(), int(x.shape[0]), _dp(x), _dp(m), _ip(b),
+                                     int(Nv), float(time)))
+
+
+def write_timeseries(path: str, t: float, diag: dict, header: bool = False):
+    """One timeseries.csv row (Core/Output.hpp:91-106); header=True truncates
+    the file and writes the column line first."""
+    d = _diag_struct(diag)
+    _check(_abi.load().alebgk_write_timeseries(str(path).encode(), float(t), ctypes.byref(d),
+                                               int(bool(header))))
+
+
+def format_step(step: int, t: float, dt: float, diag: dict) -> str:
+    """The reference's step line (printStep, Core/Output.hpp:111-115)."""
+    buf = ctypes.create_string_buffer(256)
+    d = _diag_struct(diag)
+    _check(_abi.load().alebgk_format_step(buf, 256, int(step), float(t), float(dt),
+                                          ctypes.byref(d)))
+    return buf.value.decode()
+
+
+def read_fields(path: str) -> dict:
+    """Reads a binary field dump (alebgk_write_fields): step, t, dim and the
+    xyz (N x 3), macro (N x 7) and boundary (N) arrays."""
+    lib = _abi.load()
+    h = _abi.FieldsHeader()
+    _check(lib.alebgk_read_fields(str(path).encode(), ctypes.byref(h), None, None, None))
+    n = int(h.N)
+    out = dict(step=int(h.step), t=float(h.t), dim=int(h.dim), N=n, xyz=np.zeros((n, 3)),
+               macro=np.zeros((n, 7)), boundary=np.zeros(n, np.int32))
+    _check(lib.alebgk_read_fields(str(path).encode(), ctypes.byref(h), _dp(out["xyz"]),
+                                  _dp(out["macro"]), _ip(out["boundary"])))
     return out
 
 
@@ -409,6 +472,23 @@ class Solver:
         cl = c.cloud()
         _check(self.lib.alebgk_upload_geometry(self.ctx, ctypes.byref(cl), self.dt), self.ctx)
         return counts
+
+    def write_vtk(self, outdir: str, step: int, time: float):
+        """The reference's VTK frame of the current state into
+        outdir/output_%06d.vtk (Core/Output.hpp:17-51)."""
+        _check(self.lib.alebgk_write_vtk(self.ctx, str(outdir).encode(), int(step), float(time)),
+               self.ctx)
+
+    def diagnostics(self) -> dict:
+        """Interior averages of the current state (Core/Output.hpp:66-85)."""
+        d = _abi.Diag()
+        _check(self.lib.alebgk_diagnostics(self.ctx, ctypes.byref(d)), self.ctx)
+        return _diag_dict(d)
+
+    def write_fields(self, path: str, step: int = 0, t: float = 0.0):
+        """Binary field dump of the current state at full precision."""
+        _check(self.lib.alebgk_write_fields(self.ctx, str(path).encode(), int(step), float(t)),
+               self.ctx)
 
     def checkpoint_save(self, path: str, step: int = 0, t: float = 0.0,
                         bodies: np.ndarray | None = None, voxel: np.ndarray | None = None):

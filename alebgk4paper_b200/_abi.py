@@ -50,6 +50,17 @@ class CkptHeader(ctypes.Structure):
                 ("t", ctypes.c_double), ("dim", ctypes.c_uint32), ("nbodies", ctypes.c_uint32)]
 
 
+class Diag(ctypes.Structure):
+    _fields_ = [("rho_avg", ctypes.c_double), ("KE", ctypes.c_double), ("T_avg", ctypes.c_double),
+                ("p_avg", ctypes.c_double), ("mood_count", ctypes.c_int), ("n", ctypes.c_int)]
+
+
+class FieldsHeader(ctypes.Structure):
+    _fields_ = [("magic", ctypes.c_char * 8), ("version", ctypes.c_uint32),
+                ("dim", ctypes.c_uint32), ("N", ctypes.c_uint64), ("step", ctypes.c_int64),
+                ("t", ctypes.c_double)]
+
+
 class Counters(ctypes.Structure):
     _fields_ = [
         ("steps", ctypes.c_int64), ("transport_flags", ctypes.c_int),
@@ -129,6 +140,23 @@ SIGNATURES = {
     "alebgk_checkpoint_save": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int64,
                                               ctypes.c_double, c_double_p, c_int_p, ctypes.c_int,
                                               ctypes.POINTER(Body)]),
+    "alebgk_vtk_write_host": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, c_double_p,
+                                             c_double_p, c_int_p, ctypes.c_int,
+                                             ctypes.c_double]),
+    "alebgk_write_vtk": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
+                                        ctypes.c_double]),
+    "alebgk_diagnostics_host": (ctypes.c_int, [ctypes.c_int, c_double_p, c_int_p,
+                                               ctypes.POINTER(Diag)]),
+    "alebgk_diagnostics": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Diag)]),
+    "alebgk_write_timeseries": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_double,
+                                               ctypes.POINTER(Diag), ctypes.c_int]),
+    "alebgk_format_step": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_int,
+                                          ctypes.c_double, ctypes.c_double,
+                                          ctypes.POINTER(Diag)]),
+    "alebgk_write_fields": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int64,
+                                           ctypes.c_double]),
+    "alebgk_read_fields": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(FieldsHeader),
+                                          c_double_p, c_double_p, c_int_p]),
     "alebgk_body_set_surface_velocity": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
                                                         c_double_p, c_double_p]),
     "alebgk_case_build": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int,

@@ -19,7 +19,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libalebgk_b200.so")
 
-SOURCES = ["step.cu", "march.cu", "body_noalloc.cu", "body_step.cu", "warm.cu", "coeffs_dev.cu", "classes_dev.cu", "setup.cu", "cloud.cu", "checkpoint.cpp", "batch.cpp", "slab.cpp", "api.cpp", "coeffs.cpp", "cases.cpp", "march_plan.cpp"]
+SOURCES = ["step.cu", "march.cu", "body_noalloc.cu", "body_step.cu", "warm.cu", "coeffs_dev.cu", "classes_dev.cu", "setup.cu", "cloud.cu", "checkpoint.cpp", "batch.cpp", "slab.cpp", "api.cpp", "coeffs.cpp", "cases.cpp", "march_plan.cpp", "fields.cpp"]
 # The device MLS table builder must round as the host builder (compiled
 # without contraction) does.
 FILE_FLAGS = {"coeffs_dev.cu": ["-fmad=false"]}

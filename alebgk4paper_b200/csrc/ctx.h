@@ -182,6 +182,7 @@ struct BatchLaunch
     bool persistent = false;
     int pGrid = 0;
     unsigned *bar = nullptr;
+    int *vmap = nullptr;      // virtual block -> cloud, per stage
     long long spinCap = 1ll << 24;
 };
 // cudaErrorNotSupported when the clouds cannot share launches (mixed

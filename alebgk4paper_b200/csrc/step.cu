@@ -2521,38 +2521,47 @@ __device__ void residualBody1024(const double *__restrict__ macNew,
 }
 
 // Grid-wide barrier of the persistent batch step: bar[0] counts the blocks
-// in, bar[1] is the generation, bar[2] an abort flag.  Every wait gives up
+// in, bar[kBarLine] is the generation, bar[2 kBarLine] an abort flag, and
+// bar[(3 + s) kBarLine] stage s's block counter, each on its own 128-byte
+// line so that the polls of the waiting blocks do not contend with the
+// arrivals' atomics.  Polls back off with __nanosleep.  Every wait gives up
 // after `cap` polls (or when another block has given up), raises the abort
 // flag and returns false; the caller then leaves the kernel.  The host
 // clears bar before every launch.
+constexpr int kBarLine = 32;
+constexpr int kBarWords = (3 + kBatchStages) * kBarLine;
+
 __device__ __forceinline__ bool gridBarrier(unsigned *bar, long long cap)
 {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0)
     {
-        volatile unsigned *vb = bar;
+        volatile unsigned *gen = bar + kBarLine, *abort = bar + 2 * kBarLine;
         ok = 1;
-        const unsigned gen = vb[1];
+        const unsigned g0 = *gen;
         __threadfence();
         if (atomicAdd(bar, 1u) == gridDim.x - 1)
         {
             atomicExch(bar, 0u);
             __threadfence();
-            atomicAdd(bar + 1, 1u);
+            atomicAdd(bar + kBarLine, 1u);
         }
         else
         {
             long long it = 0;
-            while (vb[1] == gen)
+            unsigned ns = 32;
+            while (*gen == g0)
             {
-                if (it >= cap || vb[2] != 0u)
+                if (it >= cap || *abort != 0u)
                 {
                     ok = 0;
-                    atomicExch(bar + 2, 1u);
+                    atomicExch(bar + 2 * kBarLine, 1u);
                     break;
                 }
                 ++it;
+                __nanosleep(ns);
+                if (ns < 256) ns <<= 1;
             }
         }
         __threadfence();
@@ -2561,56 +2570,105 @@ __device__ __forceinline__ bool gridBarrier(unsigned *bar, long long cap)
     return ok != 0;
 }
 
+// Stage bodies of the persistent batch step, each its own (not inlined)
+// function: register allocation is per function, so the particle body gets
+// the registers it gets in its own launch instead of sharing them with the
+// other stages' state (inlined together they spilled).
+template <typename T, int L>
+__device__ __noinline__ void persistentParticle(const BatchCtx<T> &B, int vb)
+{
+    k_particle_body<T, L, true>(B.pa, B.p, B.wpb, vb);
+}
+
+template <typename T, int L>
+__device__ __noinline__ void persistentRedo(const BatchCtx<T> &B, int vb, int vg)
+{
+    k_redo_body<T, L>(B.pa, B.p, vb, vg);
+}
+
+template <typename T>
+__device__ __noinline__ void persistentRecollide(const BatchCtx<T> &B, int vb, int vg)
+{
+    k_recollide_body<T>(B.pa.g, B.p, B.pa.boundary, B.pa.macNew, B.pa.massEnd, B.pa.sc, vb, vg);
+}
+
+template <typename T>
+__device__ __noinline__ void persistentResidual(const BatchCtx<T> &B)
+{
+    residualBody1024(B.pa.macNew, B.pa.macPrev, B.pa.boundary, B.p.N, B.p.R, B.resid, B.p.resU);
+}
+
 // The whole batch step in one launch: every stage of every cloud as
 // virtual blocks (the bodies, virtual block indices and grid sizes of the
 // stage launches, so every cloud computes what its own launches compute),
-// the blocks of a stage spread over a persistent grid, and a bounded
-// grid-wide barrier between stages.  A barrier that gives up sets bit 8 of
-// the first cloud's error word and ends the launch.
+// handed out to the resident blocks by a per-stage counter (the next index
+// is fetched while the current one runs), and a bounded grid-wide barrier
+// between stages.  vmap[s] is the start of stage s's virtual-block ->
+// cloud table within vmap.  A block keeps its cloud's descriptor in shared
+// memory while consecutive virtual blocks stay in that cloud.  A barrier
+// that gives up sets bit 8 of the first cloud's error word and ends the
+// launch.
 template <typename T, int L>
-__global__ void __launch_bounds__(kNT)
-k_batch_persistent(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ off, int n,
-                   unsigned *bar, long long cap)
+__global__ void __launch_bounds__(kNT, 3)
+k_batch_persistent(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ off,
+                   const int *__restrict__ vmap, int n, unsigned *bar, long long cap)
 {
-    auto blocksOf = [&](int stage) { return off[stage * (n + 1) + n]; };
-    auto barrier = [&]() {
-        if (gridBarrier(bar, cap)) return true;
+    __shared__ __align__(16) unsigned char raw[sizeof(BatchCtx<T>)];
+    __shared__ int sNext[2];
+    static_assert(sizeof(BatchCtx<T>) % 8 == 0, "descriptor words");
+    const BatchCtx<T> &B = *reinterpret_cast<const BatchCtx<T> *>(raw);
+    // Only the iteration count and the cached cloud stay live across a
+    // body (the particle body needs every register it can get): the stage's
+    // tables are re-derived from the parameters, and the next index is
+    // fetched into shared memory by the last warp at the start of each
+    // virtual block.
+    int cached = -1, it = 0;
+    bool alive = true;
+    auto run = [&](auto stageC, auto &&body) {
+        constexpr int stage = decltype(stageC)::value;
+        if (!alive) return;
+        if (threadIdx.x == 0) sNext[it & 1] = (int)atomicAdd(bar + (3 + stage) * kBarLine, 1u);
+        __syncthreads();
+        for (;;)
+        {
+            const int gb = sNext[it & 1];
+            const int *o = off + stage * (n + 1);
+            if (gb >= o[n]) break;
+            if (threadIdx.x == kNT - 32)
+                sNext[(it + 1) & 1] = (int)atomicAdd(bar + (3 + stage) * kBarLine, 1u);
+            const int c = vmap[vmap[stage] + gb];
+            if (c != cached)
+            {
+                const unsigned long long *src =
+                    reinterpret_cast<const unsigned long long *>(ctx + c);
+                unsigned long long *dst = reinterpret_cast<unsigned long long *>(raw);
+                for (int w = threadIdx.x; w < (int)(sizeof(BatchCtx<T>) / 8); w += blockDim.x)
+                    dst[w] = src[w];
+                cached = c;
+                __syncthreads();
+            }
+            body(o[c + 1] - o[c], gb - o[c]);
+            ++it;
+            __syncthreads();
+        }
+        if (gridBarrier(bar, cap)) return;
         if (threadIdx.x == 0) atomicOr(&ctx[0].pa.sc->err, 8);
-        return false;
+        alive = false;
     };
-    int vb, vg;
     // 0: counters
-    for (int b = blockIdx.x; b < blocksOf(0); b += gridDim.x)
-    {
-        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 0, vb, vg, b);
+    run(std::integral_constant<int, 0>{}, [&](int, int vb) {
         if (vb == 0 && threadIdx.x == 0)
         {
             StepScalars *sc = B.pa.sc;
             sc->nflag = 0; sc->ndeg = 0; sc->nfix = 0; sc->moodfail = 0;
         }
-        __syncthreads();
-    }
-    if (!barrier()) return;
+    });
     // 2: transport + particle stage (fused)
-    for (int b = blockIdx.x; b < blocksOf(2); b += gridDim.x)
-    {
-        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 2, vb, vg, b);
-        k_particle_body<T, L, true>(B.pa, B.p, B.wpb, vb);
-        __syncthreads();
-    }
-    if (!barrier()) return;
+    run(std::integral_constant<int, 2>{}, [&](int, int vb) { persistentParticle<T, L>(B, vb); });
     // 3: linear redo of the flagged particles
-    for (int b = blockIdx.x; b < blocksOf(3); b += gridDim.x)
-    {
-        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 3, vb, vg, b);
-        k_redo_body<T, L>(B.pa, B.p, vb, vg);
-        __syncthreads();
-    }
-    if (!barrier()) return;
+    run(std::integral_constant<int, 3>{}, [&](int vg, int vb) { persistentRedo<T, L>(B, vb, vg); });
     // 4: sigma
-    for (int b = blockIdx.x; b < blocksOf(4); b += gridDim.x)
-    {
-        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 4, vb, vg, b);
+    run(std::integral_constant<int, 4>{}, [&](int vg, int vb) {
         StepScalars *sc = B.pa.sc;
         double m;
         if (gridSumLast(B.pa.massPos, B.p.N, B.redPartial, sc, &m, vb, vg))
@@ -2618,21 +2676,11 @@ k_batch_persistent(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ 
             sc->massNew = m;
             sc->sigma = (m > 1.0e-30) ? sc->massOld / m : 1.0;
         }
-        __syncthreads();
-    }
-    if (!barrier()) return;
+    });
     // 5: fixup
-    for (int b = blockIdx.x; b < blocksOf(5); b += gridDim.x)
-    {
-        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 5, vb, vg, b);
-        k_fixup_body<T>(B.pa, B.p, vb, vg);
-        __syncthreads();
-    }
-    if (!barrier()) return;
+    run(std::integral_constant<int, 5>{}, [&](int vg, int vb) { k_fixup_body<T>(B.pa, B.p, vb, vg); });
     // 6: end-of-step mass
-    for (int b = blockIdx.x; b < blocksOf(6); b += gridDim.x)
-    {
-        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 6, vb, vg, b);
+    run(std::integral_constant<int, 6>{}, [&](int vg, int vb) {
         StepScalars *sc = B.pa.sc;
         double m;
         if (gridSumLast(B.pa.massEnd, B.p.N, B.redPartial, sc, &m, vb, vg))
@@ -2643,30 +2691,15 @@ k_batch_persistent(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ 
             sc->scale = sigma;
             sc->steps += 1;
         }
-        __syncthreads();
-    }
-    if (!barrier()) return;
+    });
     // 7: sigma on the macros, moodCheck
-    for (int b = blockIdx.x; b < blocksOf(7); b += gridDim.x)
-    {
-        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 7, vb, vg, b);
+    run(std::integral_constant<int, 7>{}, [&](int, int vb) {
         k_scale_mood_body(B.p, B.pa.boundary, B.pa.macNew, B.pa.minG, B.mood, B.pa.sc, vb);
-        __syncthreads();
-    }
-    if (!barrier()) return;
+    });
     // 8: second collision where moodCheck failed
-    for (int b = blockIdx.x; b < blocksOf(8); b += gridDim.x)
-    {
-        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 8, vb, vg, b);
-        k_recollide_body<T>(B.pa.g, B.p, B.pa.boundary, B.pa.macNew, B.pa.massEnd, B.pa.sc, vb,
-                            vg);
-        __syncthreads();
-    }
-    if (!barrier()) return;
+    run(std::integral_constant<int, 8>{}, [&](int vg, int vb) { persistentRecollide<T>(B, vb, vg); });
     // 9: end mass after a second collision
-    for (int b = blockIdx.x; b < blocksOf(9); b += gridDim.x)
-    {
-        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 9, vb, vg, b);
+    run(std::integral_constant<int, 9>{}, [&](int vg, int vb) {
         StepScalars *sc = B.pa.sc;
         double m;
         if (sc->moodfail != 0 &&
@@ -2675,17 +2708,9 @@ k_batch_persistent(const BatchCtx<T> *__restrict__ ctx, const int *__restrict__ 
             sc->massEnd = sc->sigma * m;
             sc->massOld = sc->massEnd;
         }
-        __syncthreads();
-    }
-    if (!barrier()) return;
+    });
     // 10: steady residual (1024-thread virtual blocks)
-    for (int b = blockIdx.x; b < blocksOf(10); b += gridDim.x)
-    {
-        const BatchCtx<T> &B = batchStage<T>(ctx, off, n, 10, vb, vg, b);
-        residualBody1024(B.pa.macNew, B.pa.macPrev, B.pa.boundary, B.p.N, B.p.R, B.resid,
-                         B.p.resU);
-        __syncthreads();
-    }
+    run(std::integral_constant<int, 10>{}, [&](int, int) { persistentResidual<T>(B); });
 }
 
 #undef BATCH_CTX
@@ -2757,8 +2782,21 @@ static cudaError_t buildBatchT(alebgk_ctx *const *cs, int n, double *const *resi
             e = cudaMemcpy(bl.desc[from], h[from].data(), sizeof(BatchCtx<T>) * n,
                            cudaMemcpyHostToDevice);
     }
-    if (e == cudaSuccess) e = cudaMalloc(&bl.bar, 4 * sizeof(unsigned));
-    if (e == cudaSuccess) e = cudaMemset(bl.bar, 0, 4 * sizeof(unsigned));
+    // the persistent launch's virtual-block -> cloud tables: 16 stage
+    // starts, then per stage one entry per virtual block
+    std::vector<int> vm(16, 0);
+    for (int s = 0; s < kBatchStages; ++s)
+    {
+        vm[s] = (int)vm.size();
+        for (int i = 0; i < n; ++i)
+            for (int b = off[(size_t)s * (n + 1) + i]; b < off[(size_t)s * (n + 1) + i + 1]; ++b)
+                vm.push_back(i);
+    }
+    if (e == cudaSuccess) e = cudaMalloc(&bl.vmap, sizeof(int) * vm.size());
+    if (e == cudaSuccess)
+        e = cudaMemcpy(bl.vmap, vm.data(), sizeof(int) * vm.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&bl.bar, kBarWords * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(bl.bar, 0, kBarWords * sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMalloc(&bl.off, sizeof(int) * off.size());
     if (e == cudaSuccess)
         e = cudaMemcpy(bl.off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice);
@@ -2843,7 +2881,7 @@ static cudaError_t batchPersistentT(const BatchLaunch &bl, int from, cudaStream_
     const int grid = std::min(bl.pGrid, most);
     if (grid < 1) return cudaErrorLaunchOutOfResources;
     const BatchCtx<T> *ctx = static_cast<const BatchCtx<T> *>(bl.desc[from]);
-    cudaError_t e = cudaMemsetAsync(bl.bar, 0, 4 * sizeof(unsigned), st);
+    cudaError_t e = cudaMemsetAsync(bl.bar, 0, kBarWords * sizeof(unsigned), st);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
@@ -2857,8 +2895,8 @@ static cudaError_t batchPersistentT(const BatchLaunch &bl, int from, cudaStream_
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_batch_persistent<T, L>, ctx, (const int *)bl.off, bl.n,
-                              bl.bar, bl.spinCap);
+    return cudaLaunchKernelEx(&cfg, k_batch_persistent<T, L>, ctx, (const int *)bl.off,
+                              (const int *)bl.vmap, bl.n, bl.bar, bl.spinCap);
 }
 
 cudaError_t prepareBatchLaunch(const BatchLaunch &bl)
@@ -2884,7 +2922,7 @@ cudaError_t launchBatchStep(const BatchLaunch &bl, int from, cudaStream_t st)
 
 void freeBatchLaunch(BatchLaunch &bl)
 {
-    for (void *p : {bl.desc[0], bl.desc[1], (void *)bl.off, (void *)bl.bar})
+    for (void *p : {bl.desc[0], bl.desc[1], (void *)bl.off, (void *)bl.bar, (void *)bl.vmap})
         if (p) cudaFree(p);
     bl = BatchLaunch();
 }

@@ -37,6 +37,7 @@ extern "C" {
 #define ALEBGK_ESTATE (-3)   /* call out of order (e.g. step before upload) */
 #define ALEBGK_ENOMEM (-4)   /* host or device allocation failed          */
 #define ALEBGK_EDEVICE (-5)  /* a device-side check failed (error word)   */
+#define ALEBGK_EIO (-6)      /* a field file could not be opened, read or written */
 
 #define ALEBGK_MAX_NEIGH 128 /* Core/Types.hpp:22 (MAX_NEIGH)             */
 
@@ -530,6 +531,69 @@ int alebgk_checkpoint_read(const char *path, const alebgk_ckpt_header *expect,
 int alebgk_checkpoint_save(alebgk_ctx *ctx, const char *path, int64_t step, double t,
                            const double *vgrid, const int *voxel, int nbodies,
                            const alebgk_body *bodies);
+
+/* ---- field output -------------------------------------------------------
+ * The reference's save-cycle output (Core/Output.hpp:17-115, called from
+ * Solver/Solver.cpp:548-560): an ASCII VTK frame, interior diagnostics, a
+ * timeseries.csv row and the printStep line; and a binary dump of the same
+ * fields at full precision (no reference counterpart: the VTK frame keeps
+ * seven significant digits). */
+typedef struct
+{
+    double rho_avg, KE, T_avg, p_avg;  /* interior averages (KE = 0.5 rho |u|^2) */
+    int mood_count;                    /* interior particles with moodFlag set   */
+    int n;                             /* interior particles                     */
+} alebgk_diag;
+
+/* The reference's ASCII VTK frame (writeVTK, Core/Output.hpp:17-51) from host
+ * arrays: positions xyz (N*3), per-particle rho ux uy uz T p moodFlag (macro,
+ * N*7, the layout of alebgk_download_moments), boundary flags (N), Nv_local =
+ * Nv for every particle, and the time in the title line.  Every number is
+ * printed as the reference's stream prints it (scientific, six decimals), so
+ * the file is the reference's byte for byte for the same data.  Formatted in
+ * parallel (OpenMP), written once.  ALEBGK_EIO if the file cannot be
+ * written. */
+int alebgk_vtk_write_host(const char *path, int N, const double *xyz, const double *macro,
+                          const int *boundary, int Nv, double time);
+
+/* The same for the context's current state (positions and moments from the
+ * device, boundary flags from the upload) into outdir/output_%06d.vtk, the
+ * reference's frame name.  Replaces writeVTK after cudaDownloadMoments
+ * (Solver/Solver.cpp:552-556). */
+int alebgk_write_vtk(alebgk_ctx *ctx, const char *outdir, int step, double time);
+
+/* Interior averages in particle order (computeDiagnostics,
+ * Core/Output.hpp:66-85), from host arrays or from the context. */
+int alebgk_diagnostics_host(int N, const double *macro, const int *boundary, alebgk_diag *out);
+int alebgk_diagnostics(alebgk_ctx *ctx, alebgk_diag *out);
+
+/* One timeseries.csv row (writeTimeseries, Core/Output.hpp:91-106).  header
+ * != 0 truncates the file and writes the column line first, which the
+ * reference does on its first call in the process; 0 appends. */
+int alebgk_write_timeseries(const char *path, double t, const alebgk_diag *d, int header);
+
+/* The reference's step line (printStep, Core/Output.hpp:111-115) into buf;
+ * ALEBGK_EINVAL if it does not fit in len bytes. */
+int alebgk_format_step(char *buf, size_t len, int step, double t, double dt,
+                       const alebgk_diag *d);
+
+/* Binary field dump: this header, then xyz (N*3 FP64), macro (N*7 FP64, the
+ * layout of alebgk_download_moments) and boundary (N int32), little endian
+ * as the device writes them.  Written to path.tmp and renamed.  read_fields
+ * fills the header and the non-NULL arrays; ALEBGK_EIO on a short file or a
+ * wrong magic or version. */
+typedef struct
+{
+    char magic[8];            /* "ALBGKFLD" */
+    uint32_t version;         /* 1 */
+    uint32_t dim;
+    uint64_t N;
+    int64_t step;
+    double t;
+} alebgk_fields_header;
+int alebgk_write_fields(alebgk_ctx *ctx, const char *path, int64_t step, double t);
+int alebgk_read_fields(const char *path, alebgk_fields_header *h, double *xyz, double *macro,
+                       int *boundary);
 
 /* ---- host-side MLS coefficient tables (no device work) -------------------
  * The stencil classes and FP64 transport coefficients that alebgk_upload

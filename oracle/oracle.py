@@ -178,6 +178,10 @@ class RefCase:
                                  ctypes.c_int, ctypes.c_int, ctypes.c_double]
         L.ref_sum_mass.restype = ctypes.c_double
         L.ref_max_threads.restype = ctypes.c_int
+        if hasattr(L, "ref_write_vtk"):
+            L.ref_write_vtk.argtypes = [_vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_double]
+            L.ref_write_timeseries.argtypes = [_vp, ctypes.c_char_p, ctypes.c_double]
+            L.ref_print_step.argtypes = [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double]
         self.L = L
         self.h = _vp(L.ref_create(name.encode(), int(Nx), int(Nv), float(dt), int(mls_order),
                                   int(bool(fixed_body)), float(body_scale)))
@@ -242,6 +246,24 @@ class RefCase:
 
     def sum_mass(self):
         return self.L.ref_sum_mass(self.h)
+
+    # The reference's save-cycle output (Core/Output.hpp) of the case's
+    # particles: a VTK frame, diagnostics, a timeseries row (the first call
+    # in the process writes the column line) and the step line on stdout.
+    def write_vtk(self, outdir, step, time):
+        self.L.ref_write_vtk(self.h, str(outdir).encode(), int(step), float(time))
+
+    def diagnostics(self):
+        d = np.zeros(6)
+        self.L.ref_diagnostics(self.h, _p(d))
+        return dict(rho_avg=d[0], KE=d[1], T_avg=d[2], p_avg=d[3], mood_count=int(d[4]),
+                    n=int(d[5]))
+
+    def write_timeseries(self, path, t):
+        self.L.ref_write_timeseries(self.h, str(path).encode(), float(t))
+
+    def print_step(self, step, t, dt):
+        self.L.ref_print_step(self.h, int(step), float(t), float(dt))
 
     def bodies(self):
         out = np.zeros((max(1, self.nbodies), 32))

@@ -24,6 +24,7 @@
 #include "RigidBody.hpp"
 #include "TestCases.hpp"
 #include "Checkpoint.hpp"
+#include "Output.hpp"
 
 #include <chrono>
 #include <cmath>
@@ -412,6 +413,33 @@ int ref_checkpoint_load(void *h, const char *path, long *step, double *t)
     const bool ok = ckpt::restore(path, step, t, c->P, c->bodies);
     if (ok) { c->step = *step; c->t = *t; }
     return ok ? 1 : 0;
+}
+
+// The reference's own save-cycle output (Core/Output.hpp): the VTK frame of
+// the case's particles, the interior diagnostics, one timeseries row (the
+// first call in the process writes the column line) and the step line on
+// stdout.
+void ref_write_vtk(void *h, const char *outdir, int step, double time)
+{
+    writeVTK(static_cast<RefCase *>(h)->P, outdir, step, time);
+}
+
+void ref_diagnostics(void *h, double *out)
+{
+    const Diagnostics d = computeDiagnostics(static_cast<RefCase *>(h)->P);
+    out[0] = d.rho_avg; out[1] = d.KE; out[2] = d.T_avg; out[3] = d.p_avg;
+    out[4] = d.moodCount; out[5] = d.n;
+}
+
+void ref_write_timeseries(void *h, const char *path, double t)
+{
+    writeTimeseries(path, t, computeDiagnostics(static_cast<RefCase *>(h)->P));
+}
+
+void ref_print_step(void *h, int step, double t, double dt)
+{
+    printStep(step, t, dt, computeDiagnostics(static_cast<RefCase *>(h)->P));
+    std::fflush(stdout);
 }
 
 void ref_checkpoint_sizes(int *out)

@@ -58,6 +58,24 @@ BODY_RUNS = [
     ("square_n24_v8_free", "cavity2d-square", 24, 8),
 ]
 BODY_STEPS = 8
+# A long free-body run: the cube of cavity3d-cube (Nx 12, Nv 4) moves three
+# to four lattice steps and turns by 110 degrees in 2000 steps, and the cloud
+# management changes the particle set on most steps after step 254.  Kept:
+# the particle count after every step and the body state every 10 steps.
+LONG_BODY = ("cube_n12_v4_free_s2000", "cavity3d-cube", 12, 4, 2000, 10)
+
+
+def write_long_body(tag, case, Nx, Nv, steps, every):
+    r = RefCase(case, Nx, Nv, -1.0, 2, fixed_body=False)
+    b0 = r.bodies().copy()
+    hist, counts = [], []
+    for k in range(1, steps + 1):
+        r.step(1)
+        counts.append(r.N)
+        if k % every == 0:
+            hist.append(r.bodies().copy())
+    np.savez_compressed(os.path.join(HERE, f"body_{tag}.npz"), bodies_before=b0,
+                        bodies=np.array(hist), N=np.array(counts), every=every)
 
 
 def nbr_hash(nbr: np.ndarray, nnb: np.ndarray) -> np.ndarray:
@@ -91,6 +109,8 @@ def main(only=None):
         for tag, case, Nx, Nv, order, steps, full in STEPS + LONG_STEPS:
             if tag in only:
                 write_step(tag, case, Nx, Nv, order, steps, full)
+        if LONG_BODY[0] in only:
+            write_long_body(*LONG_BODY)
         return
     for case, Nx, Nv, order, fixed in SETUPS:
         r = RefCase(case, Nx, Nv, -1.0, order, fixed_body=fixed)
@@ -116,6 +136,7 @@ def main(only=None):
             counts.append(r.N)
         np.savez_compressed(os.path.join(HERE, f"body_{tag}.npz"), bodies_before=b0,
                             bodies=np.array(hist), N=np.array(counts))
+    write_long_body(*LONG_BODY)
     print("fixtures written to", HERE)
 
 

@@ -62,6 +62,57 @@ def test_free_body_history_matches_reference(gpu, tag, case, Nx, Nv):
     s.close()
 
 
+def _long_run(precision, steps):
+    """The free cube of cavity3d-cube (Nx 12, Nv 4) for `steps` steps of
+    fluid step, Heun body step and cloud management; particle counts after
+    every step and the body state every 10 steps."""
+    c = ab.Case("cavity3d-cube", 12, 4, -1.0, 2, fixed_body=False)
+    s = ab.Solver(c, precision=precision)
+    st = c.bodies.copy()
+    counts, hist = [], []
+    for k in range(1, steps + 1):
+        s.cudaStep(1)
+        st = s.body_step(st)
+        c.bodies = st
+        s.refresh_geometry()
+        counts.append(c.N)
+        if k % 10 == 0:
+            hist.append(st[0].copy())
+    s.close()
+    return np.array(counts), np.array(hist)
+
+
+def _rotation_deg(hist, b0):
+    R = hist[:, 22:31].reshape(-1, 3, 3)
+    R0T = b0[22:31].reshape(3, 3).T
+    return np.degrees(np.arccos(np.clip((np.einsum("kii->k", R @ R0T) - 1) / 2, -1, 1)))
+
+
+def test_free_body_2000_steps_match_reference(gpu):
+    """2000 steps of the free cube in FP64 against the compiled reference's
+    own moving-body run: the cube moves three to four lattice steps and
+    turns by 110 degrees, and the cloud management changes the particle set
+    on most steps after step 254.  Every step's particle count is the
+    reference's (so every removal, merge and addition decision is), and the
+    body state follows the reference's to the bounds below."""
+    fx = golden("body_cube_n12_v4_free_s2000.npz")
+    counts, hist = _long_run(64, len(fx["N"]))
+    first = int(np.argmax(counts != fx["N"])) if (counts != fx["N"]).any() else -1
+    assert first < 0, f"particle count departs at step {first + 1}"
+    want = fx["bodies"][:, 0]
+    b0 = fx["bodies_before"][0]
+    for name, sl in (("centre", slice(0, 3)), ("velocity", slice(3, 6)),
+                     ("spin", slice(7, 10)), ("orientation", slice(22, 31))):
+        w = want[:, sl] - (b0[sl] if name == "centre" else 0.0)
+        g = hist[:, sl] - (b0[sl] if name == "centre" else 0.0)
+        err = np.abs(g - w).max() / np.abs(w).max()
+        print(f"FP64 free cube, 2000 steps: {name} max error {err:.2e} of its range")
+        assert err < 1e-6, name
+    rot, rot_ref = _rotation_deg(hist, b0)[-1], _rotation_deg(want, b0)[-1]
+    print(f"rotation after 2000 steps: {rot:.6f} deg (reference {rot_ref:.6f})")
+    assert abs(rot - rot_ref) <= 1e-6 * rot_ref
+
+
 def test_body_step_rigid_motion_and_wall_state(gpu):
     """A cube given a velocity and a spin: its surface particles move by the
     rigid motion of the old state (Rodrigues rotation about the old angular
