@@ -233,8 +233,10 @@ def _run_reference(args):
     r.set_threads(cores)
     updates = r.N * r.Nv ** 3
     # A bounded sample: the first warm-up step is timed to project the run;
-    # steps are capped so that the whole arm ends within a few minutes.
-    budget = float(os.environ.get("ALEBGK_REF_BUDGET_S", "150"))
+    # steps are capped so that the whole arm ends within a few minutes.  At
+    # the reference's 7.9 s per step on the box's 16 cores, 240 s covers the
+    # default 3 warm-up and 20 timed steps in full.
+    budget = float(os.environ.get("ALEBGK_REF_BUDGET_S", "240"))
     t0 = time.perf_counter()
     r.step(1)
     t1 = time.perf_counter() - t0
@@ -647,6 +649,9 @@ def run_free_body(args):
         s = ab.Solver(c, precision=prec, device=local)
         st = c.bodies.copy()
         path, t_step, t_body, t_refresh, changes = [st.copy()], 0.0, 0.0, 0.0, 0
+        # the density range every 100 steps (the scheme's own instability
+        # shows there first), and the first step with a non-finite body state
+        rho_range, nonfinite = [], None
         with ClockSampler(local) as clk:
             for k in range(args.warmup + args.steps):
                 if k == args.warmup:
@@ -664,18 +669,31 @@ def run_free_body(args):
                 t_body += t2 - t1
                 t_refresh += t3 - t2
                 path.append(st.copy())
+                if not np.isfinite(st).all():
+                    nonfinite = k + 1
+                    break
+                if (k + 1) % 100 == 0:
+                    m = s.cudaDownloadMoments()
+                    rho_range.append([k + 1, float(np.nanmin(m[:, 0])), float(np.nanmax(m[:, 0]))])
         s.close()
         path = np.array(path)[:, 0]
         R = path[:, 22:31].reshape(-1, 3, 3)
         R0T = R[0].T
         ang = [float(np.degrees(np.arccos(np.clip((np.trace(Ri @ R0T) - 1) / 2, -1, 1))))
                for Ri in R]
-        runs[tag] = dict(path=path, angle=np.array(ang),
-                          s_per_step=(t_step + t_body + t_refresh) / args.steps,
-                          fluid_ms=1e3 * t_step / args.steps, body_ms=1e3 * t_body / args.steps,
-                          refresh_ms=1e3 * t_refresh / args.steps, cloud_changes=changes,
+        done = max(1, len(path) - 1 - args.warmup)
+        runs[tag] = dict(path=path, angle=np.array(ang), rho_range=rho_range, nonfinite=nonfinite,
+                          s_per_step=(t_step + t_body + t_refresh) / done,
+                          fluid_ms=1e3 * t_step / done, body_ms=1e3 * t_body / done,
+                          refresh_ms=1e3 * t_refresh / done, cloud_changes=changes,
                           clocks=clk.summary())
     a, b, br = runs[32], runs[64], runs["64r"]
+    # compare over the steps every run finished with a finite body state
+    n = min(len(x["path"]) for x in (a, b, br))
+    while n > 1 and not all(np.isfinite(x["path"][n - 1]).all() for x in (a, b, br)):
+        n -= 1
+    for x in (a, b, br):
+        x["path"], x["angle"] = x["path"][:n], x["angle"][:n]
     disp64 = b["path"][-1, 0:3] - b["path"][0, 0:3]
     dev_centre = float(np.abs(a["path"][:, 0:3] - b["path"][:, 0:3]).max())
     dev_centre_r = float(np.abs(br["path"][:, 0:3] - b["path"][:, 0:3]).max())
@@ -690,9 +708,10 @@ def run_free_body(args):
         "config": {"workload": "cavity3d-cube free body Nx=40 Nv=10, rho 4.4, parabolic lid "
                                "10 m/s, dt 1.5e-11"},
         "f32": {k: a[k] for k in ("s_per_step", "fluid_ms", "body_ms", "refresh_ms",
-                                  "cloud_changes")},
+                                  "cloud_changes", "nonfinite", "rho_range")},
         "f64": {k: b[k] for k in ("s_per_step", "fluid_ms", "body_ms", "refresh_ms",
-                                  "cloud_changes")},
+                                  "cloud_changes", "nonfinite", "rho_range")},
+        "compared_steps": n - 1,
         "rotation_deg": {"f32": float(a["angle"][-1]), "f64": float(b["angle"][-1]),
                          "f64_rounded_start": float(br["angle"][-1]),
                          "rel_diff": rot_rel(a, b),
