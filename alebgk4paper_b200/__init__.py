@@ -226,38 +226,72 @@ class Case:
 
 
 class LatticeCase:
-    """A box cavity without bodies whose set-up runs on the device.
+    """A case whose set-up runs on the device.
 
-    It carries the case parameters only (``alebgk_lattice_info``); the lattice,
-    wall state, neighbour lists and rest state are built on the GPU when a
-    :class:`Solver` takes it (``alebgk_upload_lattice``), bitwise equal to
-    what :class:`Case` builds on the host.  Same arguments as :class:`Case`.
+    It carries the case parameters (``alebgk_lattice_info_ex``) and the
+    bodies' descriptions (``alebgk_lattice_bodies``); the lattice, wall
+    state, body embedding, neighbour lists and rest state are built on the
+    GPU when a :class:`Solver` takes it (``alebgk_upload_lattice_ex``),
+    bitwise equal to what :class:`Case` builds on the host.  Same arguments
+    as :class:`Case`; for a case with bodies the particle count after the
+    embedding comes from a device set-up on ``device``, and the host arrays
+    a moving-body run manages (positions, flags, wall state, neighbours) are
+    fetched from it.
     """
 
     def __init__(self, name: str, Nx: int = -1, Nv: int = -1, dt: float = -1.0,
                  mls_order: int = 2, lid_speed: float = -1.0, rho0: float = -1.0,
-                 tau: float = -1.0):
+                 tau: float = -1.0, fixed_body: bool = False, body_scale: float = 1.0,
+                 device: int = 0):
         lib = _abi.load()
         self._args = (name.encode(), int(Nx), int(Nv), float(dt), int(mls_order),
-                      float(lid_speed), float(rho0), float(tau))
+                      int(bool(fixed_body)), float(body_scale), float(lid_speed), float(rho0),
+                      float(tau))
         info = np.zeros(8, np.int32)
         prm = np.zeros(24)
-        _check(lib.alebgk_lattice_info(*self._args, _ip(info), _dp(prm)))
+        _check(lib.alebgk_lattice_info_ex(*self._args, int(device), _ip(info), _dp(prm)))
         self.name = name
         self.N, self.dim, self.Nv, self.gstride = int(info[0]), int(info[1]), int(info[2]), \
             int(info[3])
-        self.nbodies, self.mls_order, self.Nx = 0, int(info[5]), int(info[6])
-        self.moving_bodies = False
+        self.nbodies, self.mls_order, self.Nx = int(info[4]), int(info[5]), int(info[6])
+        self.moving_bodies = bool(info[7])
         keys = ("dt", "tau", "R", "dx", "dy", "dz", "radius", "minDist", "dv",
                 "vmin", "vmax", "rho0", "Tw", "xleft", "xright", "ybottom", "ytop",
                 "zfront", "zback", "dt_requested", "tfinal", "dHS", "lid_speed",
                 "save_every")
         self.params = {k: float(v) for k, v in zip(keys, prm)}
         self.dt = self.params["dt"]
-        self.bodies = np.zeros((0, 32))
+        nb = max(1, self.nbodies)
+        st, kind = np.zeros(32 * nb), np.zeros(nb, np.int32)
+        rot, size = np.zeros(nb, np.int32), np.zeros(nb)
+        n = ctypes.c_int()
+        _check(lib.alebgk_lattice_bodies(*self._args[:7], ctypes.byref(n), _dp(st), _ip(kind),
+                                         _ip(rot), _dp(size)))
+        self.bodies = st.reshape(-1, 32)[: self.nbodies].copy()
+        self.body_kind = kind[: self.nbodies].copy()
+        self.body_rotates = rot[: self.nbodies].copy()
+        self.body_size = size[: self.nbodies].copy()
         self._xyz = None
+        # host distribution and macros: none until a cloud-management change
+        # of a moving-body run reads them back (then uploads go through them)
+        self.g = self.macro = None
+        if self.nbodies:
+            out = self.build_on_device(device)
+            self.meshv = np.zeros((self.N, 3))
+            for k in ("wall", "boundary", "body_id", "nnb", "nbr"):
+                setattr(self, k, out[k])
 
     config = Case.config
+
+    def cloud(self) -> _abi.Cloud:
+        """A C-ABI view of the host arrays (geometry; g and macro only once a
+        cloud-management change has read them back)."""
+        self._keep = [None if a is None else np.ascontiguousarray(a) for a in
+                      (self.xyz, self.meshv, self.wall, self.boundary, self.body_id,
+                       self.nnb, self.nbr, self.g, self.macro)]
+        xyz, mv, wall, b, bid, nnb, nbr, g, mac = self._keep
+        return _abi.Cloud(_dp(xyz), _dp(mv), _dp(wall), _ip(b), _ip(bid), _ip(nnb), _ip(nbr),
+                          None if g is None else _dp(g), None if mac is None else _dp(mac))
 
     @property
     def xyz(self) -> np.ndarray:
@@ -266,16 +300,21 @@ class LatticeCase:
             self._xyz = self.build_on_device()["xyz"]
         return self._xyz
 
+    @xyz.setter
+    def xyz(self, value: np.ndarray):
+        self._xyz = value
+
     def build_on_device(self, device: int = 0) -> dict:
-        """The device-built arrays: xyz, wall, boundary, nnb, nbr."""
+        """The device-built arrays: xyz, wall, boundary, body_id, nnb, nbr."""
         lib = _abi.load()
         N = self.N
         out = dict(xyz=np.zeros((N, 3)), wall=np.zeros((N, 7)),
-                   boundary=np.zeros(N, np.int32), nnb=np.zeros(N, np.int32),
-                   nbr=np.zeros((N, _abi.MAX_NEIGH), np.int32))
-        _check(lib.alebgk_lattice_build_device(*self._args, int(device), _dp(out["xyz"]),
-                                               _dp(out["wall"]), _ip(out["boundary"]),
-                                               _ip(out["nnb"]), _ip(out["nbr"])))
+                   boundary=np.zeros(N, np.int32), body_id=np.zeros(N, np.int32),
+                   nnb=np.zeros(N, np.int32), nbr=np.zeros((N, _abi.MAX_NEIGH), np.int32))
+        _check(lib.alebgk_lattice_build_device_ex(*self._args, int(device), _dp(out["xyz"]),
+                                                  _dp(out["wall"]), _ip(out["boundary"]),
+                                                  _ip(out["body_id"]), _ip(out["nnb"]),
+                                                  _ip(out["nbr"])))
         self._xyz = out["xyz"]
         return out
 
@@ -308,8 +347,8 @@ class Solver:
 
     # -- reference-named API ------------------------------------------------
     def cudaUploadCloud(self, case: Case):
-        if isinstance(case, LatticeCase):
-            _check(self.lib.alebgk_upload_lattice(self.ctx, *case._args), self.ctx)
+        if isinstance(case, LatticeCase) and case.g is None:
+            _check(self.lib.alebgk_upload_lattice_ex(self.ctx, *case._args), self.ctx)
             return
         cl = case.cloud()
         _check(self.lib.alebgk_upload(self.ctx, ctypes.byref(cl), self.dt), self.ctx)

@@ -177,6 +177,27 @@ SIGNATURES = {
                                                    ctypes.c_double, ctypes.c_double,
                                                    ctypes.c_double, ctypes.c_int, c_double_p,
                                                    c_double_p, c_int_p, c_int_p, c_int_p]),
+    "alebgk_lattice_info_ex": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_double, ctypes.c_double,
+                                              ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                              c_int_p, c_double_p]),
+    "alebgk_lattice_bodies": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_double, c_int_p, c_double_p, c_int_p,
+                                             c_int_p, c_double_p]),
+    "alebgk_lattice_build_device_ex": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int,
+                                                      ctypes.c_int, ctypes.c_double,
+                                                      ctypes.c_int, ctypes.c_int,
+                                                      ctypes.c_double, ctypes.c_double,
+                                                      ctypes.c_double, ctypes.c_double,
+                                                      ctypes.c_int, c_double_p, c_double_p,
+                                                      c_int_p, c_int_p, c_int_p, c_int_p]),
+    "alebgk_upload_lattice_ex": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
+                                                ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                                ctypes.c_int, ctypes.c_double,
+                                                ctypes.c_double, ctypes.c_double,
+                                                ctypes.c_double]),
     "alebgk_upload_lattice": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
                                              ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                              ctypes.c_double, ctypes.c_double,

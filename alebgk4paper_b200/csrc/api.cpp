@@ -41,13 +41,29 @@ cudaError_t dalloc(P **p, size_t n)
     return cudaMalloc(reinterpret_cast<void **>(p), std::max<size_t>(n, 1) * sizeof(P));
 }
 
+// The row kernel visits the interior particles first, then the wall
+// particles (each in index order), so that the warps of an SM run the same
+// code at the same time: the wall rows' diffuse-wall code and the interior
+// rows' collision code then do not evict each other from the instruction
+// cache.  Rows are independent; the order changes no result.
+cudaError_t putRowOrder(alebgk_ctx *c, const int *boundary, int N)
+{
+    std::vector<int> order;
+    order.reserve(N);
+    for (int pass = 0; pass < 2; ++pass)
+        for (int i = 0; i < N; ++i)
+            if ((boundary[i] != 0) == (pass == 1)) order.push_back(i);
+    return cudaMemcpy(c->d.rowOrder, order.data(), 4 * (size_t)N, cudaMemcpyHostToDevice);
+}
+
 void freeBuffers(alebgk_ctx *c)
 {
     DeviceBuffers &d = c->d;
     void *ptrs[] = {d.f[0], d.f[1], d.coef, d.coefLin, d.pos, d.meshv, d.wall,
                     d.boundary, d.bodyId, d.cls, d.nslot, d.slots, d.macro[0],
                     d.macro[1], d.mood, d.flag, d.flagList, d.degList, d.massPos, d.massEnd, d.minG, d.nad, d.redPartial,
-                    d.dpx, d.bodyTmp, d.bodyOut, d.stage, d.surfList, d.bodyIO, d.rankAll, d.sc};
+                    d.dpx, d.bodyTmp, d.bodyOut, d.stage, d.surfList, d.bodyIO, d.rankAll, d.sc,
+                    d.rowOrder};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     d = DeviceBuffers();
@@ -321,6 +337,8 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
     CK(dalloc(&d.bodyOut, 64 * 6));
     CK(dalloc(&d.sc, 1));
     CK(dalloc(&d.stage, (size_t)N * p.gs));
+    CK(dalloc(&d.rowOrder, N));
+    CK(putRowOrder(c, cl->boundary, N));
     c->surfHost.clear();
     for (int i = 0; i < N; ++i)
         if (cl->boundary[i] && cl->body_id[i] >= 0) c->surfHost.push_back(i);
@@ -530,6 +548,7 @@ int refreshGeometryInPlace(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
     if (!c->surfHost.empty())
         CK(cudaMemcpy(d.surfList, c->surfHost.data(), 4 * c->surfHost.size(),
                       cudaMemcpyHostToDevice));
+    CK(putRowOrder(c, cl->boundary, N));
     CK(cudaStreamSynchronize(c->stream));
     // The step graphs hold the old slot stride and table pointers.
     for (auto &g : c->graph)
@@ -1147,18 +1166,15 @@ int alebgk_case_info(const alebgk_case *cs, int *info, double *prm)
 // The case parameters of a box cavity without bodies, as buildCloud sets
 // them, without building the cloud.
 static int latticeCase(const char *name, int Nx, int Nv, double dt, int mls_order,
-                       double lid_speed, double rho0, double tau, CaseParams &prm)
+                       int fixed_body, double lid_speed, double rho0, double tau,
+                       CaseParams &prm)
 {
     if (!name) return fail(nullptr, ALEBGK_EINVAL, "null argument");
     int id = 0;
     if (!caseByName(name, &id))
         return fail(nullptr, ALEBGK_EINVAL, std::string("unknown case ") + name);
-    if (!configureCase(id, Nx, Nv, dt, mls_order, false, prm))
+    if (!configureCase(id, Nx, Nv, dt, mls_order, fixed_body != 0, prm))
         return fail(nullptr, ALEBGK_EINVAL, "configureCase failed");
-    if (prm.hasBody)
-        return fail(nullptr, ALEBGK_EINVAL,
-                    std::string("case ") + name +
-                        " has rigid bodies; its set-up is host-only (alebgk_case_build_ex)");
     if (prm.Nx < 3 || prm.Nv < 2)
         return fail(nullptr, ALEBGK_EINVAL, "Nx must be >= 3 and Nv >= 2");
     if (lid_speed > 0) prm.lidSpeed = lid_speed;
@@ -1186,9 +1202,8 @@ struct LatticeBuffers
                         (void *)d.voxCursor, (void *)d.voxList, (void *)d.nnb, (void *)d.nbr})
             if (q) cudaFree(q);
     }
-    cudaError_t alloc(const CaseParams &p)
+    cudaError_t alloc(const CaseParams &p, size_t N)
     {
-        const size_t N = latticeN(p);
         const size_t nvox = (size_t)p.nbhBox * p.nbvBox * p.nbwBox;
         cudaError_t e = dalloc(&d.xyz, 3 * N);
         if (e == cudaSuccess) e = dalloc(&d.wall, 7 * N);
@@ -1229,16 +1244,123 @@ struct LatticeHost
     }
 };
 
+// The whole device set-up of a lattice case into b: the lattice, then (for
+// a case with bodies) the bodies embedded on the device, and the neighbour
+// lists.  *N = the particle count.
+cudaError_t deviceSetup(const CaseParams &p, double bodyScale, LatticeBuffers &b, size_t *N,
+                        cudaStream_t st)
+{
+    const size_t NL = latticeN(p);
+    if (!p.hasBody)
+    {
+        *N = NL;
+        cudaError_t e = b.alloc(p, NL);
+        return e == cudaSuccess ? buildLatticeDevice(p, b.d, st) : e;
+    }
+    std::vector<Body> bodies;
+    caseBodies(p, bodyScale, bodies);
+    std::vector<double> sx, sw;
+    std::vector<int> s0;
+    bodySurface(p, bodies, sx, sw, s0);
+    LatticeBuffers raw;
+    cudaError_t e = raw.alloc(p, NL);
+    if (e == cudaSuccess) e = buildLatticeDevice(p, raw.d, st, false);
+    if (e == cudaSuccess) e = b.alloc(p, NL + sx.size() / 3);
+    int n = 0;
+    if (e == cudaSuccess) e = embedLatticeDevice(p, bodies, sx, sw, s0, raw.d, (int)NL, b.d, &n, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    *N = (size_t)n;
+    return e;
+}
+
+// The body descriptor the host API uses (32 doubles, alebgk_case_bodies).
+void bodyState(const Body &r, double *o)
+{
+    double v[22] = {r.cx, r.cy, r.cz, r.velx, r.vely, r.velz, r.angularVel,
+                    r.omx, r.omy, r.omz, r.forcex, r.forcey, r.forcez,
+                    r.torque, r.tqx, r.tqy, r.tqz, r.ox, r.oy, r.mass,
+                    r.inertia(), r.T};
+    std::memcpy(o, v, sizeof v);
+    for (int k = 0; k < 9; ++k) o[22 + k] = r.Rm[k];
+    o[31] = r.surfaceArea();
+}
+
 }  // namespace
+
+int alebgk_lattice_info_ex(const char *name, int Nx, int Nv, double dt, int mls_order,
+                           int fixed_body, double body_scale, double lid_speed, double rho0,
+                           double tau, int device, int *info, double *prm)
+{
+    alebgk_ctx *c = nullptr;
+    CaseParams p;
+    int rc = latticeCase(name, Nx, Nv, dt, mls_order, fixed_body, lid_speed, rho0, tau, p);
+    if (rc) return rc;
+    const int gs = (p.dim == 3) ? p.Nv * p.Nv * p.Nv : 2 * p.Nv * p.Nv;
+    size_t N = latticeN(p);
+    int nb = 0;
+    if (p.hasBody)
+    {
+        // the count after the embedding is known once the device has run it
+        std::vector<Body> bodies;
+        caseBodies(p, body_scale, bodies);
+        nb = (int)bodies.size();
+        CK(cudaSetDevice(device));
+        LatticeBuffers b;
+        CK(deviceSetup(p, body_scale, b, &N, nullptr));
+    }
+    caseInfo(p, (int)N, gs, nb, info, prm);
+    return ALEBGK_OK;
+}
 
 int alebgk_lattice_info(const char *name, int Nx, int Nv, double dt, int mls_order,
                         double lid_speed, double rho0, double tau, int *info, double *prm)
 {
+    return alebgk_lattice_info_ex(name, Nx, Nv, dt, mls_order, 0, 1.0, lid_speed, rho0, tau, 0,
+                                  info, prm);
+}
+
+int alebgk_lattice_bodies(const char *name, int Nx, int Nv, double dt, int mls_order,
+                          int fixed_body, double body_scale, int *nbodies, double *state,
+                          int *kind, int *rotates, double *size)
+{
     CaseParams p;
-    int rc = latticeCase(name, Nx, Nv, dt, mls_order, lid_speed, rho0, tau, p);
+    int rc = latticeCase(name, Nx, Nv, dt, mls_order, fixed_body, -1.0, -1.0, -1.0, p);
     if (rc) return rc;
-    const int gs = (p.dim == 3) ? p.Nv * p.Nv * p.Nv : 2 * p.Nv * p.Nv;
-    caseInfo(p, (int)latticeN(p), gs, 0, info, prm);
+    std::vector<Body> bodies;
+    if (p.hasBody) caseBodies(p, body_scale, bodies);
+    if (nbodies) *nbodies = (int)bodies.size();
+    for (size_t b = 0; b < bodies.size(); ++b)
+    {
+        if (state) bodyState(bodies[b], state + 32 * b);
+        if (kind) kind[b] = bodies[b].kind;
+        if (rotates) rotates[b] = bodies[b].rotates ? 1 : 0;
+        if (size) size[b] = bodies[b].size;
+    }
+    return ALEBGK_OK;
+}
+
+int alebgk_lattice_build_device_ex(const char *name, int Nx, int Nv, double dt, int mls_order,
+                                   int fixed_body, double body_scale, double lid_speed,
+                                   double rho0, double tau, int device, double *xyz,
+                                   double *wall, int *boundary, int *body_id, int *nnb, int *nbr)
+{
+    alebgk_ctx *c = nullptr;
+    CaseParams p;
+    int rc = latticeCase(name, Nx, Nv, dt, mls_order, fixed_body, lid_speed, rho0, tau, p);
+    if (rc) return rc;
+    CK(cudaSetDevice(device));
+    LatticeBuffers b;
+    size_t N = 0;
+    CK(deviceSetup(p, body_scale, b, &N, nullptr));
+    CK(cudaDeviceSynchronize());
+    LatticeHost h;
+    CK(h.fetch(b.d, N));
+    if (xyz) std::memcpy(xyz, h.xyz.data(), 24 * N);
+    if (wall) std::memcpy(wall, h.wall.data(), 56 * N);
+    if (boundary) std::memcpy(boundary, h.boundary.data(), 4 * N);
+    if (body_id) std::memcpy(body_id, h.bodyId.data(), 4 * N);
+    if (nnb) std::memcpy(nnb, h.nnb.data(), 4 * N);
+    if (nbr) std::memcpy(nbr, h.nbr.data(), 4 * N * ALEBGK_MAX_NEIGH);
     return ALEBGK_OK;
 }
 
@@ -1246,24 +1368,8 @@ int alebgk_lattice_build_device(const char *name, int Nx, int Nv, double dt, int
                                 double lid_speed, double rho0, double tau, int device,
                                 double *xyz, double *wall, int *boundary, int *nnb, int *nbr)
 {
-    alebgk_ctx *c = nullptr;
-    CaseParams p;
-    int rc = latticeCase(name, Nx, Nv, dt, mls_order, lid_speed, rho0, tau, p);
-    if (rc) return rc;
-    CK(cudaSetDevice(device));
-    LatticeBuffers b;
-    CK(b.alloc(p));
-    CK(buildLatticeDevice(p, b.d, nullptr));
-    CK(cudaDeviceSynchronize());
-    const size_t N = latticeN(p);
-    LatticeHost h;
-    CK(h.fetch(b.d, N));
-    if (xyz) std::memcpy(xyz, h.xyz.data(), 24 * N);
-    if (wall) std::memcpy(wall, h.wall.data(), 56 * N);
-    if (boundary) std::memcpy(boundary, h.boundary.data(), 4 * N);
-    if (nnb) std::memcpy(nnb, h.nnb.data(), 4 * N);
-    if (nbr) std::memcpy(nbr, h.nbr.data(), 4 * N * ALEBGK_MAX_NEIGH);
-    return ALEBGK_OK;
+    return alebgk_lattice_build_device_ex(name, Nx, Nv, dt, mls_order, 0, 1.0, lid_speed, rho0,
+                                          tau, device, xyz, wall, boundary, nullptr, nnb, nbr);
 }
 
 int alebgk_neighbours_device(alebgk_ctx *c, const double *grid, const int *boxes, int *nnb,
@@ -1299,25 +1405,25 @@ int alebgk_neighbours_device(alebgk_ctx *c, const double *grid, const int *boxes
     return ALEBGK_OK;
 }
 
-int alebgk_upload_lattice(alebgk_ctx *c, const char *name, int Nx, int Nv, double dt,
-                          int mls_order, double lid_speed, double rho0, double tau)
+int alebgk_upload_lattice_ex(alebgk_ctx *c, const char *name, int Nx, int Nv, double dt,
+                             int mls_order, int fixed_body, double body_scale, double lid_speed,
+                             double rho0, double tau)
 {
     if (!c) return ALEBGK_EINVAL;
     CaseParams p;
-    int rc = latticeCase(name, Nx, Nv, dt, mls_order, lid_speed, rho0, tau, p);
+    int rc = latticeCase(name, Nx, Nv, dt, mls_order, fixed_body, lid_speed, rho0, tau, p);
     if (rc) return fail(c, rc, gCreateError);
     const StepParams &sp = c->sp;
-    const size_t N = latticeN(p);
+    CK(cudaSetDevice(c->cfg.device));
+    LatticeBuffers b;
+    size_t N = 0;
+    CK(deviceSetup(p, body_scale, b, &N, c->stream));
     if ((size_t)sp.N != N || sp.dim != p.dim || sp.Nv != p.Nv || sp.mlsOrder != p.mlsOrder ||
         sp.vmin != p.VMin || sp.dv != p.dv || sp.h != p.radius || sp.tau != p.tau ||
         sp.R != p.R)
         return fail(c, ALEBGK_EINVAL,
                     "the context's configuration does not match this lattice case "
                     "(N, dim, Nv, MLS order, velocity grid, radius, tau or R)");
-    CK(cudaSetDevice(c->cfg.device));
-    LatticeBuffers b;
-    CK(b.alloc(p));
-    CK(buildLatticeDevice(p, b.d, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     LatticeHost h;
     CK(h.fetch(b.d, N));
@@ -1339,6 +1445,13 @@ int alebgk_upload_lattice(alebgk_ctx *c, const char *name, int Nx, int Nv, doubl
     if (e != cudaSuccess)
         return fail(c, ALEBGK_ECUDA, std::string("lattice state: ") + cudaGetErrorString(e));
     return ALEBGK_OK;
+}
+
+int alebgk_upload_lattice(alebgk_ctx *c, const char *name, int Nx, int Nv, double dt,
+                          int mls_order, double lid_speed, double rho0, double tau)
+{
+    return alebgk_upload_lattice_ex(c, name, Nx, Nv, dt, mls_order, 0, 1.0, lid_speed, rho0,
+                                    tau);
 }
 
 int alebgk_case_view(alebgk_case *cs, alebgk_cloud *v)
@@ -1370,15 +1483,7 @@ int alebgk_case_bodies(const alebgk_case *cs, double *out)
     const Cloud &c = cs->cloud;
     for (size_t b = 0; b < c.bodies.size(); ++b)
     {
-        const Body &r = c.bodies[b];
-        double *o = out + 32 * b;
-        double v[22] = {r.cx, r.cy, r.cz, r.velx, r.vely, r.velz, r.angularVel,
-                        r.omx, r.omy, r.omz, r.forcex, r.forcey, r.forcez,
-                        r.torque, r.tqx, r.tqy, r.tqz, r.ox, r.oy, r.mass,
-                        r.inertia(), r.T};
-        std::memcpy(o, v, sizeof v);
-        for (int k = 0; k < 9; ++k) o[22 + k] = r.Rm[k];
-        o[31] = r.surfaceArea();
+        bodyState(c.bodies[b], out + 32 * b);
     }
     return ALEBGK_OK;
 }

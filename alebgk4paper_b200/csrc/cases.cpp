@@ -449,6 +449,36 @@ static void makeBodies(Cloud &c, double bodyScale)
     c.bodies.push_back(b);
 }
 
+void caseBodies(const CaseParams &p, double bodyScale, std::vector<Body> &bodies)
+{
+    Cloud c;
+    c.prm = p;
+    makeBodies(c, bodyScale > 0 ? bodyScale : 1.0);
+    bodies = c.bodies;
+}
+
+void bodySurface(const CaseParams &p, const std::vector<Body> &bodies,
+                 std::vector<double> &xyz, std::vector<double> &wall, std::vector<int> &start)
+{
+    const int ndim = p.dim;
+    xyz.clear(); wall.clear(); start.assign(1, 0);
+    for (const Body &B : bodies)
+    {
+        std::vector<double> s;
+        B.surfacePoints(s);
+        for (size_t q = 0; q + 2 < s.size(); q += 3)
+        {
+            const double px = s[q], py = s[q + 1], pz = (ndim == 3) ? s[q + 2] : 0.0;
+            double nx, ny, nz;
+            B.normal(px, py, (ndim == 3) ? pz : B.cz, &nx, &ny, &nz);
+            if (ndim != 3) nz = 0.0;
+            xyz.insert(xyz.end(), {px, py, pz});
+            wall.insert(wall.end(), {nx, ny, nz, B.velx, B.vely, B.velz, B.T});
+        }
+        start.push_back((int)(xyz.size() / 3));
+    }
+}
+
 // Initialization/BodyEmbedding.cpp:18-104
 static void embedBodies(Cloud &c)
 {

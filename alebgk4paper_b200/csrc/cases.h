@@ -93,6 +93,15 @@ bool configureCase(int caseId, int Nx, int Nv, double dt, int mlsOrder,
 bool buildCloud(const CaseParams &prmIn, double bodyScale, Cloud &c,
                 std::string *err);
 
+// The bodies of a configured case (TestCases/TestCases.cpp:251-294), and
+// the surface particles embedBodies appends for them
+// (Initialization/BodyEmbedding.cpp:66-96): positions (3 per point), wall
+// state (7 per point: n, U_w, T_w), and per body the first point
+// (start[b] .. start[b + 1]).
+void caseBodies(const CaseParams &p, double bodyScale, std::vector<Body> &bodies);
+void bodySurface(const CaseParams &p, const std::vector<Body> &bodies,
+                 std::vector<double> &xyz, std::vector<double> &wall, std::vector<int> &start);
+
 // Lattice spacings, support radius and voxel boxes of a configured case
 // (the scalar part of Initialization/ParticleGeneration.cpp:30-200).
 void latticeParams(CaseParams &p);

@@ -71,6 +71,8 @@ struct DeviceBuffers
     double *bodyOut = nullptr;         // up to 64 bodies x 6
     double *stage = nullptr;           // N x gs FP64 host-transfer staging
     int *surfList = nullptr;           // body-surface particles (boundary, bodyId >= 0)
+    int *rowOrder = nullptr;           // the row kernel's visiting order: interior
+                                       // particles, then wall particles
     double *bodyIO = nullptr;          // body-step staging: kBodyIOHead + 13 per surface particle
     double *rankAll = nullptr;         // multi-process slab: every rank's 4 combine words
     int rankAllCap = 0;                // ranks rankAll holds
@@ -209,7 +211,10 @@ struct LatticeDev
     int *voxStart = nullptr, *voxCursor = nullptr, *voxList = nullptr;
     int *nnb = nullptr, *nbr = nullptr;
 };
-cudaError_t buildLatticeDevice(const CaseParams &p, const LatticeDev &o, cudaStream_t st);
+// The lattice of a box cavity (positions, flags, wall state), and unless
+// neighbours is false its voxel bins and neighbour lists.
+cudaError_t buildLatticeDevice(const CaseParams &p, const LatticeDev &o, cudaStream_t st,
+                               bool neighbours = true);
 // Voxel grid of the neighbour search: origin, box sizes, box counts, radius.
 struct NeighbourGrid
 {
@@ -220,6 +225,16 @@ struct NeighbourGrid
 cudaError_t buildNeighboursDevice(const NeighbourGrid &g, const double *xyz, int N,
                                   const LatticeDev &o, cudaStream_t st);
 cudaError_t launchRestState(alebgk_ctx *c, const double *rowDev, double rho, double T0);
+struct Body;
+// Body embedding of a lattice set-up on the device (setup.cu): raw holds
+// the whole lattice (NL particles, from buildLatticeDevice); out receives the
+// kept lattice particles in order, then the surface particles, and (when
+// out.nnb is set) the neighbour lists of the result; *nOut is its count.
+cudaError_t embedLatticeDevice(const CaseParams &p, const std::vector<Body> &bodies,
+                               const std::vector<double> &surfXyz,
+                               const std::vector<double> &surfWall,
+                               const std::vector<int> &surfStart, const LatticeDev &raw, int NL,
+                               const LatticeDev &out, int *nOut, cudaStream_t st);
 struct CoeffInput;
 struct CoeffTables;
 // MLS tables of the classes `cls` built on the device (coeffs_dev.cu).

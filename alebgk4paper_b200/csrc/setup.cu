@@ -16,8 +16,10 @@
 // reference does, with the same 128-neighbour cap.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <string>
+#include <vector>
 
 #include "cases.h"
 #include "ctx.h"
@@ -238,9 +240,219 @@ __global__ void k_rest_state(const double *__restrict__ row, int gs, int ldf, in
     }
 }
 
+// ---------------------------------------------------------------------------
+// Body embedding (Initialization/BodyEmbedding.cpp:18-104): drop the lattice
+// particles inside a body or within 0.4 dx of one of its surface points,
+// keep the rest in order, append the surface particles.  The surface points
+// and their wall state come from the host (bodySurface in cases.cpp, the
+// same records the host set-up appends).
+// ---------------------------------------------------------------------------
+struct EmbedBody
+{
+    int kind, s0, s1;   // surface points [s0, s1)
+    double cx, cy, cz, size, ox, oy;
+    double Rm[9];
+};
+
+// Body::inside of cases.cpp (RigidBody/Geometry.hpp) with the host's
+// operations: explicit fma where the host writes one, separately rounded
+// products and sums elsewhere.
+__device__ bool insideBody(const EmbedBody &b, double x, double y, double z)
+{
+    switch (b.kind)
+    {
+    case 0:
+    {
+        const double xC = __dsub_rn(x, b.cx), yC = __dsub_rn(y, b.cy);
+        const double D = __dadd_rn(__dmul_rn(b.ox, b.ox), __dmul_rn(b.oy, b.oy));
+        const double xp = __dadd_rn(__dmul_rn(b.ox, xC), __dmul_rn(b.oy, yC)) / D;
+        const double yp = __dsub_rn(__dmul_rn(b.oy, xC), __dmul_rn(b.ox, yC)) / D;
+        return fabs(xp) <= b.size / 2 && fabs(yp) <= b.size / 2;
+    }
+    case 1:
+    {
+        const double dx = __dsub_rn(x, b.cx), dy = __dsub_rn(y, b.cy);
+        return fma(dx, dx, __dmul_rn(dy, dy)) <= __dmul_rn(b.size, b.size);
+    }
+    case 2:
+    {
+        const double dx = __dsub_rn(x, b.cx), dy = __dsub_rn(y, b.cy), dz = __dsub_rn(z, b.cz);
+        return fma(dz, dz, fma(dx, dx, __dmul_rn(dy, dy))) <= __dmul_rn(b.size, b.size);
+    }
+    default:
+    {
+        const double dx = __dsub_rn(x, b.cx), dy = __dsub_rn(y, b.cy), dz = __dsub_rn(z, b.cz);
+        const double bx = fma(b.Rm[6], dz, fma(b.Rm[0], dx, __dmul_rn(b.Rm[3], dy)));
+        const double by = fma(b.Rm[7], dz, fma(b.Rm[1], dx, __dmul_rn(b.Rm[4], dy)));
+        const double bz = fma(b.Rm[8], dz, fma(b.Rm[2], dx, __dmul_rn(b.Rm[5], dy)));
+        const double h = b.size / 2;
+        return fabs(bx) <= h && fabs(by) <= h && fabs(bz) <= h;
+    }
+    }
+}
+
+__global__ void k_embed_mark(const double *__restrict__ xyz, int N, int dim,
+                             const EmbedBody *__restrict__ bodies, int nb,
+                             const double *__restrict__ surf, double hug2, int *__restrict__ keep)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double x = xyz[3 * (size_t)i], y = xyz[3 * (size_t)i + 1], z = xyz[3 * (size_t)i + 2];
+    bool drop = false;
+    for (int b = 0; b < nb && !drop; ++b)
+    {
+        const EmbedBody &B = bodies[b];
+        if (insideBody(B, x, y, dim == 3 ? z : B.cz)) { drop = true; break; }
+        for (int q = B.s0; q < B.s1; ++q)
+        {
+            const double dx = __dsub_rn(x, surf[3 * q]), dy = __dsub_rn(y, surf[3 * q + 1]);
+            double d2 = fma(dx, dx, __dmul_rn(dy, dy));
+            if (dim == 3)
+            {
+                const double dz = __dsub_rn(z, surf[3 * q + 2]);
+                d2 = fma(dz, dz, d2);
+            }
+            if (d2 < hug2) { drop = true; break; }
+        }
+    }
+    keep[i] = drop ? 0 : 1;
+}
+
+// Exclusive scan of keep[0..n) in one 1024-thread block; *count = the total.
+__global__ void __launch_bounds__(1024)
+k_embed_scan(const int *__restrict__ keep, int n, int *__restrict__ pos, int *count)
+{
+    __shared__ int part[1024];
+    const int t = threadIdx.x, per = (n + 1023) / 1024;
+    const int lo = min(n, t * per), hi = min(n, lo + per);
+    int sum = 0;
+    for (int i = lo; i < hi; ++i) sum += keep[i];
+    part[t] = sum;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1)
+    {
+        const int v = (t >= off) ? part[t - off] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    int run = (t > 0) ? part[t - 1] : 0;
+    for (int i = lo; i < hi; ++i)
+    {
+        pos[i] = run;
+        run += keep[i];
+    }
+    if (t == 1023) *count = part[1023];
+}
+
+__global__ void k_embed_scatter(LatticeDev in, const int *__restrict__ keep,
+                                const int *__restrict__ pos, int N, LatticeDev out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N || !keep[i]) return;
+    const size_t j = pos[i];
+    for (int q = 0; q < 3; ++q)
+    {
+        out.xyz[3 * j + q] = in.xyz[3 * (size_t)i + q];
+        out.meshv[3 * j + q] = in.meshv[3 * (size_t)i + q];
+    }
+    for (int q = 0; q < 7; ++q) out.wall[7 * j + q] = in.wall[7 * (size_t)i + q];
+    out.boundary[j] = in.boundary[i];
+    out.bodyId[j] = in.bodyId[i];
+}
+
+__global__ void k_embed_append(const double *__restrict__ surf, const double *__restrict__ wall,
+                               const int *__restrict__ body, int nsurf,
+                               const int *__restrict__ kept, LatticeDev out)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nsurf) return;
+    const size_t j = (size_t)*kept + q;
+    for (int k = 0; k < 3; ++k)
+    {
+        out.xyz[3 * j + k] = surf[3 * (size_t)q + k];
+        out.meshv[3 * j + k] = 0.0;
+    }
+    for (int k = 0; k < 7; ++k) out.wall[7 * j + k] = wall[7 * (size_t)q + k];
+    out.boundary[j] = 1;
+    out.bodyId[j] = body[q];
+}
+
 }  // namespace
 
-cudaError_t buildLatticeDevice(const CaseParams &p, const LatticeDev &o, cudaStream_t st)
+cudaError_t embedLatticeDevice(const CaseParams &p, const std::vector<Body> &bodies,
+                               const std::vector<double> &surfXyz,
+                               const std::vector<double> &surfWall,
+                               const std::vector<int> &surfStart, const LatticeDev &raw, int NL,
+                               const LatticeDev &out, int *nOut, cudaStream_t st)
+{
+    const int nb = (int)bodies.size(), nsurf = (int)(surfXyz.size() / 3);
+    std::vector<EmbedBody> eb(nb);
+    std::vector<int> bodyOf(nsurf);
+    for (int b = 0; b < nb; ++b)
+    {
+        const Body &B = bodies[b];
+        EmbedBody &e = eb[b];
+        e.kind = B.kind; e.s0 = surfStart[b]; e.s1 = surfStart[b + 1];
+        e.cx = B.cx; e.cy = B.cy; e.cz = B.cz; e.size = B.size; e.ox = B.ox; e.oy = B.oy;
+        for (int k = 0; k < 9; ++k) e.Rm[k] = B.Rm[k];
+        for (int q = e.s0; q < e.s1; ++q) bodyOf[q] = b;
+    }
+    EmbedBody *dB = nullptr;
+    double *dSurf = nullptr, *dWall = nullptr;
+    int *dBody = nullptr, *keep = nullptr, *pos = nullptr, *count = nullptr;
+    const size_t nsa = std::max(nsurf, 1);
+    cudaError_t e = cudaMalloc(&dB, sizeof(EmbedBody) * std::max(nb, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&dSurf, 24 * nsa);
+    if (e == cudaSuccess) e = cudaMalloc(&dWall, 56 * nsa);
+    if (e == cudaSuccess) e = cudaMalloc(&dBody, 4 * nsa);
+    if (e == cudaSuccess) e = cudaMalloc(&keep, 4 * (size_t)NL);
+    if (e == cudaSuccess) e = cudaMalloc(&pos, 4 * (size_t)NL);
+    if (e == cudaSuccess) e = cudaMalloc(&count, 4);
+    if (e == cudaSuccess && nb)
+        e = cudaMemcpyAsync(dB, eb.data(), sizeof(EmbedBody) * nb, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && nsurf)
+        e = cudaMemcpyAsync(dSurf, surfXyz.data(), 24 * (size_t)nsurf, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && nsurf)
+        e = cudaMemcpyAsync(dWall, surfWall.data(), 56 * (size_t)nsurf, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && nsurf)
+        e = cudaMemcpyAsync(dBody, bodyOf.data(), 4 * (size_t)nsurf, cudaMemcpyHostToDevice, st);
+    const double hug = 0.4 * std::fabs(p.dx);
+    const double hug2 = std::pow(hug, 2);
+    int kept = 0;
+    if (e == cudaSuccess)
+    {
+        k_embed_mark<<<(NL + 127) / 128, 128, 0, st>>>(raw.xyz, NL, p.dim, dB, nb, dSurf, hug2,
+                                                       keep);
+        k_embed_scan<<<1, 1024, 0, st>>>(keep, NL, pos, count);
+        k_embed_scatter<<<(NL + 255) / 256, 256, 0, st>>>(raw, keep, pos, NL, out);
+        if (nsurf)
+            k_embed_append<<<(nsurf + 127) / 128, 128, 0, st>>>(dSurf, dWall, dBody, nsurf,
+                                                                count, out);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&kept, count, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    const int N = kept + nsurf;
+    if (e == cudaSuccess && out.nnb)
+    {
+        NeighbourGrid g;
+        g.dim = p.dim;
+        g.x0 = p.xleft; g.y0 = p.ybottom; g.z0 = p.zfront;
+        g.hx = p.hBox; g.hy = p.vBox; g.hz = p.wBox;
+        g.nx = p.nbhBox; g.ny = p.nbvBox; g.nz = p.nbwBox;
+        g.radius = p.radius;
+        e = buildNeighboursDevice(g, out.xyz, N, out, st);
+    }
+    for (void *q : {(void *)dB, (void *)dSurf, (void *)dWall, (void *)dBody, (void *)keep,
+                    (void *)pos, (void *)count})
+        if (q) cudaFree(q);
+    if (nOut) *nOut = N;
+    return e;
+}
+
+cudaError_t buildLatticeDevice(const CaseParams &p, const LatticeDev &o, cudaStream_t st,
+                               bool neighbours)
 {
     LatticeArgs a{};
     a.dim = p.dim; a.Nx = p.Nx; a.Ny = p.Ny; a.Nz = (p.dim == 3) ? p.Nz : 1;
@@ -264,6 +476,7 @@ cudaError_t buildLatticeDevice(const CaseParams &p, const LatticeDev &o, cudaStr
     if (e != cudaSuccess) return e;
     k_lattice<<<nb, 256, 0, st>>>(a, o.xyz, o.boundary, o.bodyId, o.wall, o.meshv, o.voxel,
                                   o.voxCount);
+    if (!neighbours) return cudaGetLastError();
     k_voxel_scan<<<1, 32, 0, st>>>(o.voxCount, nvox, o.voxStart, o.voxCursor);
     k_voxel_fill<<<nb, 256, 0, st>>>(o.voxel, a.N, o.voxCursor, o.voxList);
     k_voxel_sort<<<(nvox + 127) / 128, 128, 0, st>>>(o.voxStart, nvox, o.voxList);

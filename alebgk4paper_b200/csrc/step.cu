@@ -334,6 +334,7 @@ struct ParticleArgs
     const double *nad;        // NAD neighbour density range (lo, hi) per particle
     int *flag, *flagList, *degList;
     StepScalars *sc;
+    const int *rowOrder;      // visiting order of the row kernel
 };
 
 // A particle row staged in shared memory for the passes of one warp: loaded
@@ -1163,8 +1164,9 @@ k_particle_rows(ParticleArgs<float> a, StepParams p)
     const double myV = lane < 3 * NV ? velD[myNode] : 0.0;
     const double dvN = p.dvN, c1 = p.c1;
     const int W = gridDim.x * (blockDim.x >> 5);
-    for (int i = blockIdx.x * (blockDim.x >> 5) + warp; i < p.N; i += W)
+    for (int t = blockIdx.x * (blockDim.x >> 5) + warp; t < p.N; t += W)
     {
+        const int i = a.rowOrder[t];
         float *row = a.g + (size_t)i * p.ldf;
         float x[LPL][NV];
         loadRowLines<NV>(row, lane, x);
@@ -2109,6 +2111,7 @@ static cudaError_t stepT(alebgk_ctx *c, int from, cudaEvent_t *ev)
     pa.g = fb; pa.fold = fa; pa.coefLin = static_cast<const T *>(d.coefLin);
     pa.coef = static_cast<const T *>(d.coef);
     pa.boundary = d.boundary; pa.cls = d.cls; pa.nslot = d.nslot; pa.slots = d.slots;
+    pa.rowOrder = d.rowOrder;
     pa.wall = d.wall; pa.macPrev = macA; pa.macNew = macB;
     pa.massPos = d.massPos; pa.massEnd = d.massEnd; pa.minG = d.minG; pa.dpx = d.dpx;
     pa.flag = d.flag; pa.flagList = d.flagList; pa.degList = d.degList; pa.sc = d.sc;
@@ -2761,6 +2764,7 @@ static cudaError_t buildBatchT(alebgk_ctx *const *cs, int n, double *const *resi
             pa.coefLin = static_cast<const T *>(d.coefLin);
             pa.coef = static_cast<const T *>(d.coef);
             pa.boundary = d.boundary; pa.cls = d.cls; pa.nslot = d.nslot; pa.slots = d.slots;
+            pa.rowOrder = d.rowOrder;
             pa.wall = d.wall; pa.macPrev = d.macro[from]; pa.macNew = d.macro[1 - from];
             pa.massPos = d.massPos; pa.massEnd = d.massEnd; pa.minG = d.minG; pa.dpx = d.dpx;
             pa.flag = d.flag; pa.flagList = d.flagList; pa.degList = d.degList; pa.sc = d.sc;
@@ -2953,6 +2957,7 @@ static cudaError_t slabSegT(alebgk_ctx *c, int from, int seg, cudaStream_t st)
     pa.g = fb; pa.fold = fa; pa.coefLin = static_cast<const T *>(d.coefLin);
     pa.coef = static_cast<const T *>(d.coef);
     pa.boundary = d.boundary; pa.cls = d.cls; pa.nslot = d.nslot; pa.slots = d.slots;
+    pa.rowOrder = d.rowOrder;
     pa.wall = d.wall; pa.macPrev = macA; pa.macNew = macB;
     pa.massPos = d.massPos; pa.massEnd = d.massEnd; pa.minG = d.minG; pa.dpx = d.dpx;
     pa.flag = d.flag; pa.flagList = d.flagList; pa.degList = d.degList; pa.sc = d.sc;

@@ -70,7 +70,7 @@ def train(X, T, steps: int = 20000, batch: int = 16384, lr: float = 2e-3,
     return net
 
 
-def _run(specs, net=None, tol: float = 1e-6, check_every: int = 100, max_steps: int = 60000,
+def _run(specs, net=None, tol: float = 5e-7, check_every: int = 200, max_steps: int = 60000,
          residual: str = "lid"):
     """Runs the cases to steady, cold or seeded; returns (steps per case,
     seconds until all are steady incl. seeding, 13-moment rows per case).
@@ -113,7 +113,7 @@ def _reference(specs, steps: int):
     return moms
 
 
-def evaluate(net, specs, tol: float = 1e-6, check_every: int = 100, max_steps: int = 60000,
+def evaluate(net, specs, tol: float = 5e-7, check_every: int = 200, max_steps: int = 60000,
              reference_steps: int = 8000, residual: str = "lid"):
     """Cold start against warm start on the same cases; both steady states
     are also compared with the fields after a long cold run."""

@@ -648,27 +648,51 @@ int alebgk_case_bodies(const alebgk_case *c, double *out);
 int alebgk_case_body_shapes(const alebgk_case *c, int *kind, int *rotates, double *size);
 
 /* ---- lattice set-up on the device -------------------------------------------
- * Box cavities without bodies (cavity2d, cavity3d and their overrides) can be
- * set up on the GPU instead of by alebgk_case_build_ex on the host: the
- * lattice (Initialization/ParticleGeneration.cpp:30-200), the wall state
- * (Core/MLSBasis.hpp:228-287, TestCases/TestCases.cpp:230-249), the voxel
- * bins and neighbour lists (Initialization/NeighbourSearch.cpp:17-99) and the
- * rest-state Maxwellian (Initialization/InitialConditions.cpp:18-80), each
- * bitwise equal to the host set-up.  The stencil classes and transport
- * coefficients are still built on the host from the device's neighbour lists.
+ * The reference's cases can be set up on the GPU instead of by
+ * alebgk_case_build_ex on the host: the lattice
+ * (Initialization/ParticleGeneration.cpp:30-200), the wall state
+ * (Core/MLSBasis.hpp:228-287, TestCases/TestCases.cpp:230-249), the rigid
+ * bodies embedded (Initialization/BodyEmbedding.cpp:18-104: lattice particles
+ * inside a body or within 0.4 dx of its surface dropped, in order, the
+ * surface particles appended), the voxel bins and neighbour lists
+ * (Initialization/NeighbourSearch.cpp:17-99) and the rest-state Maxwellian
+ * (Initialization/InitialConditions.cpp:18-80), each bitwise equal to the
+ * host set-up.  The host computes only the bodies' surface points (a few
+ * hundred records).  The stencil classes and transport coefficients are
+ * built as alebgk_upload builds them.
  *
- * alebgk_lattice_info: info/prm as alebgk_case_info, without building a cloud
- * (cases with bodies are rejected). */
+ * alebgk_lattice_info_ex: info/prm as alebgk_case_info, without a host cloud.
+ * For a case with bodies the particle count after the embedding comes from
+ * the device set-up, run on `device`.  fixed_body and body_scale as in
+ * alebgk_case_build (the --fixed flag and the body size factor). */
+int alebgk_lattice_info_ex(const char *name, int Nx, int Nv, double dt, int mls_order,
+                           int fixed_body, double body_scale, double lid_speed, double rho0,
+                           double tau, int device, int *info, double *prm);
+/* The bodies of a lattice case (host only): count, state (32 doubles per
+ * body, the layout of alebgk_case_bodies), kind, rotates, size (any may be
+ * NULL). */
+int alebgk_lattice_bodies(const char *name, int Nx, int Nv, double dt, int mls_order,
+                          int fixed_body, double body_scale, int *nbodies, double *state,
+                          int *kind, int *rotates, double *size);
+/* The device-built arrays, copied to host buffers (any may be NULL): xyz N*3,
+ * wall N*7, boundary N, body_id N, nnb N, nbr N*ALEBGK_MAX_NEIGH (-1 padded). */
+int alebgk_lattice_build_device_ex(const char *name, int Nx, int Nv, double dt, int mls_order,
+                                   int fixed_body, double body_scale, double lid_speed,
+                                   double rho0, double tau, int device, double *xyz,
+                                   double *wall, int *boundary, int *body_id, int *nnb,
+                                   int *nbr);
+/* alebgk_upload for a lattice case set up on the device: the context (made
+ * from the alebgk_lattice_info_ex configuration) gets the same state that
+ * alebgk_upload of the host-built case gives it. */
+int alebgk_upload_lattice_ex(alebgk_ctx *ctx, const char *name, int Nx, int Nv, double dt,
+                             int mls_order, int fixed_body, double body_scale, double lid_speed,
+                             double rho0, double tau);
+/* The same without bodies' options (fixed_body 0, body_scale 1, device 0). */
 int alebgk_lattice_info(const char *name, int Nx, int Nv, double dt, int mls_order,
                         double lid_speed, double rho0, double tau, int *info, double *prm);
-/* The device-built arrays, copied to host buffers (any may be NULL): xyz N*3,
- * wall N*7, boundary N, nnb N, nbr N*ALEBGK_MAX_NEIGH (-1 padded). */
 int alebgk_lattice_build_device(const char *name, int Nx, int Nv, double dt, int mls_order,
                                 double lid_speed, double rho0, double tau, int device,
                                 double *xyz, double *wall, int *boundary, int *nnb, int *nbr);
-/* alebgk_upload for a lattice case set up on the device: the context (made
- * from the alebgk_lattice_info configuration) gets the same state that
- * alebgk_upload of the host-built case gives it. */
 int alebgk_upload_lattice(alebgk_ctx *ctx, const char *name, int Nx, int Nv, double dt,
                           int mls_order, double lid_speed, double rho0, double tau);
 

@@ -399,6 +399,17 @@ void ref_manage(void *h, int *counts)
     counts[2] = added;
 }
 
+// Test hook: resizes the particle array to n (new particles default-built),
+// so that ckpt::restore, which requires the file's particle count, can load
+// the restart file of a moving-body run whose count has changed since the
+// set-up.  The restore then overwrites every particle.
+void ref_resize(void *h, int n)
+{
+    auto *c = static_cast<RefCase *>(h);
+    c->P.resize((size_t)n, Particle(c->sp.Nv, c->cp.dim));
+    c->cp.N = n;
+}
+
 // The reference's own restart files (Core/Checkpoint.hpp): save the case's
 // state, restore into it, and the record sizes of the format.
 int ref_checkpoint_save(void *h, const char *path)

@@ -81,13 +81,32 @@ def test_setup_matches_compiled_reference(case, Nx, Nv):
     np.testing.assert_allclose(c.g, r.g(), rtol=1e-14, atol=0)
 
 
-def test_lattice_case_matches_host_parameters_and_rejects_bodies():
-    """The device set-up's case parameters are the host set-up's; cases with
-    rigid bodies keep the host set-up."""
-    from alebgk4paper_b200 import AlebgkError, Case, LatticeCase
+def test_lattice_case_matches_host_parameters_and_bodies():
+    """The device set-up's case parameters are the host set-up's, and so are
+    the bodies it embeds (state, kind, rotation flag, size); the particle
+    count of a case with bodies needs the device (tests/test_gpu_setup.py)."""
+    import ctypes
+    from alebgk4paper_b200 import Case, LatticeCase, _abi
     for name, kw in (("cavity2d", dict(Nx=24, Nv=16, lid_speed=3.0, rho0=2.0, tau=1.8e-10)),
                      ("cavity3d", dict(Nx=13, Nv=8))):
         lc, c = LatticeCase(name, **kw), Case(name, **kw)
         assert lc.params == c.params and lc.N == c.N and lc.gstride == c.gstride
-    with pytest.raises(AlebgkError, match="rigid bodies"):
-        LatticeCase("cavity2d-square", Nx=12, Nv=8)
+        assert lc.nbodies == 0
+    lib = _abi.load()
+    for name, fixed, scale in (("cavity2d-square", 0, 1.0), ("cavity2d-circle", 1, 1.0),
+                               ("cavity3d-sphere", 0, 0.8), ("cavity3d-cube", 1, 1.0)):
+        c = Case(name, 12, 4, -1.0, 2, fixed_body=bool(fixed), body_scale=scale)
+        n = ctypes.c_int()
+        st, kind = np.zeros(32), np.zeros(1, np.int32)
+        rot, size = np.zeros(1, np.int32), np.zeros(1)
+        assert lib.alebgk_lattice_bodies(name.encode(), 12, 4, -1.0, 2, fixed, scale,
+                                         ctypes.byref(n), st.ctypes.data_as(
+                                             ctypes.POINTER(ctypes.c_double)),
+                                         kind.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                         rot.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                         size.ctypes.data_as(
+                                             ctypes.POINTER(ctypes.c_double))) == 0
+        assert n.value == c.nbodies == 1
+        np.testing.assert_array_equal(st, c.bodies[0])
+        assert (kind[0], rot[0], size[0]) == (c.body_kind[0], c.body_rotates[0],
+                                              c.body_size[0])

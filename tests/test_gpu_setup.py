@@ -55,6 +55,67 @@ def test_device_setup_steps_like_host_setup(name, kw, precision):
     b.cudaFreeCloud()
 
 
+BODY_CASES = [("cavity2d-square", dict(Nx=24, Nv=8)), ("cavity2d-circle", dict(Nx=20, Nv=8)),
+              ("cavity3d-sphere", dict(Nx=12, Nv=4)), ("cavity3d-cube", dict(Nx=12, Nv=4)),
+              ("cavity3d-cube", dict(Nx=40, Nv=4, body_scale=1.3)),
+              ("cavity2d-circle", dict(Nx=60, Nv=8, fixed_body=True))]
+
+
+@pytest.mark.parametrize("name,kw", BODY_CASES)
+def test_device_body_embedding_equals_host_setup(name, kw):
+    """The bodies embedded on the device (BodyEmbedding.cpp:18-104): the
+    same particles in the same order -- lattice particles inside a body or
+    within 0.4 dx of its surface dropped, the surface particles appended --
+    with the same wall state, body ids and neighbour lists as the host."""
+    _need_gpu()
+    host = Case(name, **kw)
+    lc = LatticeCase(name, **kw)
+    assert lc.N == host.N and lc.nbodies == host.nbodies == 1
+    np.testing.assert_array_equal(lc.bodies, host.bodies)
+    dev = lc.build_on_device()
+    for k in ("xyz", "wall", "boundary", "body_id", "nnb", "nbr"):
+        assert np.array_equal(dev[k], getattr(host, k)), k
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+@pytest.mark.parametrize("name,kw", [BODY_CASES[0], BODY_CASES[3]])
+def test_device_body_setup_steps_like_host_setup(name, kw, precision):
+    """A body case set up on the device steps bitwise like the host-built
+    one, the body loads included."""
+    _need_gpu()
+    a = Solver(Case(name, **kw), precision=precision)
+    b = Solver(LatticeCase(name, **kw), precision=precision)
+    a.cudaStep(3)
+    b.cudaStep(3)
+    ga, ma = a.cudaDownloadFull()
+    gb, mb = b.cudaDownloadFull()
+    assert np.array_equal(ga, gb) and np.array_equal(ma, mb)
+    c = a.case
+    centres = c.bodies[:, 0:3].copy()
+    areas = c.bodies[:, 31].copy()
+    assert np.array_equal(a.body_loads(centres, areas), b.body_loads(centres, areas))
+    a.cudaFreeCloud()
+    b.cudaFreeCloud()
+
+
+def test_moving_body_run_from_device_setup(gpu):
+    """A free cube set up on the device, stepped with its body step and
+    cloud management, follows the host-built run bitwise."""
+    runs = []
+    for case in (Case("cavity3d-cube", 12, 4, -1.0, 2), LatticeCase("cavity3d-cube", 12, 4, -1.0, 2)):
+        s = Solver(case, precision=64)
+        st = case.bodies.copy()
+        for _ in range(6):
+            s.cudaStep(1)
+            st = s.body_step(st)
+            case.bodies = st
+            s.refresh_geometry()
+        runs.append((st.copy(), s.cudaDownloadFull()[0]))
+        s.close()
+    np.testing.assert_array_equal(runs[0][0], runs[1][0])
+    np.testing.assert_array_equal(runs[0][1], runs[1][1])
+
+
 def test_batch_with_device_setup_matches_host_setup():
     _need_gpu()
     from alebgk4paper_b200.batch import BatchSolver, batched_cavity2d
