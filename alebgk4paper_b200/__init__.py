@@ -216,13 +216,15 @@ class Case:
         return cfg
 
     def cloud(self) -> _abi.Cloud:
-        """A C-ABI view of this case's arrays (kept alive by this object)."""
-        self._keep = [np.ascontiguousarray(a) for a in
+        """A C-ABI view of this case's arrays (kept alive by this object); g
+        is NULL once a particle-set change kept the distribution on the
+        device (``Solver.refresh_geometry``)."""
+        self._keep = [None if a is None else np.ascontiguousarray(a) for a in
                       (self.xyz, self.meshv, self.wall, self.boundary, self.body_id,
                        self.nnb, self.nbr, self.g, self.macro)]
         xyz, mv, wall, b, bid, nnb, nbr, g, mac = self._keep
         return _abi.Cloud(_dp(xyz), _dp(mv), _dp(wall), _ip(b), _ip(bid), _ip(nnb),
-                          _ip(nbr), _dp(g), _dp(mac))
+                          _ip(nbr), None if g is None else _dp(g), _dp(mac))
 
 
 class LatticeCase:
@@ -347,7 +349,8 @@ class Solver:
 
     # -- reference-named API ------------------------------------------------
     def cudaUploadCloud(self, case: Case):
-        if isinstance(case, LatticeCase) and case.g is None:
+        if isinstance(case, LatticeCase) and case.g is None and \
+                not getattr(case, "_managed", False):
             _check(self.lib.alebgk_upload_lattice_ex(self.ctx, *case._args), self.ctx)
             return
         cl = case.cloud()
@@ -467,7 +470,8 @@ class Solver:
                                                  _ip(nbr)), self.ctx)
         return nnb, nbr
 
-    def refresh_geometry(self, bodies: np.ndarray | None = None, manage: bool = True):
+    def refresh_geometry(self, bodies: np.ndarray | None = None, manage: bool = True,
+                         device_state: bool = True):
         """Uploads the cloud again after :meth:`body_step` moved the surface:
         positions, mesh velocities and wall state as the device holds them.
         With ``manage`` (and bodies in the case) the reference's cloud
@@ -478,8 +482,13 @@ class Solver:
         device.  While the particle set stays the same (the usual step) the
         distribution never leaves the device (``alebgk_upload_geometry``);
         when it changes, the state is read back, managed and uploaded, and
-        the context is rebuilt for the new particle count.  Returns the cloud
-        management counts (removed, merged, added)."""
+        the context is rebuilt for the new particle count: with
+        ``device_state`` the distribution never leaves the device then either
+        (the management returns a row plan, ``alebgk_rows_build`` builds the
+        new rows from the old context and ``alebgk_upload_rows`` installs them
+        after a geometry-only upload); without it the state is read back,
+        managed on the host and uploaded.  Both give bitwise the same state.
+        Returns the cloud management counts (removed, merged, added)."""
         from .cloud import manage_cloud
         c = self.case
         xyz, mv, wall = self.download_geometry()
@@ -489,6 +498,8 @@ class Solver:
             st = c.bodies if bodies is None else bodies
             geo = dict(xyz=xyz, meshv=mv, wall=wall, boundary=c.boundary, body_id=c.body_id)
             out, counts, need = manage_cloud(c, geo, st, self.cfg.device, decide_only=True)
+            if need and device_state:
+                return self._refresh_device_state(c, geo, st)
             if need:
                 g, macro = self.cudaDownloadFull()
                 geo.update(g=g, macro=macro)
@@ -510,6 +521,45 @@ class Solver:
             c.nnb, c.nbr = self.rebuild_neighbours()
         cl = c.cloud()
         _check(self.lib.alebgk_upload_geometry(self.ctx, ctypes.byref(cl), self.dt), self.ctx)
+        return counts
+
+    def _refresh_device_state(self, c, geo, st):
+        """The particle-set change of :meth:`refresh_geometry` with the
+        distribution kept on the device."""
+        from .cloud import manage_cloud
+        geo.update(macro=self.cudaDownloadMoments())
+        out, counts, _ = manage_cloud(c, geo, st, self.cfg.device, plan=True)
+        a, b, fresh = out["plan"]
+        fresh = np.ascontiguousarray(fresh, np.float64)
+        rows = ctypes.c_void_p()
+        _check(self.lib.alebgk_rows_build(self.ctx, len(a), _ip(a), _ip(b), len(fresh),
+                                          _dp(fresh) if len(fresh) else None,
+                                          ctypes.byref(rows)), self.ctx)
+        try:
+            c.xyz, c.meshv, c.wall = out["xyz"], out["meshv"], out["wall"]
+            c.boundary, c.body_id = out["boundary"], out["body_id"]
+            c.nnb, c.nbr, c.macro = out["nnb"], out["nbr"], out["macro"]
+            c.g = None
+            c._managed = True
+            if len(c.xyz) != self.N:
+                c.N = self.N = len(c.xyz)
+                self.lib.alebgk_destroy(self.ctx)
+                self.cfg.N = self.N
+                h = ctypes.c_void_p()
+                _check(self.lib.alebgk_create(ctypes.byref(self.cfg), ctypes.byref(h)))
+                self.ctx = h
+            keep = [np.ascontiguousarray(x) for x in (c.xyz, c.meshv, c.wall, c.boundary,
+                                                        c.body_id, c.nnb, c.nbr)]
+            xyz, mv, wall, bd, bid, nnb, nbr = keep
+            cl = _abi.Cloud(_dp(xyz), _dp(mv), _dp(wall), _ip(bd), _ip(bid), _ip(nnb), _ip(nbr),
+                            None, None)
+            _check(self.lib.alebgk_upload(self.ctx, ctypes.byref(cl), self.dt), self.ctx)
+            mac = np.ascontiguousarray(c.macro, np.float64)
+            r, rows = rows, None
+            _check(self.lib.alebgk_upload_rows(self.ctx, r, _dp(mac)), self.ctx)
+        finally:
+            if rows is not None and rows.value:
+                self.lib.alebgk_rows_free(rows)
         return counts
 
     def write_vtk(self, outdir: str, step: int, time: float):

@@ -117,6 +117,12 @@ SIGNATURES = {
                                        ctypes.POINTER(ctypes.c_float)]),
     "alebgk_residual": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
     "alebgk_residual_interval": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "alebgk_managed_plan": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p, c_double_p]),
+    "alebgk_rows_build": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_int_p, c_int_p,
+                                         ctypes.c_int, c_double_p,
+                                         ctypes.POINTER(ctypes.c_void_p)]),
+    "alebgk_upload_rows": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, c_double_p]),
+    "alebgk_rows_free": (None, [ctypes.c_void_p]),
     "alebgk_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                            ctypes.POINTER(ctypes.c_void_p)]),
     "alebgk_batch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

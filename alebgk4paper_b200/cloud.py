@@ -30,14 +30,17 @@ def _params(case):
 
 
 def manage_cloud(case, cloud: dict, bodies_state: np.ndarray, device: int = 0,
-                 decide_only: bool = False):
+                 decide_only: bool = False, plan: bool = False):
     """Runs the cloud management on a host cloud (dict with xyz, meshv, wall,
     boundary, body_id, g, macro) whose bodies are at ``bodies_state``
     (nbodies x 32, the layout of ``Case.bodies``).  Returns (managed cloud
     dict with nnb and nbr, (removed, merged, added), need_state).  With
     ``decide_only`` g and macro are not passed: the call stops with
     need_state True as soon as the particle set would change, and otherwise
-    returns the unchanged cloud with rebuilt neighbour lists."""
+    returns the unchanged cloud with rebuilt neighbour lists.  With ``plan``
+    the cloud carries macro but no g: the distribution stays with the caller
+    (on the device) and the result's "plan" is (a, b, fresh), the origin of
+    every row (``alebgk_managed_plan``)."""
     lib = _abi.load()
     prm, iprm = _params(case)
     st = np.ascontiguousarray(bodies_state, np.float64).reshape(-1, 32)
@@ -52,7 +55,7 @@ def manage_cloud(case, cloud: dict, bodies_state: np.ndarray, device: int = 0,
     names = [("xyz", np.float64), ("meshv", np.float64), ("wall", np.float64),
              ("boundary", np.int32), ("body_id", np.int32)]
     if not decide_only:
-        names += [("g", np.float64), ("macro", np.float64)]
+        names += ([] if plan else [("g", np.float64)]) + [("macro", np.float64)]
     keep = {k: np.ascontiguousarray(cloud[k], dt) for k, dt in names}
     N = keep["xyz"].shape[0]
     gs = int(case.gstride)
@@ -60,7 +63,7 @@ def manage_cloud(case, cloud: dict, bodies_state: np.ndarray, device: int = 0,
     none = ctypes.POINTER(ctypes.c_double)()
     cl = _abi.Cloud(_dp(keep["xyz"]), _dp(keep["meshv"]), _dp(keep["wall"]),
                     _ip(keep["boundary"]), _ip(keep["body_id"]), _ip(dummy), _ip(dummy),
-                    none if decide_only else _dp(keep["g"]),
+                    none if decide_only or plan else _dp(keep["g"]),
                     none if decide_only else _dp(keep["macro"]))
     h = ctypes.c_void_p()
     _check(lib.alebgk_manage_cloud(int(device), _dp(prm), _ip(iprm), nb, arr, N, gs,
@@ -85,8 +88,13 @@ def manage_cloud(case, cloud: dict, bodies_state: np.ndarray, device: int = 0,
                    body_id=take(view.body_id, n, np.int32, (n,)),
                    nnb=take(view.nnb, n, np.int32, (n,)),
                    nbr=take(view.nbr, n * _abi.MAX_NEIGH, np.int32, (n, _abi.MAX_NEIGH)),
-                   g=None if decide_only else take(view.g, n * gs, np.float64, (n, gs)),
+                   g=None if decide_only or plan else take(view.g, n * gs, np.float64, (n, gs)),
                    macro=None if decide_only else take(view.macro, 7 * n, np.float64, (n, 7)))
+        if plan:
+            a, b = np.zeros(n, np.int32), np.zeros(n, np.int32)
+            fresh = np.zeros((max(1, counts[2]), gs))
+            _check(lib.alebgk_managed_plan(h, _ip(a), _ip(b), _dp(fresh)))
+            out["plan"] = (a, b, fresh[: counts[2]])
         return out, counts, False
     finally:
         lib.alebgk_managed_free(h)

@@ -428,7 +428,8 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
 
 int alebgk_upload(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
 {
-    return uploadCloud(c, cl, dt, true);
+    // without g and macros: the geometry only (the state follows separately)
+    return uploadCloud(c, cl, dt, !(cl && !cl->g && !cl->macro));
 }
 
 int alebgk_set_coeff_builder(int which)
@@ -650,6 +651,88 @@ int alebgk_upload_state(alebgk_ctx *c, const double *g, const double *macro)
     if (e != cudaSuccess)
         return fail(c, ALEBGK_ECUDA, std::string("state upload: ") + cudaGetErrorString(e));
     return ALEBGK_OK;
+}
+
+struct alebgk_rows
+{
+    int device = 0, n = 0, gs = 0;
+    double *rows = nullptr;
+};
+
+int alebgk_rows_build(alebgk_ctx *c, int n, const int *a, const int *b, int nfresh,
+                      const double *fresh, alebgk_rows **out)
+{
+    if (!c || !a || !b || !out || n < 1 || nfresh < 0 || (nfresh > 0 && !fresh))
+        return fail(c, ALEBGK_EINVAL, "null argument");
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    *out = nullptr;
+    const int N = c->sp.N, gs = c->sp.gs;
+    for (int j = 0; j < n; ++j)
+        if (a[j] >= N || (a[j] < 0 && -1 - a[j] >= nfresh) || b[j] < -1 || b[j] >= N ||
+            (a[j] < 0 && b[j] >= 0))
+            return fail(c, ALEBGK_EINVAL, "row plan entry out of range");
+    CK(cudaSetDevice(c->cfg.device));
+    auto *r = new (std::nothrow) alebgk_rows();
+    if (!r) return fail(c, ALEBGK_ENOMEM, "host allocation failed");
+    r->device = c->cfg.device; r->n = n; r->gs = gs;
+    int *da = nullptr, *db = nullptr;
+    double *df = nullptr;
+    cudaError_t e = cudaMalloc(&r->rows, 8 * (size_t)n * gs);
+    if (e == cudaSuccess) e = cudaMalloc(&da, 4 * (size_t)n);
+    if (e == cudaSuccess) e = cudaMalloc(&db, 4 * (size_t)n);
+    if (e == cudaSuccess) e = cudaMalloc(&df, 8 * (size_t)std::max(nfresh, 1) * gs);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(da, a, 4 * (size_t)n, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(db, b, 4 * (size_t)n, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && nfresh)
+        e = cudaMemcpyAsync(df, fresh, 8 * (size_t)nfresh * gs, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = launchRowsBuild(c, n, da, db, df, r->rows);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    for (void *q : {(void *)da, (void *)db, (void *)df})
+        if (q) cudaFree(q);
+    if (e != cudaSuccess)
+    {
+        alebgk_rows_free(r);
+        return fail(c, ALEBGK_ECUDA, std::string("rows build: ") + cudaGetErrorString(e));
+    }
+    *out = r;
+    return ALEBGK_OK;
+}
+
+int alebgk_upload_rows(alebgk_ctx *c, alebgk_rows *r, const double *macro)
+{
+    if (!c || !r || !macro) return fail(c, ALEBGK_EINVAL, "null argument");
+    if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
+    if (r->n != c->sp.N || r->gs != c->sp.gs || r->device != c->cfg.device)
+        return fail(c, ALEBGK_EINVAL, "the rows do not fit this context (N, gstride or device)");
+    CK(cudaSetDevice(c->cfg.device));
+    const int N = c->sp.N;
+    std::vector<double> mac(6 * (size_t)N);
+    std::vector<int> mood(N);
+    for (int i = 0; i < N; ++i)
+    {
+        for (int q = 0; q < 6; ++q) mac[6 * (size_t)i + q] = macro[7 * (size_t)i + q];
+        mood[i] = macro[7 * (size_t)i + 6] != 0.0;
+    }
+    CK(cudaMemcpy(c->d.macro[c->cur], mac.data(), mac.size() * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d.mood, mood.data(), 4 * (size_t)N, cudaMemcpyHostToDevice));
+    cudaError_t e = launchConvertIn(c, r->rows, c->cur);
+    if (e == cudaSuccess) e = launchMassInit(c);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    alebgk_rows_free(r);
+    if (e != cudaSuccess)
+        return fail(c, ALEBGK_ECUDA, std::string("rows upload: ") + cudaGetErrorString(e));
+    return ALEBGK_OK;
+}
+
+void alebgk_rows_free(alebgk_rows *r)
+{
+    if (!r) return;
+    if (r->rows)
+    {
+        cudaSetDevice(r->device);
+        cudaFree(r->rows);
+    }
+    delete r;
 }
 
 int alebgk_moments13(alebgk_ctx *c, double *out)

@@ -128,6 +128,15 @@ struct Cloud2
     int N = 0, gs = 0;
     std::vector<double> xyz, meshv, wall, g, macro;
     std::vector<int> boundary, bodyId, nnb, nbr;
+    // Plan mode (the distribution stays on the device): the origin of every
+    // row instead of the row.  originA >= 0: the input row originA (and, when
+    // originB >= 0, the mean of the input rows originA and originB, a merge);
+    // originA < 0: row -1 - originA of fresh (a refill Maxwellian, gsFresh
+    // values each).
+    bool plan = false;
+    int gsFresh = 0;
+    std::vector<int> originA, originB;
+    std::vector<double> fresh;
 
     void keep(const std::vector<char> &k)
     {
@@ -144,6 +153,11 @@ struct Cloud2
                 std::copy_n(&macro[7 * (size_t)i], 7, &macro[7 * (size_t)n]);
                 boundary[n] = boundary[i];
                 bodyId[n] = bodyId[i];
+                if (plan)
+                {
+                    originA[n] = originA[i];
+                    originB[n] = originB[i];
+                }
             }
             ++n;
         }
@@ -151,6 +165,7 @@ struct Cloud2
         xyz.resize(3 * (size_t)N); meshv.resize(3 * (size_t)N); wall.resize(7 * (size_t)N);
         g.resize((size_t)gs * N); macro.resize(7 * (size_t)N);
         boundary.resize(N); bodyId.resize(N);
+        if (plan) { originA.resize(N); originB.resize(N); }
     }
 };
 
@@ -194,14 +209,24 @@ cudaError_t manageCloud(const ManageParams &mp, const std::vector<Body> &bodies,
     Cloud2 &c = out.c;
     // Without g and macros the run only decides: it stops with needState as
     // soon as the particle set would change.
-    const bool haveState = in.g && in.macro;
-    c.N = N; c.gs = haveState ? gs : 0;
+    // Plan mode: macros without g -- the run decides as with the state and
+    // records where every row of the result comes from.
+    c.plan = !in.g && in.macro;
+    const bool haveState = (in.g && in.macro) || c.plan;
+    c.N = N; c.gs = (in.g && in.macro) ? gs : 0;
+    c.gsFresh = gs;
+    if (c.plan)
+    {
+        c.originA.resize(N);
+        c.originB.assign(N, -1);
+        for (int i = 0; i < N; ++i) c.originA[i] = i;
+    }
     c.xyz.assign(in.xyz, in.xyz + 3 * (size_t)N);
     c.meshv.assign(in.meshv, in.meshv + 3 * (size_t)N);
     c.wall.assign(in.wall, in.wall + 7 * (size_t)N);
     if (haveState)
     {
-        c.g.assign(in.g, in.g + (size_t)gs * N);
+        if (c.gs) c.g.assign(in.g, in.g + (size_t)gs * N);
         c.macro.assign(in.macro, in.macro + 7 * (size_t)N);
     }
     else
@@ -362,9 +387,14 @@ cudaError_t manageCloud(const ManageParams &mp, const std::vector<Body> &bodies,
                         pi[0] = 0.5 * (pi[0] + pj[0]);
                         pi[1] = 0.5 * (pi[1] + pj[1]);
                         if (d3) pi[2] = 0.5 * (pi[2] + pj[2]);
-                        double *gi = &c.g[(size_t)gs * i];
-                        const double *gj = &c.g[(size_t)gs * j];
-                        for (int k = 0; k < gs; ++k) gi[k] = 0.5 * (gi[k] + gj[k]);
+                        if (c.plan)
+                            c.originB[i] = c.originA[j];
+                        else
+                        {
+                            double *gi = &c.g[(size_t)gs * i];
+                            const double *gj = &c.g[(size_t)gs * j];
+                            for (int k = 0; k < gs; ++k) gi[k] = 0.5 * (gi[k] + gj[k]);
+                        }
                         dead[j] = 1;
                         ++merged;
                         break;
@@ -498,9 +528,15 @@ cudaError_t manageCloud(const ManageParams &mp, const std::vector<Body> &bodies,
                 c.boundary.push_back(0);
                 c.bodyId.push_back(-1);
                 c.macro.insert(c.macro.end(), {rho, ux, uy, d3 ? uz : 0.0, T, p, 0.0});
-                const size_t base = c.g.size();
-                c.g.resize(base + gs);
-                double *row = &c.g[base];
+                std::vector<double> &rows = c.plan ? c.fresh : c.g;
+                if (c.plan)
+                {
+                    c.originA.push_back(-1 - (int)(c.fresh.size() / gs));
+                    c.originB.push_back(-1);
+                }
+                const size_t base = rows.size();
+                rows.resize(base + gs);
+                double *row = &rows[base];
                 if (d3)
                 {
                     for (int kv = 0; kv < mp.Nv; ++kv)
@@ -567,8 +603,9 @@ int alebgk_manage_cloud(int device, const double *prm, const int *iprm, int nbod
     if (!prm || !iprm || !cloud || !out || N <= 0 || gstride <= 0 || nbodies < 0 ||
         (nbodies > 0 && !bodies))
         return ALEBGK_EINVAL;
+    // g without macros is the one combination without a meaning
     if (!cloud->xyz || !cloud->meshv || !cloud->wall || !cloud->boundary || !cloud->body_id ||
-        (!cloud->g) != (!cloud->macro))
+        (cloud->g && !cloud->macro))
         return ALEBGK_EINVAL;
     *out = nullptr;
     ManageParams mp;
@@ -630,5 +667,16 @@ int alebgk_managed_cloud(alebgk_managed *m, alebgk_cloud *view)
 }
 
 void alebgk_managed_free(alebgk_managed *m) { delete m; }
+
+int alebgk_managed_plan(const alebgk_managed *m, int *a, int *b, double *fresh)
+{
+    if (!m) return ALEBGK_EINVAL;
+    const Cloud2 &c = m->m.c;
+    if (!c.plan) return ALEBGK_ESTATE;
+    if (a) std::copy(c.originA.begin(), c.originA.end(), a);
+    if (b) std::copy(c.originB.begin(), c.originB.end(), b);
+    if (fresh) std::copy(c.fresh.begin(), c.fresh.end(), fresh);
+    return ALEBGK_OK;
+}
 
 }  // extern "C"

@@ -225,6 +225,9 @@ struct NeighbourGrid
 cudaError_t buildNeighboursDevice(const NeighbourGrid &g, const double *xyz, int N,
                                   const LatticeDev &o, cudaStream_t st);
 cudaError_t launchRestState(alebgk_ctx *c, const double *rowDev, double rho, double T0);
+// The distribution of a managed cloud from a row plan (step.cu k_rows_build).
+cudaError_t launchRowsBuild(alebgk_ctx *c, int n, const int *a, const int *b,
+                            const double *fresh, double *out);
 struct Body;
 // Body embedding of a lattice set-up on the device (setup.cu): raw holds
 // the whole lattice (NL particles, from buildLatticeDevice); out receives the

@@ -1996,6 +1996,38 @@ __global__ void k_convert_in(const double *src, T *dst, int N, int gs, int ldf)
     }
 }
 
+// The distribution of a managed cloud from the current one (the row plan of
+// the cloud management): what k_convert_out, the host management and
+// k_convert_in give, without the round trip.  A kept row is the stored row
+// at true scale; a merged row the mean of two such rows, rounded as the
+// host rounds it (products kept separate from the sum); a refill row comes
+// from the host.
+template <typename T>
+__global__ void k_rows_build(const T *__restrict__ src, int ldf, int gs, int n,
+                             const int *__restrict__ a, const int *__restrict__ b,
+                             const double *__restrict__ fresh,
+                             const StepScalars *__restrict__ sc, double *__restrict__ out)
+{
+    const double scale = sc->scale;
+    const size_t tot = (size_t)n * gs;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < tot;
+         idx += (size_t)gridDim.x * blockDim.x)
+    {
+        const size_t j = idx / gs, k = idx % gs;
+        const int ia = a[j];
+        double v;
+        if (ia >= 0)
+        {
+            const double va = __dmul_rn((double)src[(size_t)ia * ldf + k], scale);
+            const int ib = b[j];
+            v = (ib >= 0) ? 0.5 * (va + __dmul_rn((double)src[(size_t)ib * ldf + k], scale)) : va;
+        }
+        else
+            v = fresh[(size_t)(-1 - ia) * gs + k];
+        out[idx] = v;
+    }
+}
+
 template <typename T>
 __global__ void k_convert_out(const T *src, double *dst, int N, int gs, int ldf,
                               const StepScalars *__restrict__ sc)
@@ -3112,6 +3144,21 @@ cudaError_t launchConvertIn(alebgk_ctx *c, const double *src, int buf)
     else
         k_convert_in<float><<<1184, 256, 0, c->stream>>>(
             src, static_cast<float *>(c->d.f[buf]), p.N, p.gs, p.ldf);
+    return cudaGetLastError();
+}
+
+cudaError_t launchRowsBuild(alebgk_ctx *c, int n, const int *a, const int *b,
+                            const double *fresh, double *out)
+{
+    const StepParams &p = c->sp;
+    if (c->cfg.precision == 64)
+        k_rows_build<double><<<1184, 256, 0, c->stream>>>(
+            static_cast<const double *>(c->d.f[c->cur]), p.ldf, p.gs, n, a, b, fresh, c->d.sc,
+            out);
+    else
+        k_rows_build<float><<<1184, 256, 0, c->stream>>>(
+            static_cast<const float *>(c->d.f[c->cur]), p.ldf, p.gs, n, a, b, fresh, c->d.sc,
+            out);
     return cudaGetLastError();
 }
 

@@ -134,7 +134,9 @@ int alebgk_last_error(const alebgk_ctx *ctx, char *buf, size_t len);
  * classes and coefficient tables for the given dt.
  * Replaces cudaUploadCloud (Solver/Solver.cpp:68,
  * Solver/CudaBackend.cu:1223-1381); dt is the step the tables are built for
- * (the reference passes it to every cudaStep instead). */
+ * (the reference passes it to every cudaStep instead).  With cloud->g and
+ * cloud->macro both NULL only the geometry is uploaded; the state follows by
+ * alebgk_upload_state or alebgk_upload_rows. */
 int alebgk_upload(alebgk_ctx *ctx, const alebgk_cloud *cloud, double dt);
 
 /* Replaces only the distribution and macro fields (same geometry), e.g. a
@@ -444,7 +446,14 @@ int alebgk_neighbours_device(alebgk_ctx *ctx, const double *grid, const int *box
  * needState.  With cloud->g and cloud->macro NULL the call only decides: it
  * stops with needState = 1 as soon as the particle set would change (then
  * call again with the state), and otherwise returns the same cloud with
- * rebuilt neighbour lists. */
+ * rebuilt neighbour lists.  With cloud->macro set and cloud->g NULL (plan
+ * mode) it manages the cloud as with the state but keeps no distribution:
+ * alebgk_managed_plan gives, per row of the result, its origin in the input
+ * (a[j] >= 0: input row a[j], or the mean of input rows a[j] and b[j] when
+ * b[j] >= 0, as mergeCloseParticles forms it) or, for a[j] < 0, row
+ * -1 - a[j] of `fresh` (the refill Maxwellians, `added` rows of gstride
+ * FP64 values).  alebgk_rows_build then builds the distribution on the
+ * device. */
 typedef struct alebgk_managed alebgk_managed;
 int alebgk_manage_cloud(int device, const double *prm, const int *iprm, int nbodies,
                         const alebgk_body *bodies, int N, int gstride,
@@ -452,6 +461,23 @@ int alebgk_manage_cloud(int device, const double *prm, const int *iprm, int nbod
 int alebgk_managed_info(const alebgk_managed *m, int *info);
 int alebgk_managed_cloud(alebgk_managed *m, alebgk_cloud *view);
 void alebgk_managed_free(alebgk_managed *m);
+int alebgk_managed_plan(const alebgk_managed *m, int *a, int *b, double *fresh);
+
+/* The distribution of a managed cloud, built on the device from ctx's
+ * current one by a plan of alebgk_managed_plan (n rows, nfresh fresh rows):
+ * every value is what alebgk_download_full, the host management and
+ * alebgk_upload give it, computed without the host round trip.  The rows
+ * (FP64, device memory) live in *out until alebgk_upload_rows or
+ * alebgk_rows_free; ctx may be destroyed in between. */
+typedef struct alebgk_rows alebgk_rows;
+int alebgk_rows_build(alebgk_ctx *ctx, int n, const int *a, const int *b, int nfresh,
+                      const double *fresh, alebgk_rows **out);
+/* Installs rows as the distribution of ctx, whose cloud was uploaded without
+ * a state (alebgk_upload with cloud->g and cloud->macro NULL uploads the
+ * geometry only), with the host macros (N*7) as alebgk_upload_state takes
+ * them; frees the rows. */
+int alebgk_upload_rows(alebgk_ctx *ctx, alebgk_rows *rows, const double *macro);
+void alebgk_rows_free(alebgk_rows *rows);
 
 /* ---- slab mode ---------------------------------------------------------------
  * One cavity split into slabs along its outermost lattice axis, one context

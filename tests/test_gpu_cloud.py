@@ -102,6 +102,20 @@ def test_merge_of_close_particles_equals_reference():
     assert counts == tuple(cnt) and counts[1] >= 1
     for k in ("xyz", "boundary", "body_id", "nnb", "nbr", "g"):
         assert np.array_equal(got[k], want[k]), k
+    # The same management in plan mode (no distribution passed): the row
+    # plan applied to the input rows gives the managed distribution bitwise.
+    geo = {k: v for k, v in before.items() if k != "g"}
+    pl, pcounts, _ = manage_cloud(Case(name, Nx=Nx, Nv=Nv), geo, bodies, plan=True)
+    assert pcounts == counts and pl["g"] is None
+    pa, pb, fresh = pl["plan"]
+    g0 = before["g"]
+    rows = np.where((pb >= 0)[:, None], 0.5 * (g0[pa] + g0[np.maximum(pb, 0)]), g0[pa])
+    if len(fresh):
+        rows[pa < 0] = fresh[-1 - pa[pa < 0]]
+    assert (pb >= 0).sum() == counts[1]
+    np.testing.assert_array_equal(rows, got["g"])
+    for k in ("xyz", "boundary", "body_id", "nnb", "nbr", "macro"):
+        assert np.array_equal(pl[k], got[k]), k
 
 
 @pytest.mark.parametrize("name,Nx,Nv,v", [("cavity2d-square", 24, 6, (900.0, 300.0, 0.0)),
@@ -141,3 +155,43 @@ def test_fast_body_run_manages_the_cloud_like_the_reference(name, Nx, Nv, v):
     g_ref = r.g()
     assert np.abs(g_ours - g_ref).max() <= 1e-9 * np.abs(g_ref).max()
     s.close()
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+@pytest.mark.parametrize("name,Nx,Nv,v", [("cavity2d-square", 24, 6, (900.0, 300.0, 0.0)),
+                                          ("cavity3d-cube", 12, 4, (700.0, 0.0, 400.0))])
+def test_particle_set_changes_keep_the_state_on_the_device(name, Nx, Nv, v, precision):
+    """The fast-body run with its removals, merges and refills, once with the
+    distribution kept on the device across every particle-set change (the
+    management's row plan, ``alebgk_rows_build``) and once through the host
+    (download, host management, upload): the same particle counts and
+    bitwise the same body history, distribution and macros at every step."""
+    _need()
+    from alebgk4paper_b200 import Solver
+    runs = []
+    for device_state in (True, False):
+        c = Case(name, Nx=Nx, Nv=Nv)
+        st = c.bodies.copy()
+        st[0, 3:6] = v
+        c.bodies = st
+        s = Solver(c, precision=precision)
+        hist = []
+        changed = [0, 0, 0]
+        for _ in range(8):
+            s.cudaStep(1)
+            st = s.body_step(st)
+            c.bodies = st
+            counts = s.refresh_geometry(device_state=device_state)
+            changed = [x + y for x, y in zip(changed, counts)]
+            g, m = s.cudaDownloadFull()
+            hist.append((c.N, st.copy(), g, m))
+        runs.append((hist, changed))
+        s.close()
+    (ha, ca), (hb, cb) = runs
+    print("removed, merged, added over the run:", ca)
+    assert ca == cb and sum(ca) > 0, (ca, cb)
+    for (na, sa, ga, ma), (nb, sb, gb, mb) in zip(ha, hb):
+        assert na == nb
+        np.testing.assert_array_equal(sa, sb)
+        np.testing.assert_array_equal(ga, gb)
+        np.testing.assert_array_equal(ma, mb)
