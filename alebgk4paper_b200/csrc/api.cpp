@@ -487,6 +487,12 @@ int refreshGeometryInPlace(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
     std::string err;
     DeviceBuffers &d = c->d;
     const size_t es = f64 ? 8 : 4;
+    // What the captured step graphs hold: the step parameters (by value) and
+    // the buffers the refresh may reallocate.  When none of them changes,
+    // the graphs stay valid and are kept.
+    unsigned char spBefore[sizeof(StepParams)];
+    std::memcpy(spBefore, &p, sizeof p);
+    const void *bufBefore[] = {d.coef, d.coefLin, d.slots, d.surfList, d.bodyIO};
     // Geometry first: the class keys are computed from the device copy.
     CK(cudaMemcpy(d.pos, cl->xyz, 24 * (size_t)N, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d.meshv, cl->meshv, 24 * (size_t)N, cudaMemcpyHostToDevice));
@@ -551,9 +557,14 @@ int refreshGeometryInPlace(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
                       cudaMemcpyHostToDevice));
     CK(putRowOrder(c, cl->boundary, N));
     CK(cudaStreamSynchronize(c->stream));
-    // The step graphs hold the old slot stride and table pointers.
-    for (auto &g : c->graph)
-        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    // The step graphs hold the slot stride and the table pointers: rebuilt
+    // when either changed.
+    const void *bufAfter[] = {d.coef, d.coefLin, d.slots, d.surfList, d.bodyIO};
+    bool same = std::memcmp(spBefore, &p, sizeof p) == 0;
+    for (int k = 0; k < 5 && same; ++k) same = bufBefore[k] == bufAfter[k];
+    if (!same)
+        for (auto &g : c->graph)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     if (c->macSnap) { cudaFree(c->macSnap); c->macSnap = nullptr; }
     c->snapSteps = -1;
     c->bodyIdHost.assign(cl->body_id, cl->body_id + N);
