@@ -5,14 +5,14 @@ MLS, the case's default dt, stepped by the reference's own CPU code
 (``oracle/_ref``, compiled unmodified by ``oracle/Makefile``) through
 ``oracle/ref_driver.cpp`` with the reference's step order
 (Solver/Solver.cpp:632-705).  The full distribution is 512 MB, so the
-fixture keeps, at steps 1 and 10:
+fixture keeps, at steps 1, 10 and 50:
 
 * the moment fields rho, ux, uy, uz, T of every particle,
 * the row sums sum_k g and sum_k |g| of every particle,
 * 256 seeded full rows of g (walls, corners and interior alike),
 
 plus the transport-flag and moodCheck counts and the total mass of every
-step.  About ten minutes on eight cores::
+step.  About fifteen minutes on eight cores::
 
     make -C oracle ref && python tests/golden/make_golden_c3d40.py
 """
@@ -29,8 +29,9 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from oracle.oracle import RefCase  # noqa: E402
 
-CHECKPOINTS = (1, 10)
+CHECKPOINTS = (1, 10, 50)
 NROWS = 256
+FIXTURE = "step_c3d_n40_v10_q_s1_s10_s50.npz"
 SEED = 40
 
 
@@ -55,8 +56,8 @@ def main():
             del g
     out["flags"] = np.array(flags)
     out["mass"] = np.array(mass)
-    np.savez_compressed(os.path.join(HERE, "step_c3d_n40_v10_q_s1_s10.npz"), **out)
-    print("written", os.path.join(HERE, "step_c3d_n40_v10_q_s1_s10.npz"))
+    np.savez_compressed(os.path.join(HERE, FIXTURE), **out)
+    print("written", os.path.join(HERE, FIXTURE))
 
 
 if __name__ == "__main__":
