@@ -60,6 +60,9 @@ def parse():
                     choices=["auto", "stages", "branches", "persistent"],
                     help="batched-cavity2d graph form: autotuned, stage groups (4), one "
                          "persistent launch per step, or per-cavity branches")
+    ap.add_argument("--screen-floor-run", action="store_true",
+                    help="free-body: a fourth run, FP64 with the FP32 MOOD screen's rounding "
+                         "floor, to separate the screen's decisions from FP32 arithmetic")
     ap.add_argument("--no-steady", action="store_true",
                     help="batched-cavity2d: skip the run to the steady residual")
     ap.add_argument("--ncu", action="store_true",
@@ -647,7 +650,10 @@ def run_free_body(args):
     # third run measures how far the body's path moves under a perturbation
     # of the size of FP32 rounding alone, against which the FP32 run's
     # deviation from FP64 is read.
-    for tag, prec, rounded in ((32, 32, False), (64, 64, False), ("64r", 64, True)):
+    plan = [(32, 32, False), (64, 64, False), ("64r", 64, True)]
+    if args.screen_floor_run:
+        plan.append(("64f", 64, False))
+    for tag, prec, rounded in plan:
         c = ab.Case("cavity3d-cube", 40, 10, -1.0, 2, fixed_body=False)
         if rounded:
             c.g[:] = c.g.astype(np.float32).astype(np.float64)
@@ -659,6 +665,9 @@ def run_free_body(args):
         rho_range, nonfinite = [], None
         with ClockSampler(local) as clk:
             for k in range(args.warmup + args.steps):
+                if tag == "64f":
+                    # the FP32 screen's floor (a rebuilt context starts without it)
+                    s.set_nad_floor(64 * 2.0 ** -24)
                 if k == args.warmup:
                     t_step = t_body = t_refresh = 0.0
                 t0 = time.perf_counter()
@@ -693,11 +702,12 @@ def run_free_body(args):
                           refresh_ms=1e3 * t_refresh / done, cloud_changes=changes,
                           clocks=clk.summary())
     a, b, br = runs[32], runs[64], runs["64r"]
+    allr = list(runs.values())
     # compare over the steps every run finished with a finite body state
-    n = min(len(x["path"]) for x in (a, b, br))
-    while n > 1 and not all(np.isfinite(x["path"][n - 1]).all() for x in (a, b, br)):
+    n = min(len(x["path"]) for x in allr)
+    while n > 1 and not all(np.isfinite(x["path"][n - 1]).all() for x in allr):
         n -= 1
-    for x in (a, b, br):
+    for x in allr:
         x["path"], x["angle"] = x["path"][:n], x["angle"][:n]
     disp64 = b["path"][-1, 0:3] - b["path"][0, 0:3]
     dev_centre = float(np.abs(a["path"][:, 0:3] - b["path"][:, 0:3]).max())
@@ -727,6 +737,12 @@ def run_free_body(args):
                                                   {"angle": b["angle"][:k + 1]})}
             for k in sorted({min(len(b["angle"]) - 1, m) for m in (500, 1000, 2000, 3000,
                                                                    4000, 5000)})},
+        # FP32 against FP64 run with the FP32 screen's floor: what FP32
+        # arithmetic alone contributes
+        "rotation_rel_diff_f32_vs_f64_fp32_floor": None if "64f" not in runs else {
+            str(k): rot_rel({"angle": a["angle"][:k + 1]}, {"angle": runs["64f"]["angle"][:k + 1]})
+            for k in sorted({min(len(b["angle"]) - 1, m) for m in (100, 250, 500, 1000, 2000,
+                                                                   3000)})},
         "displacement_m": {"f64": disp64.tolist(),
                            "max_centre_diff_m": dev_centre,
                            "max_centre_diff_f64_rounded_start_m": dev_centre_r,
