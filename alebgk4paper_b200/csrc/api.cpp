@@ -56,6 +56,31 @@ cudaError_t putRowOrder(alebgk_ctx *c, const int *boundary, int N)
     return cudaMemcpy(c->d.rowOrder, order.data(), 4 * (size_t)N, cudaMemcpyHostToDevice);
 }
 
+// Pinned host staging of at least `bytes` bytes, kept for the context's
+// life (grown when a larger cloud needs more), and the ring's events.
+cudaError_t pinnedStaging(alebgk_ctx *c, size_t bytes)
+{
+    for (auto &ev : c->pinEv)
+        if (!ev)
+        {
+            const cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+            if (e != cudaSuccess) return e;
+        }
+    if (c->pinBytes >= bytes) return cudaSuccess;
+    if (c->pin)
+    {
+        const cudaError_t e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) return e;
+        cudaFreeHost(c->pin);
+        c->pin = nullptr;
+        c->pinBytes = 0;
+    }
+    const cudaError_t e = cudaHostAlloc(&c->pin, bytes, cudaHostAllocDefault);
+    if (e == cudaSuccess) c->pinBytes = bytes;
+    else c->pin = nullptr;
+    return e;
+}
+
 void freeBuffers(alebgk_ctx *c)
 {
     DeviceBuffers &d = c->d;
@@ -161,6 +186,9 @@ int alebgk_destroy(alebgk_ctx *c)
     if (c->stream2) cudaStreamDestroy(c->stream2);
     if (c->evFork) cudaEventDestroy(c->evFork);
     if (c->evJoin) cudaEventDestroy(c->evJoin);
+    for (auto ev : c->pinEv)
+        if (ev) cudaEventDestroy(ev);
+    if (c->pin) cudaFreeHost(c->pin);
     delete c;
     return ALEBGK_OK;
 }
@@ -644,23 +672,71 @@ int alebgk_upload_state(alebgk_ctx *c, const double *g, const double *macro)
     if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
     CK(cudaSetDevice(c->cfg.device));
     const StepParams &p = c->sp;
-    const int N = p.N;
-    std::vector<double> mac(6 * (size_t)N);
-    std::vector<int> mood(N);
-    for (int i = 0; i < N; ++i)
+    const size_t N = p.N, gs = p.gs, ldf = p.ldf;
+    const bool fp32 = c->cfg.precision != 64;
+    // Staging: the macros (N x 6 doubles), the MOOD flags (N ints), and for
+    // FP32 a ring of row chunks of about 8 MB.
+    const size_t macBytes = 48 * N, moodOff = macBytes, moodBytes = (4 * N + 15) / 16 * 16;
+    const size_t rowBytes = 4 * ldf;
+    const size_t chunkRows = std::max<size_t>(1, (size_t(8) << 20) / rowBytes);
+    const size_t ringOff = moodOff + moodBytes;
+    const size_t need = ringOff + (fp32 ? alebgk_ctx::kPinChunks * chunkRows * rowBytes : 0);
+    cudaError_t e = pinnedStaging(c, need);
+    if (e != cudaSuccess)
+        return fail(c, ALEBGK_ECUDA, std::string("state upload staging: ") + cudaGetErrorString(e));
+    char *pin = static_cast<char *>(c->pin);
+    double *mac = reinterpret_cast<double *>(pin);
+    int *mood = reinterpret_cast<int *>(pin + moodOff);
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < (long long)N; ++i)
     {
-        for (int q = 0; q < 6; ++q) mac[6 * (size_t)i + q] = macro[7 * (size_t)i + q];
-        mood[i] = macro[7 * (size_t)i + 6] != 0.0;
+        for (int q = 0; q < 6; ++q) mac[6 * i + q] = macro[7 * i + q];
+        mood[i] = macro[7 * i + 6] != 0.0;
     }
-    CK(cudaMemcpy(c->d.macro[c->cur], mac.data(), mac.size() * 8, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->d.mood, mood.data(), 4 * (size_t)N, cudaMemcpyHostToDevice));
-    cudaError_t e = cudaMemcpyAsync(c->d.stage, g, (size_t)N * p.gs * 8,
-                                    cudaMemcpyHostToDevice, c->stream);
-    if (e == cudaSuccess) e = launchConvertIn(c, c->d.stage, c->cur);
+    e = cudaMemcpyAsync(c->d.macro[c->cur], mac, macBytes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c->d.mood, mood, 4 * N, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && fp32)
+    {
+        // FP32: the host rounds each value to FP32 (round to nearest, as the
+        // device conversion does) into a ring chunk while the copy engine
+        // moves the previous chunk, so half the bytes cross the bus and the
+        // conversion overlaps the transfer.
+        float *ring = reinterpret_cast<float *>(pin + ringOff);
+        float *f = static_cast<float *>(c->d.f[c->cur]);
+        int slot = 0;
+        for (size_t r0 = 0; r0 < N && e == cudaSuccess; r0 += chunkRows)
+        {
+            const size_t r1 = std::min(N, r0 + chunkRows);
+            if (r0 >= alebgk_ctx::kPinChunks * chunkRows) e = cudaEventSynchronize(c->pinEv[slot]);
+            if (e != cudaSuccess) break;
+            float *dst = ring + (size_t)slot * chunkRows * ldf;
+#pragma omp parallel for schedule(static)
+            for (long long i = (long long)r0; i < (long long)r1; ++i)
+            {
+                const double *src = g + (size_t)i * gs;
+                float *row = dst + (size_t)(i - r0) * ldf;
+                for (size_t k = 0; k < gs; ++k) row[k] = (float)src[k];
+                for (size_t k = gs; k < ldf; ++k) row[k] = 0.0f;
+            }
+            e = cudaMemcpyAsync(f + r0 * ldf, dst, (r1 - r0) * rowBytes, cudaMemcpyHostToDevice,
+                                c->stream);
+            if (e == cudaSuccess) e = cudaEventRecord(c->pinEv[slot], c->stream);
+            slot = (slot + 1) % alebgk_ctx::kPinChunks;
+        }
+    }
+    else if (e == cudaSuccess)
+    {
+        e = cudaMemcpyAsync(c->d.stage, g, N * gs * 8, cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess) e = launchConvertIn(c, c->d.stage, c->cur);
+    }
     if (e == cudaSuccess) e = launchMassInit(c);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess)
+    {
+        cudaStreamSynchronize(c->stream);
         return fail(c, ALEBGK_ECUDA, std::string("state upload: ") + cudaGetErrorString(e));
+    }
     return ALEBGK_OK;
 }
 
@@ -889,17 +965,19 @@ int alebgk_download_moments(alebgk_ctx *c, double *macro)
     if (!c || !macro) return fail(c, ALEBGK_EINVAL, "null argument");
     if (!c->uploaded) return fail(c, ALEBGK_ESTATE, "upload the cloud first");
     CK(cudaSetDevice(c->cfg.device));
-    const int N = c->sp.N;
-    std::vector<double> mac(6 * (size_t)N);
-    std::vector<int> mood(N);
-    CK(cudaMemcpyAsync(mac.data(), c->d.macro[c->cur], mac.size() * 8, cudaMemcpyDeviceToHost,
-                       c->stream));
-    CK(cudaMemcpyAsync(mood.data(), c->d.mood, 4 * (size_t)N, cudaMemcpyDeviceToHost, c->stream));
+    const size_t N = c->sp.N;
+    const size_t macBytes = 48 * N;
+    CK(pinnedStaging(c, macBytes + 4 * N));
+    double *mac = static_cast<double *>(c->pin);
+    int *mood = reinterpret_cast<int *>(static_cast<char *>(c->pin) + macBytes);
+    CK(cudaMemcpyAsync(mac, c->d.macro[c->cur], macBytes, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(mood, c->d.mood, 4 * N, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    for (int i = 0; i < N; ++i)
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < (long long)N; ++i)
     {
-        for (int q = 0; q < 6; ++q) macro[7 * (size_t)i + q] = mac[6 * (size_t)i + q];
-        macro[7 * (size_t)i + 6] = mood[i];
+        for (int q = 0; q < 6; ++q) macro[7 * i + q] = mac[6 * i + q];
+        macro[7 * i + 6] = mood[i];
     }
     return ALEBGK_OK;
 }

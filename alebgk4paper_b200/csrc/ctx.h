@@ -123,6 +123,13 @@ struct alebgk_ctx
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;          // side stream of the step graph
     cudaEvent_t evFork = nullptr, evJoin = nullptr;
+    // Pinned host staging of the state transfers (alebgk_upload_state,
+    // alebgk_download_moments), allocated on first use: the macro rows, then
+    // a ring of kPinChunks chunks of FP32 rows; one event per ring chunk.
+    static constexpr int kPinChunks = 4;
+    void *pin = nullptr;
+    size_t pinBytes = 0;
+    cudaEvent_t pinEv[kPinChunks] = {};
     int cur = 0;                 // buffer holding the current h and macros
     bool uploaded = false;
     int ncls = 0;

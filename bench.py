@@ -364,8 +364,15 @@ def run_ours(args):
     barrier()
     te = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
     e2e_value = weak_value(world, updates, args.e2e_steps, te)
-    h2d = N * case.gstride * 8 + N * 7 * 8
-    d2h = N * 7 * 8
+    # Bytes that cross the bus per step.  The host rows are FP64 (N x
+    # gstride); an FP32 context rounds them on the host and copies FP32 rows
+    # of the device stride (V rounded up to a multiple of four), an FP64
+    # context copies the FP64 rows.  Macros go up and come back as N x 6
+    # doubles plus the N MOOD flags (4-byte ints).
+    ldf = (V + 3) // 4 * 4
+    h2d = (N * ldf * 4 if args.precision == 32 else N * case.gstride * 8) + N * (48 + 4)
+    d2h = N * (48 + 4)
+    host_in = N * case.gstride * 8 + N * 7 * 8
 
     cnt = s.counters()
     s.close()
@@ -432,8 +439,11 @@ def run_ours(args):
                           "note": "whole step against 8 B/update (FP32) algorithmic bytes"},
         "e2e": {"value": e2e_value, "unit": "updates/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
+                "host_input_bytes_per_step": host_in,
                 "path": "alebgk_upload_state + alebgk_step + alebgk_download_moments, "
-                        "pinned host buffers, wall clock"},
+                        "pinned host buffers, wall clock" +
+                        ("; FP32 rows rounded on the host cores into a pinned ring, "
+                         "overlapped with the copies" if args.precision == 32 else "")},
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "counters": {"transport_flags": cnt["transport_flags"],

@@ -141,7 +141,12 @@ int alebgk_upload(alebgk_ctx *ctx, const alebgk_cloud *cloud, double dt);
 
 /* Replaces only the distribution and macro fields (same geometry), e.g. a
  * checkpoint restore.  No reference counterpart (cudaUploadCloud's
- * layout-reuse path, Solver/CudaBackend.cu:1262-1263, covers it). */
+ * layout-reuse path, Solver/CudaBackend.cu:1262-1263, covers it).
+ * g is N x gstride doubles, macro N x 7 (rho, u, v, w, T, p, moodFlag).
+ * A precision-32 context rounds g to FP32 (round to nearest, ties to even)
+ * on the host's OpenMP threads, chunk by chunk into pinned staging that the
+ * context keeps, while the copy engine moves the previous chunk; a
+ * precision-64 context copies the FP64 rows.  Returns after the copies. */
 int alebgk_upload_state(alebgk_ctx *ctx, const double *g, const double *macro);
 
 /* Moments rho, u, T, p and moodFlag into macro (N*7).
