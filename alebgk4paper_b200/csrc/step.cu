@@ -1144,7 +1144,16 @@ k_particle_rows(ParticleArgs<float> a, StepParams p)
     __shared__ double velD[kMaxNv];
     __shared__ float velF[kMaxNv];
     __shared__ int idxT[V];
+    // One staged row per warp (the next row to process, by one bulk copy).
+    constexpr int LDF = (V + 3) / 4 * 4;
+    __shared__ __align__(16) float rowBuf[kRowsThreads / 32][LDF];
+    __shared__ __align__(8) uint64_t rowBar[kRowsThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+    {
+        mbarInit(&rowBar[warp], 1);
+        mbarInitFence();
+    }
     for (int k = threadIdx.x; k < V; k += blockDim.x)
     {
         const int iv = k % NV, jv = (k / NV) % NV, kv = k / (NV * NV);
@@ -1164,13 +1173,58 @@ k_particle_rows(ParticleArgs<float> a, StepParams p)
     const double myV = lane < 3 * NV ? velD[myNode] : 0.0;
     const double dvN = p.dvN, c1 = p.c1;
     const int W = gridDim.x * (blockDim.x >> 5);
-    for (int t = blockIdx.x * (blockDim.x >> 5) + warp; t < p.N; t += W)
+    constexpr uint32_t kRowBytes = 4u * LDF;
+    // The warp's rows: t, t + W, ...; the index, wall flag and screen range
+    // of the next row are loaded one row ahead, and the next row itself is
+    // staged into rowBuf by one bulk copy while the current row is processed.
+    int t = blockIdx.x * (blockDim.x >> 5) + warp;
+    int inext = t < p.N ? a.rowOrder[t] : 0;
+    int wallN = t < p.N ? a.boundary[inext] : 0;
+    double2 nadN = (t < p.N && p.limiter == 2) ? reinterpret_cast<const double2 *>(a.nad)[inext]
+                                                 : make_double2(INFINITY, -INFINITY);
+    int inext2 = t + W < p.N ? a.rowOrder[t + W] : 0;
+    if (lane == 0 && t < p.N)
     {
-        const int i = a.rowOrder[t];
+        mbarExpectTx(&rowBar[warp], kRowBytes);
+        bulkLoad(&rowBuf[warp][0], a.g + (size_t)inext * p.ldf, kRowBytes, &rowBar[warp]);
+    }
+    bool dead = false;
+    for (uint32_t it = 0; t < p.N; t += W, ++it)
+    {
+        const int i = inext;
+        const int wallI = wallN;
+        const double2 nadI = nadN;
+        const bool more = t + W < p.N;
+        inext = inext2;
+        // loads for the next row, first used in the next iteration
+        wallN = more ? a.boundary[inext] : 0;
+        nadN = (more && p.limiter == 2) ? reinterpret_cast<const double2 *>(a.nad)[inext]
+                                        : make_double2(INFINITY, -INFINITY);
+        inext2 = t + 2 * W < p.N ? a.rowOrder[t + 2 * W] : 0;
         float *row = a.g + (size_t)i * p.ldf;
         float x[LPL][NV];
-        loadRowLines<NV>(row, lane, x);
-        const int wallI = a.boundary[i];
+        mbarWait(&rowBar[warp], it & 1u, dead);
+        if (__any_sync(0xffffffffu, dead))
+        {
+            // The row never arrived: report, give the copy a second bounded
+            // wait, stop.
+            if (lane == 0)
+            {
+                atomicOr(&a.sc->err, 4);
+                bool d2 = false;
+                mbarWait(&rowBar[warp], it & 1u, d2);
+            }
+            __syncwarp();
+            return;
+        }
+        loadRowLines<NV>(&rowBuf[warp][0], lane, x);
+        __syncwarp();
+        if (lane == 0 && more)
+        {
+            fenceProxyAsync();     // the warp's reads of rowBuf are done
+            mbarExpectTx(&rowBar[warp], kRowBytes);
+            bulkLoad(&rowBuf[warp][0], a.g + (size_t)inext * p.ldf, kRowBytes, &rowBar[warp]);
+        }
         float s0 = 0.f, sn = 0.f, sx = 0.f, sy = 0.f, sz = 0.f, se = 0.f;
 #pragma unroll
         for (int j = 0; j < LPL; ++j)
@@ -1217,7 +1271,7 @@ k_particle_rows(ParticleArgs<float> a, StepParams p)
         int flagged = 0;
         if (p.limiter == 2)
         {
-            const double2 nad = reinterpret_cast<const double2 *>(a.nad)[i];
+            const double2 nad = nadI;
             if (bad || m <= 0.0) flagged = 1;
             else if (isfinite(nad.x) && isfinite(nad.y))
             {
@@ -2287,8 +2341,10 @@ static cudaError_t prepareT(alebgk_ctx *c)
         // The register-row form of the same stages (FP32, Nv of an
         // instance): the default, unless the shared-memory form is asked for.
         c->pRows = false;
+        // (Its staged rows are (V + 3) / 4 * 4 floats, the FP32 row stride.)
         const RowsKernel rk = rowsKernel(p.Nv);
-        if (e == cudaSuccess && c->pStream && sizeof(T) == 4 && c->cfg.particle != 3 && rk)
+        if (e == cudaSuccess && c->pStream && sizeof(T) == 4 && c->cfg.particle != 3 && rk &&
+            p.dim == 3 && p.ldf == (p.V + 3) / 4 * 4)
         {
             int occ = 0, sms = 0;
             e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
