@@ -673,11 +673,13 @@ int alebgk_upload_state(alebgk_ctx *c, const double *g, const double *macro)
     CK(cudaSetDevice(c->cfg.device));
     const StepParams &p = c->sp;
     const size_t N = p.N, gs = p.gs, ldf = p.ldf;
-    const bool fp32 = c->cfg.precision != 64;
     // Staging: the macros (N x 6 doubles), the MOOD flags (N ints), and for
-    // FP32 a ring of row chunks of about 8 MB.
-    const size_t macBytes = 48 * N, moodOff = macBytes, moodBytes = (4 * N + 15) / 16 * 16;
+    // FP32 clouds of at least 32 MB of rows a ring of row chunks of about
+    // 8 MB.  Smaller clouds copy the FP64 rows and convert on the device, so
+    // that a batch of many small contexts pins little host memory.
     const size_t rowBytes = 4 * ldf;
+    const bool fp32 = c->cfg.precision != 64 && N * rowBytes >= (size_t(32) << 20);
+    const size_t macBytes = 48 * N, moodOff = macBytes, moodBytes = (4 * N + 15) / 16 * 16;
     const size_t chunkRows = std::max<size_t>(1, (size_t(8) << 20) / rowBytes);
     const size_t ringOff = moodOff + moodBytes;
     const size_t need = ringOff + (fp32 ? alebgk_ctx::kPinChunks * chunkRows * rowBytes : 0);

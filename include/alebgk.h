@@ -143,10 +143,12 @@ int alebgk_upload(alebgk_ctx *ctx, const alebgk_cloud *cloud, double dt);
  * checkpoint restore.  No reference counterpart (cudaUploadCloud's
  * layout-reuse path, Solver/CudaBackend.cu:1262-1263, covers it).
  * g is N x gstride doubles, macro N x 7 (rho, u, v, w, T, p, moodFlag).
- * A precision-32 context rounds g to FP32 (round to nearest, ties to even)
- * on the host's OpenMP threads, chunk by chunk into pinned staging that the
- * context keeps, while the copy engine moves the previous chunk; a
- * precision-64 context copies the FP64 rows.  Returns after the copies. */
+ * A precision-32 context whose FP32 rows take at least 32 MB rounds g to
+ * FP32 (round to nearest, ties to even) on the host's OpenMP threads, chunk
+ * by chunk into pinned staging that the context keeps (four 8 MB chunks),
+ * while the copy engine moves the previous chunk.  Smaller clouds and
+ * precision-64 contexts copy the FP64 rows and convert on the device; the
+ * stored state is the same bits either way.  Returns after the copies. */
 int alebgk_upload_state(alebgk_ctx *ctx, const double *g, const double *macro);
 
 /* Moments rho, u, T, p and moodFlag into macro (N*7).

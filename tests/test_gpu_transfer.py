@@ -1,10 +1,11 @@
 """State transfers through the C-ABI: alebgk_upload_state puts the host
 rows on the device as the device conversion would (FP64: unchanged; FP32:
 each value rounded to the nearest FP32, ties to even), and
-alebgk_download_full / alebgk_download_moments bring them back.  The FP32
-upload converts on the host into a pinned ring of about 8 MB row chunks
-while the copy engine moves the previous chunk; cavity3d Nx=30 Nv=10 is
-108 MB of FP32 rows, so the ring wraps several times."""
+alebgk_download_full / alebgk_download_moments bring them back.  An FP32
+upload of at least 32 MB of rows converts on the host into a pinned ring of
+about 8 MB row chunks while the copy engine moves the previous chunk;
+cavity3d Nx=30 Nv=10 is 108 MB of FP32 rows, so the ring wraps several
+times."""
 import ctypes
 
 import numpy as np
@@ -29,9 +30,11 @@ def _state(N, gs, seed):
     return g
 
 
-@pytest.mark.parametrize("precision", [32, 64])
-def test_state_upload_rounds_each_value_once(gpu, precision):
-    c = ab.Case("cavity3d", 30, 10, -1.0, 2)
+@pytest.mark.parametrize("precision,Nx", [(32, 30), (64, 30), (32, 12)])
+def test_state_upload_rounds_each_value_once(gpu, precision, Nx):
+    """Nx 30: the host-rounding ring (108 MB of FP32 rows); Nx 12: below the
+    ring's 32 MB threshold, the device conversion."""
+    c = ab.Case("cavity3d", Nx, 10, -1.0, 2)
     s = ab.Solver(c, precision=precision)
     g = _state(s.N, s.gstride, 11)
     m = np.array(c.macro, dtype=np.float64, copy=True)
