@@ -409,9 +409,11 @@ def run_ours(args):
                    "parallelism": f"{world} independent cavities, one per GPU",
                    "l2": "inputs larger than L2: two 256 MB distribution buffers "
                          "ping-pong, no flush needed"},
-        # one launch per stage: step_begin, transport, particle, redo, sigma,
-        # fixup, mass_sum, scale_mood, recollide, mass_end
-        "gpu_launches": 10 * args.steps,
+        # per step in the step graph: k_step_begin twice (the one-block
+        # scalar reset, then the NAD ranges on the side stream beside the
+        # transport), then transport, particle, redo, sigma, fixup, mass_sum,
+        # scale_mood, recollide, mass_end
+        "gpu_launches": 11 * args.steps,
         "kernels": kernels,
         "stage_ms": {k: round(v, 5) for k, v in stage_ms.items()},
         "roofline": {"bound": "hbm", "kernel": kern_name, "achieved": achieved,
