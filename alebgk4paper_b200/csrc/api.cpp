@@ -56,6 +56,30 @@ cudaError_t putRowOrder(alebgk_ctx *c, const int *boundary, int N)
     return cudaMemcpy(c->d.rowOrder, order.data(), 4 * (size_t)N, cudaMemcpyHostToDevice);
 }
 
+// The neighbour lists of a cloud: counts within 0..ALEBGK_MAX_NEIGH, indices
+// of other particles.  Checked on the host's OpenMP threads; the error names
+// the first particle that fails, as a serial check would.
+int checkNeighbours(alebgk_ctx *c, const alebgk_cloud *cl, int N)
+{
+    auto bad = [&](int i) -> int {
+        if (cl->nnb[i] < 0 || cl->nnb[i] > ALEBGK_MAX_NEIGH) return 1;
+        for (int s = 0; s < cl->nnb[i]; ++s)
+        {
+            const int j = cl->nbr[(size_t)i * ALEBGK_MAX_NEIGH + s];
+            if (j < 0 || j >= N || j == i) return 2;
+        }
+        return 0;
+    };
+    int first = N;
+#pragma omp parallel for schedule(static) reduction(min : first)
+    for (int i = 0; i < N; ++i)
+        if (i < first && bad(i)) first = i;
+    if (first == N) return ALEBGK_OK;
+    return fail(c, ALEBGK_EINVAL,
+                std::string(bad(first) == 1 ? "neighbour count" : "neighbour index") +
+                    " out of range at particle " + std::to_string(first));
+}
+
 // Pinned host staging of at least `bytes` bytes, kept for the context's
 // life (grown when a larger cloud needs more), and the ring's events.
 cudaError_t pinnedStaging(alebgk_ctx *c, size_t bytes)
@@ -221,19 +245,7 @@ static int uploadCloud(alebgk_ctx *c, const alebgk_cloud *cl, double dt, bool wi
     p.c1 = 1.0 / (1.0 + p.lam);
     p.inv3R = 1.0 / (3.0 * p.R);
     const int N = p.N;
-    for (int i = 0; i < N; ++i)
-    {
-        if (cl->nnb[i] < 0 || cl->nnb[i] > ALEBGK_MAX_NEIGH)
-            return fail(c, ALEBGK_EINVAL, "neighbour count out of range at particle " +
-                                              std::to_string(i));
-        for (int s = 0; s < cl->nnb[i]; ++s)
-        {
-            int j = cl->nbr[(size_t)i * ALEBGK_MAX_NEIGH + s];
-            if (j < 0 || j >= N || j == i)
-                return fail(c, ALEBGK_EINVAL, "neighbour index out of range at particle " +
-                                                  std::to_string(i));
-        }
-    }
+    if (const int r = checkNeighbours(c, cl, N)) return r;
     CoeffInput in;
     in.dim = p.dim; in.N = N; in.Nv = p.Nv; in.mlsOrder = p.mlsOrder;
     in.dt = dt; in.h = p.h; in.vmin = p.vmin; in.dv = p.dv;
@@ -488,19 +500,7 @@ int refreshGeometryInPlace(alebgk_ctx *c, const alebgk_cloud *cl, double dt)
     if (!f64 && c->cfg.transport != 1 && !anyBody &&
         marchEligible(cl->xyz, N, p.dim, cl->nnb, cl->nbr, ALEBGK_MAX_NEIGH))
         return 1;
-    for (int i = 0; i < N; ++i)
-    {
-        if (cl->nnb[i] < 0 || cl->nnb[i] > ALEBGK_MAX_NEIGH)
-            return fail(c, ALEBGK_EINVAL, "neighbour count out of range at particle " +
-                                              std::to_string(i));
-        for (int s = 0; s < cl->nnb[i]; ++s)
-        {
-            int j = cl->nbr[(size_t)i * ALEBGK_MAX_NEIGH + s];
-            if (j < 0 || j >= N || j == i)
-                return fail(c, ALEBGK_EINVAL, "neighbour index out of range at particle " +
-                                                  std::to_string(i));
-        }
-    }
+    if (const int r = checkNeighbours(c, cl, N)) return r;
     p.dt = dt;
     p.lam = dt / p.tau;
     p.c1 = 1.0 / (1.0 + p.lam);

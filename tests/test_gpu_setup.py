@@ -180,3 +180,33 @@ def test_device_mls_tables_equal_host_tables(name, kw, precision):
     assert np.array_equal(ga, gb) and np.array_equal(ma, mb)
     a.cudaFreeCloud()
     b.cudaFreeCloud()
+
+
+def test_bad_neighbour_lists_are_refused_at_the_first_bad_particle(gpu):
+    """The upload and the in-place geometry refresh check every neighbour
+    list (counts within 0..ALEBGK_MAX_NEIGH, indices of other particles) and
+    name the first particle that fails."""
+    import ctypes
+    import alebgk4paper_b200 as ab
+    c = ab.Case("cavity3d", 8, 4, -1.0, 2)
+    good_nbr, good_nnb = c.nbr.copy(), c.nnb.copy()
+    c.nbr[40, 2] = c.N                 # index past the cloud
+    c.nbr[17, 0] = 17                  # itself
+    with pytest.raises(ab.AlebgkError, match="neighbour index out of range at particle 17"):
+        ab.Solver(c, precision=64)
+    c.nbr[:], c.nnb[:] = good_nbr, good_nnb
+    c.nnb[9] = -1
+    with pytest.raises(ab.AlebgkError, match="neighbour count out of range at particle 9"):
+        ab.Solver(c, precision=64)
+    # the in-place refresh of an uploaded context (FP64: the general path)
+    c.nbr[:], c.nnb[:] = good_nbr, good_nnb
+    s = ab.Solver(c, precision=64)
+    c.nbr[33, 1] = -5
+    cl = c.cloud()
+    rc = s.lib.alebgk_upload_geometry(s.ctx, ctypes.byref(cl), c.dt)
+    assert rc != 0
+    buf = ctypes.create_string_buffer(512)
+    s.lib.alebgk_last_error(s.ctx, buf, 512)
+    assert "neighbour index out of range at particle 33" in buf.value.decode()
+    c.nbr[:] = good_nbr
+    s.close()
