@@ -167,8 +167,16 @@ int alebgk_create(const alebgk_config *cfg, alebgk_ctx **out)
     if (!c) return fail(nullptr, ALEBGK_ENOMEM, "host allocation failed");
     c->cfg = *cfg;
     cudaError_t e = cudaSetDevice(cfg->device);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking);
+    // The step's stream at the highest priority, the side stream (the NAD
+    // ranges beside the transport) at the lowest: the transport's CTAs are
+    // placed first, the side work fills the SMs the transport's last wave
+    // leaves idle.
+    int prLeast = 0, prGreatest = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&prLeast, &prGreatest);
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, prGreatest);
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prLeast);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->evFork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->evJoin, cudaEventDisableTiming);
     if (e != cudaSuccess)
@@ -877,7 +885,8 @@ int alebgk_step(alebgk_ctx *c, int nsteps)
                             std::string("step capture: ") +
                                 cudaGetErrorString(le != cudaSuccess ? le : ee));
             }
-            cudaError_t ie = cudaGraphInstantiate(&c->graph[from], g, 0);
+            cudaError_t ie =
+                cudaGraphInstantiate(&c->graph[from], g, cudaGraphInstantiateFlagUseNodePriority);
             cudaGraphDestroy(g);
             if (ie != cudaSuccess)
                 return fail(c, ALEBGK_ECUDA, std::string("graph instantiate: ") +
