@@ -265,7 +265,8 @@ def test_streamed_particle_kernel_matches_general(gpu, case, Nx, Nv, precision, 
     g.close()
 
 
-@pytest.mark.parametrize("case,Nx,Nv,steps", [("cavity3d", 13, 10, 4), ("cavity3d", 9, 5, 3),
+@pytest.mark.parametrize("case,Nx,Nv,steps", [("cavity3d", 13, 10, 4), ("cavity3d", 10, 8, 3),
+                                              ("cavity3d", 9, 5, 3),
                                               ("cavity3d-sphere", 12, 4, 2)])
 def test_row_kernels_match_streamed_particle_kernel(gpu, case, Nx, Nv, steps):
     """FP32: the three row kernels (row sums; per-particle decisions and
