@@ -1144,14 +1144,16 @@ k_particle_rows(ParticleArgs<float> a, StepParams p)
     __shared__ double velD[kMaxNv];
     __shared__ float velF[kMaxNv];
     __shared__ int idxT[V];
-    // One staged row per warp (the next row to process, by one bulk copy).
+    // Two staged rows per warp: the row being processed (the wall rows' flux
+    // balance reads it from here) and the next one, arriving by one bulk copy.
     constexpr int LDF = (V + 3) / 4 * 4;
-    __shared__ __align__(16) float rowBuf[kRowsThreads / 32][LDF];
-    __shared__ __align__(8) uint64_t rowBar[kRowsThreads / 32];
+    __shared__ __align__(16) float rowBuf[kRowsThreads / 32][2][LDF];
+    __shared__ __align__(8) uint64_t rowBar[kRowsThreads / 32][2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0)
     {
-        mbarInit(&rowBar[warp], 1);
+        mbarInit(&rowBar[warp][0], 1);
+        mbarInit(&rowBar[warp][1], 1);
         mbarInitFence();
     }
     for (int k = threadIdx.x; k < V; k += blockDim.x)
@@ -1176,7 +1178,8 @@ k_particle_rows(ParticleArgs<float> a, StepParams p)
     constexpr uint32_t kRowBytes = 4u * LDF;
     // The warp's rows: t, t + W, ...; the index, wall flag and screen range
     // of the next row are loaded one row ahead, and the next row itself is
-    // staged into rowBuf by one bulk copy while the current row is processed.
+    // staged into the other rowBuf by one bulk copy while the current row is
+    // processed.
     int t = blockIdx.x * (blockDim.x >> 5) + warp;
     int inext = t < p.N ? a.rowOrder[t] : 0;
     int wallN = t < p.N ? a.boundary[inext] : 0;
@@ -1185,8 +1188,8 @@ k_particle_rows(ParticleArgs<float> a, StepParams p)
     int inext2 = t + W < p.N ? a.rowOrder[t + W] : 0;
     if (lane == 0 && t < p.N)
     {
-        mbarExpectTx(&rowBar[warp], kRowBytes);
-        bulkLoad(&rowBuf[warp][0], a.g + (size_t)inext * p.ldf, kRowBytes, &rowBar[warp]);
+        mbarExpectTx(&rowBar[warp][0], kRowBytes);
+        bulkLoad(&rowBuf[warp][0][0], a.g + (size_t)inext * p.ldf, kRowBytes, &rowBar[warp][0]);
     }
     bool dead = false;
     for (uint32_t it = 0; t < p.N; t += W, ++it)
@@ -1203,7 +1206,9 @@ k_particle_rows(ParticleArgs<float> a, StepParams p)
         inext2 = t + 2 * W < p.N ? a.rowOrder[t + 2 * W] : 0;
         float *row = a.g + (size_t)i * p.ldf;
         float x[LPL][NV];
-        mbarWait(&rowBar[warp], it & 1u, dead);
+        const int b = it & 1;
+        const uint32_t par = (it >> 1) & 1u;
+        mbarWait(&rowBar[warp][b], par, dead);
         if (__any_sync(0xffffffffu, dead))
         {
             // The row never arrived: report, give the copy a second bounded
@@ -1212,18 +1217,19 @@ k_particle_rows(ParticleArgs<float> a, StepParams p)
             {
                 atomicOr(&a.sc->err, 4);
                 bool d2 = false;
-                mbarWait(&rowBar[warp], it & 1u, d2);
+                mbarWait(&rowBar[warp][b], par, d2);
             }
             __syncwarp();
             return;
         }
-        loadRowLines<NV>(&rowBuf[warp][0], lane, x);
+        loadRowLines<NV>(&rowBuf[warp][b][0], lane, x);
         __syncwarp();
         if (lane == 0 && more)
         {
-            fenceProxyAsync();     // the warp's reads of rowBuf are done
-            mbarExpectTx(&rowBar[warp], kRowBytes);
-            bulkLoad(&rowBuf[warp][0], a.g + (size_t)inext * p.ldf, kRowBytes, &rowBar[warp]);
+            fenceProxyAsync();     // the warp's reads of the other buffer are done
+            mbarExpectTx(&rowBar[warp][b ^ 1], kRowBytes);
+            bulkLoad(&rowBuf[warp][b ^ 1][0], a.g + (size_t)inext * p.ldf, kRowBytes,
+                     &rowBar[warp][b ^ 1]);
         }
         float s0 = 0.f, sn = 0.f, sx = 0.f, sy = 0.f, sz = 0.f, se = 0.f;
 #pragma unroll
@@ -1264,7 +1270,8 @@ k_particle_rows(ParticleArgs<float> a, StepParams p)
                 if (pv.fix) atomicAdd(&a.sc->nfix, 1);
                 a.massPos[i] = m * dvN;
             }
-            finishWallStream(a, p, i, row, idxT, velD, pv, wtab[warp], lane);
+            finishWallStream(a, p, i, (const float *)&rowBuf[warp][b][0], idxT, velD, pv,
+                             wtab[warp], lane);
             __syncwarp();
             continue;
         }
