@@ -93,6 +93,22 @@ def weak_value(world: int, updates_per_rank: int, steps: int, seconds: float) ->
     return world * updates_per_rank * steps / seconds
 
 
+def e2e_bytes(N: int, V: int, gstride: int, precision: int):
+    """(host-to-device, device-to-host, host input) bytes of one end-to-end
+    step: alebgk_upload_state of the FP64 host rows (N x gstride) and macros
+    (N x 7), then alebgk_download_moments.  An FP32 context whose FP32 rows
+    (the device stride: V rounded up to a multiple of four) take at least
+    32 MiB rounds them on the host and copies FP32 rows; smaller FP32 clouds
+    and FP64 contexts copy the FP64 rows.  The macros cross as N x 6 doubles
+    plus the N MOOD flags (4-byte ints), each way."""
+    ldf = (V + 3) // 4 * 4
+    ring = precision == 32 and N * ldf * 4 >= (32 << 20)
+    h2d = (N * ldf * 4 if ring else N * gstride * 8) + N * (48 + 4)
+    d2h = N * (48 + 4)
+    host_in = N * gstride * 8 + N * 7 * 8
+    return h2d, d2h, host_in
+
+
 # ---------------------------------------------------------------------------
 class ClockSampler:
     """Samples nvidia-smi clocks and throttle reasons during the timed region."""
@@ -370,15 +386,7 @@ def run_ours(args):
         windows.append(max_over_ranks(time.perf_counter() - t0, dist, "cuda"))
     te = sorted(windows)[1]
     e2e_value = weak_value(world, updates, args.e2e_steps, te)
-    # Bytes that cross the bus per step.  The host rows are FP64 (N x
-    # gstride); an FP32 context rounds them on the host and copies FP32 rows
-    # of the device stride (V rounded up to a multiple of four), an FP64
-    # context copies the FP64 rows.  Macros go up and come back as N x 6
-    # doubles plus the N MOOD flags (4-byte ints).
-    ldf = (V + 3) // 4 * 4
-    h2d = (N * ldf * 4 if args.precision == 32 else N * case.gstride * 8) + N * (48 + 4)
-    d2h = N * (48 + 4)
-    host_in = N * case.gstride * 8 + N * 7 * 8
+    h2d, d2h, host_in = e2e_bytes(N, V, case.gstride, args.precision)
 
     cnt = s.counters()
     s.close()
@@ -453,7 +461,7 @@ def run_ours(args):
                 "path": "alebgk_upload_state + alebgk_step + alebgk_download_moments, "
                         "pinned host buffers, wall clock" +
                         ("; FP32 rows rounded on the host cores into a pinned ring, "
-                         "overlapped with the copies" if args.precision == 32 else "")},
+                         "overlapped with the copies" if h2d < host_in else "")},
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "counters": {"transport_flags": cnt["transport_flags"],
